@@ -1,0 +1,279 @@
+#!/usr/bin/env python
+"""Benchmark: matrix-free H.x effective HBM bandwidth on B200.
+
+Workload: periodic spin-1/2 Heisenberg chain, N=28, J=1, Sz=0 sector
+(dim 40,116,600), OpSum Sz_i Sz_i+1 + 0.5 (Sp_i Sm_i+1 + Sm_i Sp_i+1).
+One step = one y = H x over the whole sector.  Effective bytes per step
+= dim * (bytes(x) + bytes(y)), the metric's algorithmic traffic (sector
+tables, term tables and repeated gathers are not counted).
+
+  value  device H.x on complex128 vectors resident in HBM (the drop-in
+         fp64 path); x (642 MB) is larger than L2, so no flush is needed
+  e2e    the same apply through the C ABI entry point with host buffers
+         (qkrylov_hamiltonian_apply_complex_f64): H2D of x, kernel, D2H of y
+  variants  the same kernel on complex64 / float64 / float32 vectors
+
+--impl reference times the reference's own CPU implementation (its
+unchanged sources, oracle/_ref, OpenMP on all host cores) on a bounded
+sample of the workload, on the same metric.
+
+Multi-GPU (--gpus N under torchrun): the operator does not shard in this
+build, so every rank runs an independent replica; value = N * bytes / max
+rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu, self.samples, self.proc = gpu, [], None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        time.sleep(0.25)
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=2)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def heisenberg_opsum(qk, N, dtype):
+    os_ = qk.OpSum(dtype=dtype)
+    for i in range(N):
+        j = (i + 1) % N
+        os_.add_term(1.0, "Sz", i, "Sz", j)
+        os_.add_term(0.5, "Sp", i, "Sm", j)
+        os_.add_term(0.5, "Sm", i, "Sp", j)
+    return os_
+
+
+def cpu_reference_gbs(N=24, steps=3, use_ref=True):
+    """Reference CPU H.x (its CSR SpMV through the host-pointer apply) on
+    all host threads; returns GB/s on the same effective-bytes metric."""
+    import oracle as O
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    kind = "reference" if use_ref and O.have_ref() else "port"
+    back = O.ref() if kind == "reference" else O.port()
+    t0 = time.perf_counter()
+    H = back.hamiltonian("spin", N, dict(use_sz=1, sz2=0), O.heisenberg_chain(N))
+    setup = time.perf_counter() - t0
+    x = np.random.default_rng(0).standard_normal(H.dim) + 1j * np.random.default_rng(1).standard_normal(H.dim)
+    H.apply(x)
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        H.apply(x)
+        ts.append(time.perf_counter() - t0)
+    t = float(np.median(ts))
+    return dict(value=H.dim * 32 / t / 1e9, unit="GB/s", cores=int(os.environ.get("OMP_NUM_THREADS", threads)),
+                kind=kind, sample=f"Heisenberg N={N} Sz=0 (dim {H.dim}) complex128 H.x, median of {steps}; "
+                f"setup (basis + CSR build) {setup:.1f} s; N=28 needs ~100 GB of CSR + reserve on the host",
+                seconds_per_apply=t)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cb = cpu_reference_gbs(N=24, steps=max(1, min(args.steps, 5)))
+    line = {"metric": "Hx effective HBM GB/s (Heisenberg N=28 Sz=0)", "value": cb["value"], "unit": "GB/s",
+            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cb["seconds_per_apply"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": "heisenberg_chain_N28_Sz0_Hx", "N": 28, "dim": 40116600,
+                       "sample_N": 24, "parallelism": "cpu-openmp"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    import qkrylov_b200 as qk
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    N = args.n
+    H = qk.MatrixFreeHamiltonian(qk.SpinHalfBasis(N, sz=0), qk.SpinHalfSite(), heisenberg_opsum(qk, N, np.float64),
+                                 device=f"cuda:{local}", dtype=np.float64)
+    D = H.dimension
+    stream = torch.cuda.ExternalStream(H.stream)
+    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
+
+    def time_apply(dt_code, tdt, bytes_per, steps, warmup):
+        x = torch.randn(D, dtype=tdt, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        torch.cuda.synchronize()
+        for _ in range(warmup):
+            H.apply_device(x.data_ptr(), y.data_ptr(), dt_code)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = qk.lib().qkrylov_b200_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            H.apply_device(x.data_ptr(), y.data_ptr(), dt_code)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms = e0.elapsed_time(e1) / steps
+        launches = int(qk.lib().qkrylov_b200_launch_count() - l0)
+        del x, y
+        return ms, launches
+
+    peak, peak_kind = peaks()
+    with ClockSampler(local) as clk:
+        ms, launches = time_apply(qk.DTYPE_C128, torch.complex128, 32, args.steps, args.warmup)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    bytes_step = D * 32
+    value = world * bytes_step / (ms * 1e-3) / 1e9
+
+    variants = {}
+    for name, code, tdt, b in [("c64", qk.DTYPE_C64, torch.complex64, 16), ("f64", qk.DTYPE_F64, torch.float64, 16),
+                               ("f32", qk.DTYPE_F32, torch.float32, 8)]:
+        vms, _ = time_apply(code, tdt, b, max(3, args.steps // 2), 2)
+        variants[name] = {"ms_per_apply": vms, "GBs_effective": D * b / (vms * 1e-3) / 1e9,
+                          "frac_of_measured_hbm": D * b / (vms * 1e-3) / 1e9 / peak}
+
+    # e2e through the C ABI with pinned host buffers
+    xh = torch.randn(D, dtype=torch.complex128, generator=torch.Generator().manual_seed(7)).pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    L = qk.lib()
+    for _ in range(2):
+        L.qkrylov_hamiltonian_apply_complex_f64(H._h, xh.data_ptr(), yh.data_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ke2e = max(3, args.steps // 2)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(ke2e):
+        rc = L.qkrylov_hamiltonian_apply_complex_f64(H._h, xh.data_ptr(), yh.data_ptr())
+        assert rc == 0
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / ke2e
+
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "hx_heisenberg_n28_c128.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    line = {"metric": "Hx effective HBM GB/s (Heisenberg N=28 Sz=0)", "value": value, "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic",
+            "config": {"workload": "heisenberg_chain_N28_Sz0_Hx", "N": N, "dim": D, "terms": 3 * N,
+                       "vector": "complex128", "l2": "inputs larger than L2 (x = 642 MB)",
+                       "parallelism": "replicas" if world > 1 else "single-gpu"},
+            "roofline": {"bound": "hbm", "achieved": bytes_step / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": bytes_step / (ms * 1e-3) / 1e9 / peak, "traffic": traffic,
+                         "peak_source": peak_kind, "kernel": "k_hx<complex128, real coefficients>"},
+            "e2e": {"value": world * bytes_step / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
+                    "h2d_bytes_per_step": D * 16, "d2h_bytes_per_step": D * 16, "ms_per_step": e2e_ms,
+                    "path": "qkrylov_hamiltonian_apply_complex_f64, pinned host buffers"},
+            "variants": variants,
+            "gpu_launches": launches,
+            "clocks": clk.summary()}
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_reference_gbs(N=24, steps=2)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as e:  # reported, never silently replaced
+            line["cpu_baseline"] = {"value": None, "unit": "GB/s", "error": str(e)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=28)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,123 @@
+/* Extensions of the qkrylov C ABI provided by libqkrylov_b200.so.
+ *
+ * qkrylov's own C ABI (qkrylov_c_api.h) runs in single precision.  The
+ * functions here add: double-precision Hamiltonians and solvers (the
+ * reference's fp64 C++ namespace, src/solvers/*.cpp compiled with
+ * QKRYLOV_DOUBLE_PRECISION), device-pointer H.x for callers that keep
+ * vectors in HBM, a multi-temperature FTLM, the OpSum compiler's output for
+ * inspection, and library diagnostics.  They reuse the opaque handles of
+ * qkrylov_c_api.h.  All return QKRYLOV_SUCCESS / QKRYLOV_ERROR_INVALID_ARG /
+ * QKRYLOV_ERROR_EXCEPTION unless stated; qkrylov_b200_last_error() describes
+ * the last failure on the calling thread.
+ */
+#ifndef QKRYLOV_B200_H
+#define QKRYLOV_B200_H
+
+#include "qkrylov_c_api.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Vector element types of the device-pointer entry points. */
+#define QKRYLOV_DTYPE_C128 0 /* interleaved complex double */
+#define QKRYLOV_DTYPE_C64 1  /* interleaved complex float */
+#define QKRYLOV_DTYPE_F64 2  /* real double (real Hamiltonians only) */
+#define QKRYLOV_DTYPE_F32 3  /* real float (real Hamiltonians only) */
+
+/* ------------------------------------------------------------ diagnostics */
+const char* qkrylov_b200_last_error(void);
+/* Kernels launched by this library since it was loaded. */
+uint64_t qkrylov_b200_launch_count(void);
+int qkrylov_b200_device_count(void);
+
+/* Select which of N_up / N_dn a sector conserves after
+ * qkrylov_sector_set_hubbard_particles (c_api.h:33), which always sets
+ * both; qkrylov's C++ Sector allows either alone (sector.hpp:20-24). */
+int qkrylov_b200_sector_set_species(qkrylov_sector_h sector, int use_nup, int use_ndn);
+
+/* Site::apply (site.hpp:19-23) for a site handle: one operator on one state. */
+int qkrylov_b200_site_apply(qkrylov_site_h site, const char* op, int site_index, uint64_t state, int* valid,
+                            uint64_t* new_state, double* matrix_element /* [2] */);
+
+/* ------------------------------------------------------ basis (host only)
+ * Replaces the per-state loops a caller of qkrylov_basis_state /
+ * qkrylov_basis_index (c_api.h:51-52) would write. */
+int qkrylov_basis_states(qkrylov_basis_h basis, uint64_t first, uint64_t count, uint64_t* states_out);
+int qkrylov_basis_index_many(qkrylov_basis_h basis, const uint64_t* states, uint64_t n, int64_t* index_out);
+
+/* ------------------------------------------------------------------ OpSum
+ * qkrylov_opsum_add_term_nbody (c_api.h:75-76) with double coefficients. */
+int qkrylov_opsum_add_term_nbody_f64(qkrylov_opsum_h opsum, double coeff_real, double coeff_imag, int n_factors,
+                                     const char** ops, const int* sites);
+uint64_t qkrylov_opsum_size(qkrylov_opsum_h opsum);
+
+/* The OpSum compiler's output for (basis, site, opsum), without a GPU.
+ * Term t: valid on |s> iff (s & mask[3t]) == mask[3t+1]; element
+ * (coef[2t] + i coef[2t+1]) * (-1)^popcount(s & mask[3t+2]); terms
+ * [first[g], first[g]+count[g]) of group g reach s ^ flip[g]; check[g] = 1
+ * when that target may leave the sector.  Pass NULL arrays to get counts. */
+int qkrylov_opsum_compile(qkrylov_basis_h basis, qkrylov_site_h site, qkrylov_opsum_h opsum, int* n_terms,
+                          int* n_groups, int* has_diag, int* all_real, uint64_t* mask, double* coef,
+                          uint64_t* flip, uint32_t* first, uint32_t* count, uint32_t* check);
+
+/* ------------------------------------------------------------ Hamiltonian
+ * qkrylov_hamiltonian_create (c_api.h:81-83) with a precision (32: complex
+ * float vectors as the reference C ABI, 64: complex double as the
+ * reference's fp64 C++ API) and a CUDA device ordinal. */
+qkrylov_hamiltonian_h qkrylov_hamiltonian_create_ex(qkrylov_basis_h basis, qkrylov_site_h site,
+                                                   qkrylov_opsum_h opsum, int precision, int device);
+int qkrylov_hamiltonian_precision(qkrylov_hamiltonian_h h);
+int qkrylov_hamiltonian_all_real(qkrylov_hamiltonian_h h);
+uint64_t qkrylov_hamiltonian_device_bytes(qkrylov_hamiltonian_h h);
+/* The CUDA stream (cudaStream_t) the library uses on the handle's device. */
+void* qkrylov_hamiltonian_stream(qkrylov_hamiltonian_h h);
+
+/* qkrylov_hamiltonian_apply_complex / _diagonal (c_api.h:94-100) on
+ * double host arrays (64-bit Hamiltonians). */
+int qkrylov_hamiltonian_apply_complex_f64(qkrylov_hamiltonian_h h, const double* x_complex, double* y_complex);
+int qkrylov_hamiltonian_diagonal_complex_f64(qkrylov_hamiltonian_h h, double* diag_complex_out);
+
+/* y = H x on device pointers of `dtype` (any precision handle; real dtypes
+ * need a real operator), issued on `stream` (NULL: the library stream)
+ * without synchronising.  MatrixFreeHamiltonian::apply(VectorView, VectorView)
+ * (matrix_free_hamiltonian.hpp:38) as a C entry point. */
+int qkrylov_hamiltonian_apply_device(qkrylov_hamiltonian_h h, int dtype, const void* x, void* y, void* stream);
+int qkrylov_hamiltonian_diagonal_device(qkrylov_hamiltonian_h h, int dtype, void* diag, void* stream);
+
+/* -------------------------------------------------- double-precision solvers */
+typedef struct {
+  double energy;
+  int iterations;
+  int converged;
+  int n_alpha;
+  int n_beta;
+} qkrylov_lanczos_result_f64_t;
+
+/* lanczos_ground_state (lanczos.hpp:20-25).  start_complex: NULL for the
+ * reference start vector, else dimension() complex doubles.  alphas and
+ * betas (maxiter doubles each, may be NULL) receive the tridiagonal. */
+int qkrylov_lanczos_ground_state_f64(qkrylov_hamiltonian_h h, int maxiter, double tol, const double* start_complex,
+                                     qkrylov_lanczos_result_f64_t* result, double* eigenvector_complex,
+                                     double* alphas, double* betas);
+/* davidson_lowest (davidson.hpp:21-27) */
+int qkrylov_davidson_lowest_f64(qkrylov_hamiltonian_h h, int n_eig, int max_subspace, double tol,
+                                double* eigenvalues_out, double* eigenvectors_complex_out,
+                                qkrylov_davidson_result_c_t* result_info);
+/* continued_fraction_coeffs (dynamics.hpp:21-25) */
+int qkrylov_continued_fraction_coeffs_f64(qkrylov_hamiltonian_h h, const double* phi0_complex, int n_iter,
+                                          double* alphas_out, double* betas_out, double* norm_phi0_out,
+                                          int* n_alpha_out, int* n_beta_out);
+/* evaluate_spectral_function (dynamics.hpp:28-38); betas has n-1 entries */
+double qkrylov_evaluate_spectral_function_f64(const double* alphas, const double* betas, size_t n,
+                                              double norm_phi0, double omega, double E0, double eta);
+/* ftlm (ftlm.hpp:21-27) at n_beta inverse temperatures from one set of
+ * random-vector tridiagonals; entry q equals ftlm(h, betas[q], ...). */
+int qkrylov_ftlm_sweep_f64(qkrylov_hamiltonian_h h, int n_beta, const double* betas, int n_random, int n_steps,
+                           double* Z_out, double* U_out, double* Cv_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QKRYLOV_B200_H */

@@ -1,0 +1,587 @@
+"""qkrylov_b200: qkrylov's matrix-free H.x and Krylov solvers on NVIDIA B200.
+
+Python mirror of qkrylov's Python API (bindings/python/qkrylov/*.py: same
+class and function names, argument meaning and errors) over this project's
+C ABI, libqkrylov_b200.so (include/qkrylov_c_api.h, include/qkrylov_b200.h).
+All numerical work runs in the CUDA library; this module only marshals
+arguments.  ``dtype=np.float64`` selects the double-precision path (the
+reference's fp64 C++ namespace), ``np.float32`` the single-precision one
+(the reference's C ABI and default Python dtype).
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+from typing import List, Optional, Sequence, Tuple, Union
+
+import numpy as np
+
+from ._lib import lib, LibraryError  # noqa: F401
+
+__all__ = [
+    "Op", "OpSum", "Sz", "Sp", "Sm", "Sx", "Sy", "CdagUp", "CUp", "CdagDn", "CDn", "Nup", "Ndn", "Nupdn",
+    "Bdag", "B", "N", "Site", "SpinHalfSite", "FermionSite", "HubbardSite", "TJSite", "Basis", "SpinHalfBasis",
+    "FermionBasis", "HubbardBasis", "TJBasis", "MatrixFreeHamiltonian", "LanczosResult", "lanczos_ground_state",
+    "DavidsonResult", "davidson_lowest", "DynamicsResult", "continued_fraction_coeffs",
+    "evaluate_spectral_function", "FTLMResult", "ftlm", "ftlm_sweep", "find_gpu", "gpu_count",
+]
+
+DTYPE_C128, DTYPE_C64, DTYPE_F64, DTYPE_F32 = 0, 1, 2, 3
+
+
+def _check(rc, what):
+    if rc == -1:
+        raise ValueError(f"{what}: invalid argument ({lib().qkrylov_b200_last_error().decode()})")
+    if rc != 0:
+        raise RuntimeError(f"{what}: {lib().qkrylov_b200_last_error().decode()}")
+
+
+# ----------------------------------------------------------------- operators
+class Op(str, enum.Enum):
+    Sz = "Sz"; Sp = "Sp"; Sm = "Sm"; Sx = "Sx"; Sy = "Sy"
+    CdagUp = "CdagUp"; CUp = "CUp"; CdagDn = "CdagDn"; CDn = "CDn"
+    Nup = "Nup"; Ndn = "Ndn"; Nupdn = "Nupdn"; Bdag = "Bdag"; B = "B"; N = "N"
+
+
+class LocalOpExpr:
+    def __init__(self, name: str, site: int):
+        self.name, self.site = name, site
+
+    def __mul__(self, other):
+        if isinstance(other, LocalOpExpr):
+            return TermExpr(1.0, [self, other])
+        if isinstance(other, (int, float, complex)):
+            return TermExpr(complex(other), [self])
+        return NotImplemented
+
+    def __rmul__(self, other):
+        if isinstance(other, (int, float, complex)):
+            return TermExpr(complex(other), [self])
+        return NotImplemented
+
+
+class TermExpr:
+    def __init__(self, coeff, ops):
+        self.coeff, self.ops = coeff, ops
+
+    def __mul__(self, other):
+        if isinstance(other, LocalOpExpr):
+            return TermExpr(self.coeff, self.ops + [other])
+        if isinstance(other, TermExpr):
+            return TermExpr(self.coeff * other.coeff, self.ops + other.ops)
+        if isinstance(other, (int, float, complex)):
+            return TermExpr(self.coeff * complex(other), self.ops)
+        return NotImplemented
+
+    def __rmul__(self, other):
+        if isinstance(other, (int, float, complex)):
+            return TermExpr(self.coeff * complex(other), self.ops)
+        return NotImplemented
+
+    def __add__(self, other):
+        if isinstance(other, TermExpr):
+            return OpSumExpr([self, other])
+        if isinstance(other, OpSumExpr):
+            return OpSumExpr([self] + other.terms)
+        return NotImplemented
+
+    def __sub__(self, other):
+        if isinstance(other, TermExpr):
+            return OpSumExpr([self, TermExpr(-other.coeff, other.ops)])
+        return NotImplemented
+
+
+class OpSumExpr:
+    def __init__(self, terms):
+        self.terms = terms
+
+    def __add__(self, other):
+        if isinstance(other, TermExpr):
+            return OpSumExpr(self.terms + [other])
+        if isinstance(other, OpSumExpr):
+            return OpSumExpr(self.terms + other.terms)
+        return NotImplemented
+
+    def __mul__(self, other):
+        if isinstance(other, (int, float, complex)):
+            return OpSumExpr([t * other for t in self.terms])
+        return NotImplemented
+
+    __rmul__ = __mul__
+
+    def __sub__(self, other):
+        if isinstance(other, TermExpr):
+            return OpSumExpr(self.terms + [TermExpr(-other.coeff, other.ops)])
+        if isinstance(other, OpSumExpr):
+            return OpSumExpr(self.terms + [TermExpr(-t.coeff, t.ops) for t in other.terms])
+        return NotImplemented
+
+
+def Sz(i): return LocalOpExpr("Sz", i)
+def Sp(i): return LocalOpExpr("Sp", i)
+def Sm(i): return LocalOpExpr("Sm", i)
+def Sx(i): return LocalOpExpr("Sx", i)
+def Sy(i): return LocalOpExpr("Sy", i)
+def CdagUp(i): return LocalOpExpr("CdagUp", i)
+def CUp(i): return LocalOpExpr("CUp", i)
+def CdagDn(i): return LocalOpExpr("CdagDn", i)
+def CDn(i): return LocalOpExpr("CDn", i)
+def Nup(i): return LocalOpExpr("Nup", i)
+def Ndn(i): return LocalOpExpr("Ndn", i)
+def Nupdn(i): return LocalOpExpr("Nupdn", i)
+def Bdag(i): return LocalOpExpr("Bdag", i)
+def B(i): return LocalOpExpr("B", i)
+def N(i): return LocalOpExpr("N", i)
+
+
+class OpSum:
+    """Ordered list of terms (coeff, [(op, site), ...]); factors act in list order."""
+
+    def __init__(self, dtype=np.float32):
+        self.dtype = dtype
+        self.terms: List[Tuple[complex, List[Tuple[str, int]]]] = []
+
+    def add_term(self, coeff: complex, *ops: Union[str, Op, int]):
+        if len(ops) % 2 != 0:
+            raise ValueError("Operators must be provided in (name, site) pairs.")
+        factors = []
+        for i in range(0, len(ops), 2):
+            name = ops[i].value if isinstance(ops[i], Op) else str(ops[i])
+            factors.append((name, int(ops[i + 1])))
+        if not factors:
+            raise ValueError("Term must be a tuple of (coeff, op1, site1, ...)")
+        self.terms.append((complex(coeff), factors))
+
+    def __iadd__(self, term):
+        if isinstance(term, tuple):
+            if len(term) < 3 or len(term) % 2 == 0:
+                raise ValueError("Term must be a tuple of (coeff, op1, site1, ...)")
+            self.add_term(term[0], *term[1:])
+        elif isinstance(term, TermExpr):
+            self.terms.append((complex(term.coeff), [(o.name, o.site) for o in term.ops]))
+        elif isinstance(term, OpSumExpr):
+            for t in term.terms:
+                self.__iadd__(t)
+        else:
+            raise ValueError("Unsupported type for += on OpSum")
+        return self
+
+    def clear(self):
+        self.terms.clear()
+
+    @property
+    def size(self) -> int:
+        return len(self.terms)
+
+    def _handle(self):
+        L = lib()
+        h = L.qkrylov_opsum_create()
+        for c, f in self.terms:
+            names = (ctypes.c_char_p * len(f))(*[n.encode() for n, _ in f])
+            sites = (ctypes.c_int * len(f))(*[s for _, s in f])
+            if self.dtype == np.float32:
+                c = complex(np.float32(c.real), np.float32(c.imag))  # the reference's float coefficients
+            _check(L.qkrylov_opsum_add_term_nbody_f64(h, c.real, c.imag, len(f), names, sites), "OpSum")
+        return h
+
+    def __repr__(self):
+        return f"OpSum(terms={self.size})"
+
+
+# --------------------------------------------------------------------- sites
+class Site:
+    family = -1
+
+    def __init__(self, dtype=np.float32):
+        self.dtype = dtype
+
+    def _handle(self):
+        L = lib()
+        return {0: L.qkrylov_spinhalf_site_create, 1: L.qkrylov_fermion_site_create,
+                2: L.qkrylov_hubbard_site_create, 3: L.qkrylov_tj_site_create}[self.family]()
+
+
+class SpinHalfSite(Site):
+    """Spin-1/2 site: Sz, Sp, Sm, Sx, Sy."""
+    family = 0
+
+
+class FermionSite(Site):
+    """Spinless fermion mode: N, Id, C, Cdag."""
+    family = 1
+
+
+class HubbardSite(Site):
+    """Hubbard site: Nup, Ndn, Nupdn, CUp, CdagUp, CDn, CdagDn."""
+    family = 2
+
+
+class TJSite(Site):
+    """t-J site: as Hubbard without double occupancy (no Nupdn)."""
+    family = 3
+
+
+# --------------------------------------------------------------------- bases
+class Basis:
+    family = -1
+
+    def __init__(self, N: int, sector: Optional[dict] = None, dtype=np.float32):
+        self._N, self._sector, self.dtype = N, dict(sector or {}), dtype
+        L = lib()
+        sec = L.qkrylov_sector_create()
+        try:
+            s = self._sector
+            if s.get("use_sz"):
+                _check(L.qkrylov_sector_set_sz(sec, int(s.get("sz2", 0))), "sector")
+            if s.get("use_n"):
+                _check(L.qkrylov_sector_set_n(sec, int(s.get("n", 0))), "sector")
+            self._h = self._create(L, N, sec)
+        finally:
+            L.qkrylov_sector_destroy(sec)
+        if not self._h:
+            raise RuntimeError(L.qkrylov_b200_last_error().decode())
+
+    def _create(self, L, N, sec):
+        raise NotImplementedError
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().qkrylov_basis_destroy(h)
+            self._h = None
+
+    @property
+    def size(self) -> int:
+        return int(lib().qkrylov_basis_dimension(self._h))
+
+    @property
+    def nsites(self) -> int:
+        return self._N
+
+    def states(self, first: int = 0, count: Optional[int] = None) -> np.ndarray:
+        count = self.size - first if count is None else count
+        out = np.zeros(count, dtype=np.uint64)
+        _check(lib().qkrylov_basis_states(self._h, first, count, out.ctypes.data), "basis states")
+        return out
+
+    def state(self, i: int) -> int:
+        if i < 0 or i >= self.size:
+            raise IndexError("basis index out of range")
+        return int(lib().qkrylov_basis_state(self._h, i))
+
+    def index(self, s: int) -> int:
+        r = int(lib().qkrylov_basis_index(self._h, s))
+        if r < 0:
+            raise KeyError("State not present in basis")
+        return r
+
+    def contains(self, s: int) -> bool:
+        return bool(lib().qkrylov_basis_contains(self._h, s))
+
+    def index_many(self, states) -> np.ndarray:
+        s = np.ascontiguousarray(states, dtype=np.uint64)
+        out = np.zeros(s.size, dtype=np.int64)
+        _check(lib().qkrylov_basis_index_many(self._h, s.ctypes.data, s.size, out.ctypes.data), "index")
+        return out
+
+
+class SpinHalfBasis(Basis):
+    """Spin-1/2 chain; ``sz`` (total Sz) selects a sector as in qkrylov."""
+    family = 0
+
+    def __init__(self, N: int, conserve_sz: bool = False, sz: Optional[float] = None, dtype=np.float32):
+        if sz is not None:
+            conserve_sz = True
+        else:
+            sz = 0
+        sec = {"use_sz": True, "sz2": int(2 * sz)} if conserve_sz else {}
+        self._conserve_sz, self._sz = conserve_sz, sz
+        super().__init__(N, sec, dtype)
+
+    def _create(self, L, N, sec):
+        return L.qkrylov_spinhalf_basis_create(N, sec)
+
+    def __repr__(self):
+        return f"SpinHalfBasis(N={self.nsites}, dim={self.size}" + (f", sz={self._sz})" if self._conserve_sz else ")")
+
+
+class FermionBasis(Basis):
+    family = 1
+
+    def __init__(self, N: int, conserve_n: bool = False, n: int = 0, dtype=np.float32):
+        if n != 0:
+            conserve_n = True
+        super().__init__(N, {"use_n": True, "n": n} if conserve_n else {}, dtype)
+
+    def _create(self, L, N, sec):
+        return L.qkrylov_fermion_basis_create(N, sec)
+
+
+class _PairBasis(Basis):
+    def __init__(self, N, conserve_nup=False, nup=0, conserve_ndn=False, ndn=0, dtype=np.float32):
+        if nup != 0:
+            conserve_nup = True
+        if ndn != 0:
+            conserve_ndn = True
+        self._pairs = (conserve_nup, nup, conserve_ndn, ndn)
+        super().__init__(N, {}, dtype)
+
+    def _create(self, L, N, sec):
+        cu, nu, cd, nd = self._pairs
+        # The C ABI sets both counts together (c_api.cpp:80-91); a single
+        # conserved species goes through the extended sector setters.
+        if cu or cd:
+            _check(L.qkrylov_sector_set_hubbard_particles(sec, nu, nd), "sector")
+            if not (cu and cd):
+                _check(L.qkrylov_b200_sector_set_species(sec, int(cu), int(cd)), "sector")
+        return self._ctor(L)(N, sec)
+
+
+class HubbardBasis(_PairBasis):
+    family = 2
+
+    def _ctor(self, L):
+        return L.qkrylov_hubbard_basis_create
+
+
+class TJBasis(_PairBasis):
+    family = 3
+
+    def _ctor(self, L):
+        return L.qkrylov_tj_basis_create
+
+
+# --------------------------------------------------------------- Hamiltonian
+class MatrixFreeHamiltonian:
+    """y = H x generated on the fly on the GPU from (basis, site, ops)."""
+
+    def __init__(self, basis: Basis, site: Site, ops: OpSum, device: str = "cuda", dtype=np.float32):
+        self.basis, self.site, self.ops, self.device, self.dtype = basis, site, ops, device, dtype
+        dev = device.lower()
+        if dev == "cpu":
+            raise ValueError("qkrylov_b200 has no CPU back-end; use device='cuda'")
+        dev_id = int(dev.split(":")[1]) if ":" in dev else 0
+        L = lib()
+        sh, oh = site._handle(), ops._handle()
+        try:
+            self._h = L.qkrylov_hamiltonian_create_ex(basis._h, sh, oh, 64 if dtype == np.float64 else 32, dev_id)
+        finally:
+            L.qkrylov_site_destroy(sh)
+            L.qkrylov_opsum_destroy(oh)
+        if not self._h:
+            raise RuntimeError(L.qkrylov_b200_last_error().decode())
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().qkrylov_hamiltonian_destroy(h)
+            self._h = None
+
+    @property
+    def dimension(self) -> int:
+        return int(lib().qkrylov_hamiltonian_dimension(self._h))
+
+    @property
+    def cdtype(self):
+        return np.complex128 if self.dtype == np.float64 else np.complex64
+
+    @property
+    def all_real(self) -> bool:
+        return bool(lib().qkrylov_hamiltonian_all_real(self._h))
+
+    def apply(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=self.cdtype)
+        if x.shape != (self.dimension,):
+            raise ValueError("Input array size does not match Hamiltonian dimension")
+        y = np.zeros_like(x)
+        if self.dtype == np.float64:
+            _check(lib().qkrylov_hamiltonian_apply_complex_f64(self._h, x.ctypes.data, y.ctypes.data), "apply")
+        else:
+            _check(lib().qkrylov_hamiltonian_apply_complex(self._h, x.ctypes.data, y.ctypes.data), "apply")
+        return y
+
+    __matmul__ = apply
+
+    def diagonal(self) -> np.ndarray:
+        d = np.zeros(self.dimension, dtype=np.complex128)
+        _check(lib().qkrylov_hamiltonian_diagonal_complex_f64(self._h, d.ctypes.data), "diagonal")
+        return d.astype(self.cdtype)
+
+    def apply_device(self, x_ptr: int, y_ptr: int, dtype: int, stream: int = 0):
+        """y = H x on device pointers (e.g. torch ``tensor.data_ptr()``), no sync."""
+        _check(lib().qkrylov_hamiltonian_apply_device(self._h, dtype, ctypes.c_void_p(x_ptr),
+                                                      ctypes.c_void_p(y_ptr), ctypes.c_void_p(stream or None)),
+               "apply_device")
+
+    @property
+    def stream(self) -> int:
+        return int(lib().qkrylov_hamiltonian_stream(self._h) or 0)
+
+    def __repr__(self):
+        return f"MatrixFreeHamiltonian(dim={self.dimension})"
+
+
+# ------------------------------------------------------------------- solvers
+class LanczosResult:
+    def __init__(self, energy, eigenvector, iterations=0, converged=False, alphas=None, betas=None):
+        self.energy, self.eigenvector = energy, eigenvector
+        self.iterations, self.converged = iterations, converged
+        self.alphas = np.zeros(0) if alphas is None else alphas
+        self.betas = np.zeros(0) if betas is None else betas
+
+    def __repr__(self):
+        return f"LanczosResult(energy={self.energy:.10f})"
+
+
+def lanczos_ground_state(H: MatrixFreeHamiltonian, maxiter: int = 200, tol: float = 1e-12,
+                         start: Optional[np.ndarray] = None) -> LanczosResult:
+    L = lib()
+    dim = H.dimension
+    if H.dtype == np.float64:
+        res = _LanczosF64()
+        ev = np.zeros(dim, dtype=np.complex128)
+        a, b = np.zeros(max(maxiter, 1)), np.zeros(max(maxiter, 1))
+        st = None if start is None else np.ascontiguousarray(start, dtype=np.complex128)
+        _check(L.qkrylov_lanczos_ground_state_f64(H._h, maxiter, tol, st.ctypes.data if st is not None else None,
+                                                  ctypes.byref(res), ev.ctypes.data, a.ctypes.data, b.ctypes.data),
+               "lanczos_ground_state")
+        return LanczosResult(res.energy, ev, res.iterations, bool(res.converged), a[:res.n_alpha].copy(),
+                             b[:res.n_beta].copy())
+    if start is not None:
+        raise ValueError("a start vector needs dtype=np.float64")
+    res = _LanczosC()
+    ev = np.zeros(dim, dtype=np.complex64)
+    _check(L.qkrylov_lanczos_ground_state_complex(H._h, maxiter, ctypes.c_float(tol), ctypes.byref(res),
+                                                  ev.ctypes.data), "lanczos_ground_state")
+    return LanczosResult(float(res.energy), ev, res.iterations, bool(res.converged))
+
+
+class DavidsonResult:
+    def __init__(self, eigenvalues, eigenvectors, iterations=0, converged=False):
+        self.eigenvalues, self.eigenvectors = eigenvalues, eigenvectors
+        self.iterations, self.converged = iterations, converged
+
+    def __repr__(self):
+        return f"DavidsonResult(energies={self.eigenvalues})"
+
+
+def davidson_lowest(H: MatrixFreeHamiltonian, n_eig: int = 1, max_subspace: int = 20,
+                    tol: float = 1e-8) -> DavidsonResult:
+    L = lib()
+    dim = H.dimension
+    k = max(1, min(n_eig, dim))
+    info = _DavidsonInfo()
+    if H.dtype == np.float64:
+        ev, vec = np.zeros(k), np.zeros((k, dim), dtype=np.complex128)
+        _check(L.qkrylov_davidson_lowest_f64(H._h, n_eig, max_subspace, tol, ev.ctypes.data, vec.ctypes.data,
+                                             ctypes.byref(info)), "davidson_lowest")
+    else:
+        ev, vec = np.zeros(k, dtype=np.float32), np.zeros((k, dim), dtype=np.complex64)
+        _check(L.qkrylov_davidson_lowest_complex(H._h, n_eig, max_subspace, ctypes.c_float(tol), ev.ctypes.data,
+                                                 vec.ctypes.data, ctypes.byref(info)), "davidson_lowest")
+    return DavidsonResult(ev.astype(float), list(vec), info.iterations, bool(info.converged))
+
+
+class DynamicsResult:
+    def __init__(self, alphas, betas, norm_phi0):
+        self.alphas, self.betas, self.norm_phi0 = np.asarray(alphas), np.asarray(betas), norm_phi0
+
+
+def continued_fraction_coeffs(H: MatrixFreeHamiltonian, phi0: np.ndarray, n_iter: int = 100) -> DynamicsResult:
+    L = lib()
+    phi0 = np.ascontiguousarray(phi0, dtype=H.cdtype)
+    if phi0.shape != (H.dimension,):
+        raise ValueError("phi0 vector size does not match Hamiltonian dimension")
+    if H.dtype == np.float64:
+        a, b = np.zeros(n_iter), np.zeros(n_iter)
+        nrm, na, nb = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        _check(L.qkrylov_continued_fraction_coeffs_f64(H._h, phi0.ctypes.data, n_iter, a.ctypes.data, b.ctypes.data,
+                                                       ctypes.byref(nrm), ctypes.byref(na), ctypes.byref(nb)),
+               "continued_fraction_coeffs")
+        return DynamicsResult(a[:na.value].copy(), b[:nb.value].copy(), nrm.value)
+    a, b = np.zeros(n_iter, np.float32), np.zeros(n_iter, np.float32)
+    nrm, nc = ctypes.c_float(), ctypes.c_int()
+    _check(L.qkrylov_continued_fraction_coeffs_complex(H._h, phi0.ctypes.data, n_iter, a.ctypes.data, b.ctypes.data,
+                                                       ctypes.byref(nrm), ctypes.byref(nc)),
+           "continued_fraction_coeffs")
+    n = nc.value
+    return DynamicsResult(a[:n].copy(), b[:max(n - 1, 0)].copy(), nrm.value)
+
+
+def evaluate_spectral_function(res: DynamicsResult, omega: float, E0: float, eta: float = 0.1) -> float:
+    a = np.ascontiguousarray(res.alphas, dtype=np.float64)
+    b = np.ascontiguousarray(res.betas, dtype=np.float64)
+    if len(a) == 0:
+        return 0.0
+    return lib().qkrylov_evaluate_spectral_function_f64(a.ctypes.data, b.ctypes.data if len(b) else None, len(a),
+                                                        res.norm_phi0, omega, E0, eta)
+
+
+class FTLMResult:
+    def __init__(self, beta, Z, U, Cv):
+        self.beta, self.partition_function, self.internal_energy, self.specific_heat = beta, Z, U, Cv
+
+
+def ftlm_sweep(H: MatrixFreeHamiltonian, betas: Sequence[float], n_random: int = 50, n_steps: int = 100):
+    b = np.ascontiguousarray(betas, dtype=np.float64)
+    Z, U, C = np.zeros(len(b)), np.zeros(len(b)), np.zeros(len(b))
+    _check(lib().qkrylov_ftlm_sweep_f64(H._h, len(b), b.ctypes.data, n_random, n_steps, Z.ctypes.data,
+                                        U.ctypes.data, C.ctypes.data), "ftlm")
+    return [FTLMResult(float(b[q]), Z[q], U[q], C[q]) for q in range(len(b))]
+
+
+def ftlm(H: MatrixFreeHamiltonian, beta: float, n_random: int = 50, n_steps: int = 100) -> FTLMResult:
+    if H.dtype == np.float64:
+        return ftlm_sweep(H, [beta], n_random, n_steps)[0]
+    r = _FTLMC()
+    _check(lib().qkrylov_ftlm(H._h, ctypes.c_float(beta), n_random, n_steps, ctypes.byref(r)), "ftlm")
+    return FTLMResult(r.beta, r.partition_function, r.internal_energy, r.specific_heat)
+
+
+def find_gpu():
+    return "cuda" if gpu_count() > 0 else None
+
+
+def gpu_count() -> int:
+    return int(lib().qkrylov_b200_device_count())
+
+
+def compile_info(basis: Basis, site: Site, ops: OpSum) -> dict:
+    """The OpSum compiler's bit-mask tables for (basis, site, ops), no GPU needed."""
+    L = lib()
+    sh, oh = site._handle(), ops._handle()
+    try:
+        nt, ng, hd, ar = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(L.qkrylov_opsum_compile(basis._h, sh, oh, ctypes.byref(nt), ctypes.byref(ng), ctypes.byref(hd),
+                                       ctypes.byref(ar), None, None, None, None, None, None), "compile")
+        mask = np.zeros((nt.value, 3), np.uint64)
+        coef = np.zeros(nt.value, np.complex128)
+        flip = np.zeros(ng.value, np.uint64)
+        first, count, check = (np.zeros(ng.value, np.uint32) for _ in range(3))
+        _check(L.qkrylov_opsum_compile(basis._h, sh, oh, None, None, None, None, mask.ctypes.data, coef.ctypes.data,
+                                       flip.ctypes.data, first.ctypes.data, count.ctypes.data, check.ctypes.data),
+               "compile")
+        return dict(mask=mask, coef=coef, flip=flip, first=first, count=count, check=check,
+                    has_diag=bool(hd.value), all_real=bool(ar.value))
+    finally:
+        L.qkrylov_site_destroy(sh)
+        L.qkrylov_opsum_destroy(oh)
+
+
+class _LanczosF64(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("iterations", ctypes.c_int), ("converged", ctypes.c_int),
+                ("n_alpha", ctypes.c_int), ("n_beta", ctypes.c_int)]
+
+
+class _LanczosC(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_float), ("iterations", ctypes.c_int), ("converged", ctypes.c_int)]
+
+
+class _DavidsonInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int)]
+
+
+class _FTLMC(ctypes.Structure):
+    _fields_ = [("beta", ctypes.c_float), ("partition_function", ctypes.c_float),
+                ("internal_energy", ctypes.c_float), ("specific_heat", ctypes.c_float)]

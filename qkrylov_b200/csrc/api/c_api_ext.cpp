@@ -1,0 +1,263 @@
+// Extended C ABI (include/qkrylov_b200.h): double precision, device
+// pointers, multi-temperature FTLM, compiler inspection, diagnostics.
+#include <cstring>
+#include <exception>
+
+#include "api/handles.hpp"
+#include "engine/solvers.hpp"
+#include "qkrylov_b200.h"
+
+namespace qkapi {
+const char* last_error();
+}
+
+namespace {
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::exception& e) {
+    qkapi::set_error(e.what());
+    return QKRYLOV_ERROR_EXCEPTION;
+  } catch (...) {
+    qkapi::set_error("unknown exception");
+    return QKRYLOV_ERROR_EXCEPTION;
+  }
+}
+bool valid_dtype(int t) { return t >= QKRYLOV_DTYPE_C128 && t <= QKRYLOV_DTYPE_F32; }
+}  // namespace
+
+extern "C" {
+
+const char* qkrylov_b200_last_error(void) { return qkapi::last_error(); }
+uint64_t qkrylov_b200_launch_count(void) { return qkd_launch_count(); }
+int qkrylov_b200_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) { (void)cudaGetLastError(); return 0; }
+  return n;
+}
+
+int qkrylov_b200_sector_set_species(qkrylov_sector_h sector, int use_nup, int use_ndn) {
+  if (!sector) return QKRYLOV_ERROR_INVALID_ARG;
+  sector->s.use_nup = use_nup != 0;
+  sector->s.use_ndn = use_ndn != 0;
+  return QKRYLOV_SUCCESS;
+}
+
+int qkrylov_b200_site_apply(qkrylov_site_h site, const char* op, int site_index, uint64_t state, int* valid,
+                            uint64_t* new_state, double* me) {
+  if (!site || !op || !valid || !new_state || !me) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const auto a = qkb::apply_factor(site->family, op, site_index, state);
+    *valid = a.valid;
+    *new_state = a.new_state;
+    me[0] = a.me.real();
+    me[1] = a.me.imag();
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_basis_states(qkrylov_basis_h basis, uint64_t first, uint64_t count, uint64_t* out) {
+  if (!basis || !basis->table || (count && !out)) return QKRYLOV_ERROR_INVALID_ARG;
+  if (first > basis->table->dim || count > basis->table->dim - first) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    for (uint64_t i = 0; i < count; ++i) out[i] = basis->table->state(first + i);
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_basis_index_many(qkrylov_basis_h basis, const uint64_t* states, uint64_t n, int64_t* out) {
+  if (!basis || !basis->table || (n && (!states || !out))) return QKRYLOV_ERROR_INVALID_ARG;
+  for (uint64_t i = 0; i < n; ++i) out[i] = basis->table->index(states[i]);
+  return QKRYLOV_SUCCESS;
+}
+
+int qkrylov_opsum_add_term_nbody_f64(qkrylov_opsum_h opsum, double cr, double ci, int n, const char** ops,
+                                     const int* sites) {
+  if (!opsum || !ops || !sites || n <= 0) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    qkb::TermIn t;
+    t.coeff = {cr, ci};
+    for (int i = 0; i < n; ++i) {
+      if (!ops[i]) return QKRYLOV_ERROR_INVALID_ARG;
+      t.factors.push_back({std::string(ops[i]), sites[i]});
+    }
+    opsum->terms.push_back(std::move(t));
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+uint64_t qkrylov_opsum_size(qkrylov_opsum_h opsum) { return opsum ? opsum->terms.size() : 0; }
+
+int qkrylov_opsum_compile(qkrylov_basis_h basis, qkrylov_site_h site, qkrylov_opsum_h opsum, int* n_terms,
+                          int* n_groups, int* has_diag, int* all_real, uint64_t* mask, double* coef,
+                          uint64_t* flip, uint32_t* first, uint32_t* count, uint32_t* check) {
+  if (!basis || !basis->table || !site || !opsum) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const auto op = qkb::compile_opsum(site->family, *basis->table, opsum->terms);
+    if (n_terms) *n_terms = int(op.terms.size());
+    if (n_groups) *n_groups = int(op.groups.size());
+    if (has_diag) *has_diag = op.has_diag;
+    if (all_real) *all_real = op.all_real;
+    for (size_t t = 0; t < op.terms.size(); ++t) {
+      if (mask) { mask[3 * t] = op.terms[t].cmask; mask[3 * t + 1] = op.terms[t].cval; mask[3 * t + 2] = op.terms[t].smask; }
+      if (coef) { coef[2 * t] = op.terms[t].wre; coef[2 * t + 1] = op.terms[t].wim; }
+    }
+    for (size_t g = 0; g < op.groups.size(); ++g) {
+      if (flip) flip[g] = op.groups[g].flip;
+      if (first) first[g] = op.groups[g].first;
+      if (count) count[g] = op.groups[g].count;
+      if (check) check[g] = op.groups[g].check;
+    }
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+qkrylov_hamiltonian_h qkrylov_hamiltonian_create_ex(qkrylov_basis_h basis, qkrylov_site_h site,
+                                                   qkrylov_opsum_h opsum, int precision, int device) {
+  if (!basis || !basis->table || !site || !opsum || (precision != 32 && precision != 64) || device < 0) {
+    qkapi::set_error("invalid argument");
+    return nullptr;
+  }
+  try {
+    auto h = std::make_unique<qkrylov_hamiltonian_t>();
+    h->op = std::make_shared<qkb::Operator>(site->family, basis->table, opsum->terms, device);
+    h->precision = precision;
+    return h.release();
+  } catch (const std::exception& e) {
+    qkapi::set_error(e.what());
+    return nullptr;
+  }
+}
+
+int qkrylov_hamiltonian_precision(qkrylov_hamiltonian_h h) { return (h && h->op) ? h->precision : 0; }
+int qkrylov_hamiltonian_all_real(qkrylov_hamiltonian_h h) { return (h && h->op) ? int(h->op->all_real()) : 0; }
+uint64_t qkrylov_hamiltonian_device_bytes(qkrylov_hamiltonian_h h) {
+  return (h && h->op) ? qkd_plan_device_bytes(h->op->plan()) : 0;
+}
+void* qkrylov_hamiltonian_stream(qkrylov_hamiltonian_h h) {
+  if (!h || !h->op) return nullptr;
+  try { return h->op->ctx().stream; } catch (...) { return nullptr; }
+}
+
+int qkrylov_hamiltonian_apply_complex_f64(qkrylov_hamiltonian_h h, const double* x, double* y) {
+  if (!h || !h->op || !x || !y) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const uint64_t dim = h->op->dim();
+    if (dim == 0) return QKRYLOV_SUCCESS;
+    auto& c = h->op->ctx();
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->stage(QK_C128);
+    qkb::cuda_check(cudaMemcpyAsync(h->sx.data(), x, dim * 16, cudaMemcpyHostToDevice, c.stream), "H2D");
+    h->op->apply(QK_C128, h->sx.data(), h->sy.data());
+    qkb::cuda_check(cudaMemcpyAsync(y, h->sy.data(), dim * 16, cudaMemcpyDeviceToHost, c.stream), "D2H");
+    c.sync();
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_hamiltonian_diagonal_complex_f64(qkrylov_hamiltonian_h h, double* d) {
+  if (!h || !h->op || !d) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const uint64_t dim = h->op->dim();
+    if (dim == 0) return QKRYLOV_SUCCESS;
+    auto& c = h->op->ctx();
+    qkb::DevVec dd(dim, QK_C128, h->op->device(), false);
+    h->op->diagonal(QK_C128, dd.data());
+    qkb::cuda_check(cudaMemcpyAsync(d, dd.data(), dim * 16, cudaMemcpyDeviceToHost, c.stream), "D2H");
+    c.sync();
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_hamiltonian_apply_device(qkrylov_hamiltonian_h h, int dtype, const void* x, void* y, void* stream) {
+  if (!h || !h->op || !x || !y || !valid_dtype(dtype)) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    auto& c = h->op->ctx();
+    const int rc = qkd_apply(h->op->plan(), qk_dtype(dtype), x, y, stream ? cudaStream_t(stream) : c.stream);
+    if (rc == QKD_EINVAL) { qkapi::set_error("invalid dtype for this operator or aliased x/y"); return QKRYLOV_ERROR_INVALID_ARG; }
+    qkb::qkd_check(rc, "H.x");
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_hamiltonian_diagonal_device(qkrylov_hamiltonian_h h, int dtype, void* d, void* stream) {
+  if (!h || !h->op || !d || !valid_dtype(dtype)) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    auto& c = h->op->ctx();
+    const int rc = qkd_diagonal(h->op->plan(), qk_dtype(dtype), d, stream ? cudaStream_t(stream) : c.stream);
+    if (rc == QKD_EINVAL) return QKRYLOV_ERROR_INVALID_ARG;
+    qkb::qkd_check(rc, "diagonal");
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_lanczos_ground_state_f64(qkrylov_hamiltonian_h h, int maxiter, double tol, const double* start,
+                                     qkrylov_lanczos_result_f64_t* result, double* evec, double* alphas,
+                                     double* betas) {
+  if (!h || !h->op || !result) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    std::vector<std::complex<double>> ritz;
+    auto r = qkb::lanczos<double>(*h->op, maxiter, tol, reinterpret_cast<const std::complex<double>*>(start),
+                                  evec ? &ritz : nullptr);
+    result->energy = r.energy;
+    result->iterations = r.iterations;
+    result->converged = r.converged;
+    result->n_alpha = int(r.alphas.size());
+    result->n_beta = int(r.betas.size());
+    if (evec && !ritz.empty()) std::memcpy(evec, ritz.data(), ritz.size() * 16);
+    if (alphas) std::copy(r.alphas.begin(), r.alphas.end(), alphas);
+    if (betas) std::copy(r.betas.begin(), r.betas.end(), betas);
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_davidson_lowest_f64(qkrylov_hamiltonian_h h, int n_eig, int max_subspace, double tol, double* evals,
+                                double* evecs, qkrylov_davidson_result_c_t* info) {
+  if (!h || !h->op || !evals || n_eig <= 0) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    auto r = qkb::davidson<double>(*h->op, n_eig, max_subspace, tol);
+    const size_t k = std::min(size_t(n_eig), r.eigenvalues.size());
+    for (size_t i = 0; i < k; ++i) evals[i] = r.eigenvalues[i];
+    if (info) { info->iterations = r.iterations; info->converged = r.converged; }
+    if (evecs) {
+      const uint64_t dim = h->op->dim();
+      for (size_t q = 0; q < k; ++q) std::memcpy(evecs + 2 * q * dim, r.eigenvectors[q].data(), dim * 16);
+    }
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_continued_fraction_coeffs_f64(qkrylov_hamiltonian_h h, const double* phi0, int n_iter,
+                                          double* alphas, double* betas, double* norm_phi0, int* na, int* nb) {
+  if (!h || !h->op || !phi0 || !alphas || !betas || !norm_phi0 || n_iter <= 0) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    auto r = qkb::continued_fraction<double>(*h->op, reinterpret_cast<const std::complex<double>*>(phi0), n_iter);
+    *norm_phi0 = r.norm_phi0;
+    std::copy(r.alphas.begin(), r.alphas.end(), alphas);
+    std::copy(r.betas.begin(), r.betas.end(), betas);
+    if (na) *na = int(r.alphas.size());
+    if (nb) *nb = int(r.betas.size());
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+double qkrylov_evaluate_spectral_function_f64(const double* alphas, const double* betas, size_t n,
+                                              double norm_phi0, double omega, double E0, double eta) {
+  if (!alphas || n == 0 || (n > 1 && !betas)) return 0.0;
+  std::vector<double> b(n, 0.0);
+  for (size_t i = 0; i + 1 < n; ++i) b[i] = betas[i];
+  return qkb::spectral_function<double>(alphas, b.data(), n, norm_phi0, omega, E0, eta);
+}
+
+int qkrylov_ftlm_sweep_f64(qkrylov_hamiltonian_h h, int n_beta, const double* betas, int n_random, int n_steps,
+                           double* Z, double* U, double* Cv) {
+  if (!h || !h->op || n_beta <= 0 || !betas || !Z || !U || !Cv) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    auto r = qkb::ftlm<double>(*h->op, std::vector<double>(betas, betas + n_beta), n_random, n_steps);
+    for (int q = 0; q < n_beta; ++q) { Z[q] = r[q].Z; U[q] = r[q].U; Cv[q] = r[q].Cv; }
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+}  // extern "C"

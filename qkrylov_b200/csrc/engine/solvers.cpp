@@ -1,0 +1,482 @@
+#include "solvers.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <random>
+
+#include "dense.hpp"
+
+namespace qkb {
+
+namespace {
+
+template <class Real> using C = std::complex<Real>;
+
+// Device helpers on the operator's context stream.
+struct Dev {
+  const Operator& H;
+  Context& c;
+  qk_dtype t;
+  uint64_t n;
+  explicit Dev(const Operator& op, qk_dtype dt) : H(op), c(op.ctx()), t(dt), n(op.dim()) {}
+
+  DevVec vec(bool zero = true) const { return DevVec(n, t, H.device(), zero); }
+  template <class Real> void upload(const C<Real>* h, DevVec& v) const {
+    cuda_check(cudaMemcpyAsync(v.data(), h, n * sizeof(C<Real>), cudaMemcpyHostToDevice, c.stream), "H2D");
+  }
+  template <class Real> void download(const DevVec& v, std::vector<C<Real>>& h) const {
+    h.resize(n);
+    cuda_check(cudaMemcpyAsync(h.data(), v.data(), n * sizeof(C<Real>), cudaMemcpyDeviceToHost, c.stream), "D2H");
+    c.sync();
+  }
+  std::complex<double> dot(const void* x, const void* y) const {
+    qkd_check(qkd_dot(c.ws, t, n, x, y, c.dres(0), c.stream), "dot");
+    const double* r = c.fetch(c.dres(0), 2);
+    return {r[0], r[1]};
+  }
+  void scal(double a, void* x) const { qkd_check(qkd_scal(t, n, a, 0.0, x, c.stream), "scal"); }
+  void scale_into(double a, const void* x, void* y) const {
+    qkd_check(qkd_axpby(t, n, a, 0.0, x, 0.0, 0.0, y, c.stream), "scale");
+  }
+  void axpy(std::complex<double> a, const void* x, void* y) const {
+    qkd_check(qkd_axpy(t, n, a.real(), a.imag(), x, y, c.stream), "axpy");
+  }
+  // out[j] = <P_j, x> for j < k, after x -= sum a_m U_m (M <= 2); P chunked by 511.
+  void update_mdot(int M, const void* const* U, const double* a, const PtrArray& P, int k, void* x,
+                   double* out) const {
+    constexpr int kChunk = 511;
+    if (k == 0) {
+      if (M > 0) qkd_check(qkd_update_mdot(c.ws, t, n, M, U, a, 0, nullptr, x, out, c.stream), "update");
+      return;
+    }
+    for (int j0 = 0; j0 < k; j0 += kChunk) {
+      const int kk = std::min(kChunk, k - j0);
+      qkd_check(qkd_update_mdot(c.ws, t, n, j0 == 0 ? M : 0, U, a, kk, P.at(j0), x, out + 2 * j0, c.stream),
+                "multi-dot");
+    }
+  }
+  // x -= sum_j coef_j P_j (coef device, 2k doubles); nrm2 (device) if given.
+  void mupdate(const PtrArray& P, int k, const double* coef, void* x, double* nrm2) const {
+    constexpr int kChunk = 511;
+    if (k == 0) {
+      if (nrm2) qkd_check(qkd_mupdate(c.ws, t, n, 0, nullptr, nullptr, x, nrm2, c.stream), "norm");
+      return;
+    }
+    for (int j0 = 0; j0 < k; j0 += kChunk) {
+      const int kk = std::min(kChunk, k - j0);
+      const bool last = (j0 + kk == k);
+      qkd_check(qkd_mupdate(c.ws, t, n, kk, P.at(j0), coef + 2 * j0, x, last ? nrm2 : nullptr, c.stream),
+                "block update");
+    }
+  }
+};
+
+template <class Real> void normalize(const Dev& d, void* x) {  // vector_ops.hpp:90-96
+  const Real nr = Real(std::sqrt(Real(d.dot(x, x).real())));
+  if (nr == Real(0)) return;
+  d.scal(double(Real(1) / nr), x);
+}
+
+}  // namespace
+
+template <class Real>
+void reference_uniform_start(uint64_t dim, std::vector<std::complex<Real>>& v) {
+  std::mt19937 rng(1234);
+  std::uniform_real_distribution<Real> dist(-1.0, 1.0);
+  v.resize(dim);
+  for (uint64_t i = 0; i < dim; ++i) {
+    const Real im = dist(rng);
+    const Real re = dist(rng);
+    v[i] = {re, im};
+  }
+}
+
+template <class Real>
+LanczosOut<Real> lanczos(const Operator& H, int maxiter, Real tol, const std::complex<Real>* start,
+                         std::vector<std::complex<Real>>* ritz) {
+  LanczosOut<Real> res;
+  const uint64_t dim = H.dim();
+  if (dim == 0) return res;
+  const qk_dtype T = complex_dtype<Real>();
+  Dev d(H, T);
+  const int lim = int(std::min<uint64_t>(uint64_t(std::max(maxiter, 0)), dim));
+
+  std::vector<DevVec> V;
+  PtrArray P(size_t(lim) + 3, H.device());
+  DevVec w = d.vec();
+  DevVec coef(size_t(2) * (lim + 4), QK_F64, H.device());
+  double* cd = static_cast<double*>(coef.data());
+
+  {
+    std::vector<C<Real>> hv;
+    if (start) hv.assign(start, start + dim);
+    else reference_uniform_start<Real>(dim, hv);
+    V.push_back(d.vec(false));
+    d.upload<Real>(hv.data(), V[0]);
+  }
+  normalize<Real>(d, V[0].data());
+  P.set(0, V[0].data(), d.c.stream);
+
+  std::vector<Real>& alphas = res.alphas;
+  std::vector<Real>& betas = res.betas;
+  bool converged = false;
+  Real e_old = Real(1e100);
+  int actual = 0;
+  for (int iter = 0; iter < lim; ++iter) {
+    actual = iter + 1;
+    const int k = int(V.size()) - 1;  // current vector index (== iter)
+    H.apply_dot(T, V[k].data(), w.data(), d.c.dres(0));
+    const Real alpha = Real(d.c.fetch(d.c.dres(0), 1)[0]);
+    alphas.push_back(alpha);
+
+    // w -= alpha v_k + beta v_{k-1}, then c_j = <v_j, w> (j <= k) and <w, w>.
+    const void* U[2] = {V[k].data(), k > 0 ? V[k - 1].data() : nullptr};
+    const double a[4] = {double(alpha), 0.0, k > 0 ? double(betas.back()) : 0.0, 0.0};
+    P.set(k + 1, w.data(), d.c.stream);
+    d.update_mdot(k > 0 ? 2 : 1, U, a, P, k + 2, w.data(), cd);
+    d.mupdate(P, k + 1, cd, w.data(), cd + 2 * (k + 2));
+    const double* h = d.c.fetch(cd + 2 * (k + 1), 4);
+    const double before = h[0];
+    double after = h[2];
+    if (after < 0.25 * before) {  // CGS lost accuracy: project once more
+      ++res.reorth_second_rounds;
+      d.update_mdot(0, nullptr, nullptr, P, k + 1, w.data(), cd);
+      d.mupdate(P, k + 1, cd, w.data(), cd + 2 * (k + 2));
+      after = d.c.fetch(cd + 2 * (k + 2), 1)[0];
+    }
+    const Real beta = Real(std::sqrt(Real(after)));
+    if (beta < Real(1e-15)) { converged = true; break; }
+    if (iter + 1 == lim) break;
+    betas.push_back(beta);
+    V.push_back(d.vec(false));
+    d.scale_into(double(Real(1) / beta), w.data(), V.back().data());
+    P.set(k + 1, V.back().data(), d.c.stream);
+    if (iter > 0) {
+      const Real e = tridiag_ground<Real>(alphas, betas, int(alphas.size()), nullptr);
+      if (std::abs(e - e_old) < tol) { e_old = e; converged = true; break; }
+      e_old = e;
+    }
+  }
+  std::vector<Real> z;
+  res.energy = tridiag_ground<Real>(alphas, betas, int(alphas.size()), &z);
+  res.iterations = actual;
+  res.converged = converged;
+  if (ritz) {
+    DevVec r = d.vec(true);
+    const int m = int(alphas.size());
+    std::vector<double> nz(2 * size_t(std::max(m, 1)), 0.0);
+    for (int i = 0; i < m; ++i) nz[2 * i] = -double(z[i]);
+    cuda_check(cudaMemcpyAsync(cd, nz.data(), sizeof(double) * 2 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
+    d.mupdate(P, m, cd, r.data(), nullptr);
+    normalize<Real>(d, r.data());
+    d.download<Real>(r, *ritz);
+  }
+  return res;
+}
+
+template <class Real>
+CFOut<Real> continued_fraction(const Operator& H, const std::complex<Real>* phi0, int n_iter) {
+  CFOut<Real> res;
+  const uint64_t dim = H.dim();
+  if (dim == 0) return res;
+  const qk_dtype T = complex_dtype<Real>();
+  Dev d(H, T);
+  DevVec v = d.vec(false), vp = d.vec(true), w = d.vec(false);
+  d.upload<Real>(phi0, v);
+  const Real nphi = Real(std::sqrt(Real(d.dot(v.data(), v.data()).real())));
+  if (nphi < Real(1e-15)) return res;
+  d.scal(double(Real(1) / nphi), v.data());
+  res.norm_phi0 = nphi;
+  PtrArray P(1, H.device());
+  P.set(0, w.data(), d.c.stream);
+  double* r = d.c.dres(0);
+  for (int iter = 0; iter < n_iter; ++iter) {
+    H.apply_dot(T, v.data(), w.data(), r);
+    const Real alpha = Real(d.c.fetch(r, 1)[0]);
+    res.alphas.push_back(alpha);
+    const void* U[2] = {v.data(), vp.data()};
+    const double a[4] = {double(alpha), 0.0, iter > 0 ? double(res.betas.back()) : 0.0, 0.0};
+    d.update_mdot(iter > 0 ? 2 : 1, U, a, P, 1, w.data(), r);
+    const Real beta = Real(std::sqrt(Real(d.c.fetch(r, 1)[0])));
+    if (beta < Real(1e-15)) break;
+    res.betas.push_back(beta);
+    d.scale_into(double(Real(1) / beta), w.data(), vp.data());
+    std::swap(v, vp);  // v <- w / beta, v_prev <- old v
+  }
+  return res;
+}
+
+namespace {
+// src/solvers/ftlm.cpp:24-53 on a device start vector (not modified).
+template <class Real>
+void ftlm_tridiag(const Dev& d, const DevVec& start, int n_steps, std::vector<Real>& a,
+                  std::vector<Real>& b, DevVec& v, DevVec& vp, DevVec& w, PtrArray& P) {
+  const qk_dtype T = d.t;
+  qkd_check(qkd_copy(T, d.n, start.data(), v.data(), d.c.stream), "copy");
+  normalize<Real>(d, v.data());
+  qkd_check(qkd_fill(T, d.n, vp.data(), 0.0, 0.0, d.c.stream), "fill");
+  a.clear(); b.clear();
+  double* r = d.c.dres(0);
+  P.set(0, w.data(), d.c.stream);
+  for (int i = 0; i < n_steps; ++i) {
+    d.H.apply_dot(T, v.data(), w.data(), r);
+    const Real alpha = Real(d.c.fetch(r, 1)[0]);
+    a.push_back(alpha);
+    const void* U[2] = {v.data(), vp.data()};
+    const double co[4] = {double(alpha), 0.0, i > 0 ? double(b.back()) : 0.0, 0.0};
+    d.update_mdot(i > 0 ? 2 : 1, U, co, P, 1, w.data(), r);
+    const Real beta = Real(std::sqrt(Real(d.c.fetch(r, 1)[0])));
+    if (beta < Real(1e-15)) break;
+    b.push_back(beta);
+    d.scale_into(double(Real(1) / beta), w.data(), vp.data());
+    std::swap(v, vp);
+  }
+}
+}  // namespace
+
+template <class Real>
+std::vector<FTLMOut<Real>> ftlm(const Operator& H, const std::vector<Real>& betas, int n_random,
+                                int n_steps) {
+  std::vector<FTLMOut<Real>> out(betas.size());
+  for (size_t q = 0; q < betas.size(); ++q) out[q].beta = betas[q];
+  const uint64_t dim = H.dim();
+  if (dim == 0) return out;
+  const qk_dtype T = complex_dtype<Real>();
+  Dev d(H, T);
+  std::mt19937 rng(42);
+  std::normal_distribution<Real> dist(0.0, 1.0);
+  std::vector<Real> Z(betas.size(), 0), E(betas.size(), 0), E2(betas.size(), 0);
+  DevVec rv = d.vec(false), v = d.vec(false), vp = d.vec(false), w = d.vec(false);
+  PtrArray P(1, H.device());
+  std::vector<C<Real>> hv(dim);
+  std::vector<Real> a, b, ev, fc;
+  for (int r = 0; r < n_random; ++r) {
+    for (uint64_t i = 0; i < dim; ++i) {
+      const Real im = dist(rng);
+      const Real re = dist(rng);
+      hv[i] = {re, im};
+    }
+    d.upload<Real>(hv.data(), rv);
+    const Real nrm = Real(std::sqrt(Real(d.dot(rv.data(), rv.data()).real())));
+    ftlm_tridiag<Real>(d, rv, n_steps, a, b, v, vp, w, P);
+    tridiag_first<Real>(a, b, ev, fc);
+    for (size_t q = 0; q < betas.size(); ++q) {
+      for (size_t i = 0; i < ev.size(); ++i) {
+        const Real wgt = nrm * nrm * fc[i] * fc[i] * std::exp(-betas[q] * ev[i]);
+        Z[q] += wgt;
+        E[q] += ev[i] * wgt;
+        E2[q] += ev[i] * ev[i] * wgt;
+      }
+    }
+  }
+  for (size_t q = 0; q < betas.size(); ++q) {
+    const Real z = Z[q] / Real(n_random), e = E[q] / Real(n_random), e2 = E2[q] / Real(n_random);
+    out[q].Z = z;
+    out[q].U = e / z;
+    out[q].Cv = (betas[q] * betas[q]) * (e2 / z - (e / z) * (e / z));
+  }
+  return out;
+}
+
+template <class Real>
+DavidsonOut<Real> davidson(const Operator& H, int n_eig, int max_subspace, Real tol) {
+  DavidsonOut<Real> res;
+  const uint64_t dim = H.dim();
+  if (dim == 0) return res;
+  const qk_dtype T = complex_dtype<Real>();
+  Dev d(H, T);
+  n_eig = int(std::min<uint64_t>(uint64_t(std::max(n_eig, 0)), dim));
+  max_subspace = std::max(max_subspace, 2 * n_eig);
+  const int dev = H.device();
+
+  DevVec diag = d.vec(false);
+  H.diagonal(T, diag.data());
+  std::vector<C<Real>> dh;
+  d.download<Real>(diag, dh);
+
+  std::mt19937 rng(1234);
+  std::uniform_real_distribution<Real> dist(-1.0, 1.0);
+  std::vector<uint64_t> idx(dim);
+  std::iota(idx.begin(), idx.end(), uint64_t(0));
+  // Same comparator and std::sort as the reference, so ties among equal
+  // diagonal entries resolve the same way.
+  std::sort(idx.begin(), idx.end(), [&](uint64_t i, uint64_t j) { return dh[i].real() < dh[j].real(); });
+
+  const int cap = max_subspace + 2 * n_eig + 2;
+  std::vector<DevVec> V, HV;
+  PtrArray PV(size_t(cap) * 2, dev);   // [V..., HV...] for residuals
+  DevVec coef(size_t(4) * cap + 8, QK_F64, dev);
+  double* cd = static_cast<double*>(coef.data());
+  auto set_ptrs = [&]() {
+    for (size_t i = 0; i < V.size(); ++i) PV.set(i, V[i].data(), d.c.stream);
+  };
+  // t <- t - sum_v <v, t> v over the current V, twice (classical GS with
+  // reorthogonalisation; the reference runs one modified GS sweep).
+  auto orthogonalize = [&](DevVec& t) {
+    set_ptrs();
+    const int m = int(V.size());
+    for (int round = 0; round < 2 && m > 0; ++round) {
+      d.update_mdot(0, nullptr, nullptr, PV, m, t.data(), cd);
+      d.mupdate(PV, m, cd, t.data(), nullptr);
+    }
+  };
+  for (int i = 0; i < n_eig; ++i) {
+    DevVec v = d.vec(true);
+    const C<Real> one(1, 0);
+    cuda_check(cudaMemcpyAsync(static_cast<char*>(v.data()) + idx[i] * sizeof(C<Real>), &one, sizeof(one),
+                               cudaMemcpyHostToDevice, d.c.stream), "H2D");
+    orthogonalize(v);
+    Real nrm = Real(std::sqrt(Real(d.dot(v.data(), v.data()).real())));
+    if (nrm < Real(1e-10)) {
+      std::vector<C<Real>> hv(dim);
+      for (uint64_t j = 0; j < dim; ++j) { const Real im = dist(rng); const Real re = dist(rng); hv[j] = {re, im}; }
+      d.upload<Real>(hv.data(), v);
+      orthogonalize(v);
+      nrm = Real(std::sqrt(Real(d.dot(v.data(), v.data()).real())));
+    }
+    d.scal(double(Real(1) / nrm), v.data());
+    DevVec hv = d.vec(false);
+    H.apply(T, v.data(), hv.data());
+    V.push_back(std::move(v));
+    HV.push_back(std::move(hv));
+  }
+
+  std::vector<std::vector<C<Real>>> Hs;  // cached <V_i, HV_j>, i >= j
+  for (int iter = 0; iter < 100; ++iter) {
+    const int m = int(V.size());
+    set_ptrs();
+    // Entries involving new vectors; unchanged vectors give the same values.
+    if (int(Hs.size()) != m) {
+      Hs.assign(m, std::vector<C<Real>>(m));
+      for (int j = 0; j < m; ++j) {
+        d.update_mdot(0, nullptr, nullptr, PV, m, HV[j].data(), cd);
+        const double* h = d.c.fetch(cd, 2 * m);
+        for (int i = j; i < m; ++i) {
+          Hs[i][j] = C<Real>(Real(h[2 * i]), Real(h[2 * i + 1]));
+          if (i != j) Hs[j][i] = std::conj(Hs[i][j]);
+        }
+      }
+    }
+    std::vector<C<Real>> Hflat(size_t(m) * m);
+    for (int i = 0; i < m; ++i) for (int j = 0; j < m; ++j) Hflat[size_t(i) * m + j] = Hs[i][j];
+    std::vector<Real> ev;
+    std::vector<C<Real>> es;
+    jacobi_hermitian<Real>(Hflat, m, ev, es);
+
+    bool all = true;
+    std::vector<DevVec> corr;
+    for (int k = 0; k < n_eig; ++k) {
+      const Real lam = ev[k];
+      // r = sum_i s_i HV_i - lambda s_i V_i
+      for (int i = 0; i < m; ++i) PV.set(m + i, HV[i].data(), d.c.stream);
+      std::vector<double> nc(4 * size_t(m));
+      for (int i = 0; i < m; ++i) {
+        const C<Real> s = es[size_t(k) * m + i];
+        nc[2 * i] = double(lam * s.real());  nc[2 * i + 1] = double(lam * s.imag());      // -(-lambda s)
+        nc[2 * (m + i)] = -double(s.real()); nc[2 * (m + i) + 1] = -double(s.imag());     // -(s)
+      }
+      cuda_check(cudaMemcpyAsync(cd, nc.data(), sizeof(double) * 4 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
+      DevVec r = d.vec(true);
+      d.mupdate(PV, 2 * m, cd, r.data(), cd + 4 * m);
+      const Real rn = Real(std::sqrt(Real(d.c.fetch(cd + 4 * m, 1)[0])));
+      if (rn > tol) {
+        all = false;
+        DevVec t = d.vec(false);
+        qkd_check(qkd_dav_precond(T, dim, diag.data(), double(lam), r.data(), t.data(), d.c.stream), "precond");
+        corr.push_back(std::move(t));
+      }
+    }
+    if (all || iter == 99) {
+      res.iterations = iter + 1;
+      res.converged = all;
+      for (int k = 0; k < n_eig; ++k) {
+        res.eigenvalues.push_back(ev[k]);
+        std::vector<double> nc(2 * size_t(m));
+        for (int i = 0; i < m; ++i) { nc[2 * i] = -double(es[size_t(k) * m + i].real()); nc[2 * i + 1] = -double(es[size_t(k) * m + i].imag()); }
+        cuda_check(cudaMemcpyAsync(cd, nc.data(), sizeof(double) * 2 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
+        DevVec e = d.vec(true);
+        d.mupdate(PV, m, cd, e.data(), nullptr);
+        std::vector<C<Real>> he;
+        d.download<Real>(e, he);
+        res.eigenvectors.push_back(std::move(he));
+      }
+      return res;
+    }
+    if (V.size() + corr.size() > size_t(max_subspace)) {
+      std::vector<DevVec> nV, nHV;
+      for (int i = 0; i < m; ++i) PV.set(m + i, HV[i].data(), d.c.stream);
+      for (int k = 0; k < n_eig; ++k) {
+        std::vector<double> nc(2 * size_t(m));
+        for (int i = 0; i < m; ++i) { nc[2 * i] = -double(es[size_t(k) * m + i].real()); nc[2 * i + 1] = -double(es[size_t(k) * m + i].imag()); }
+        cuda_check(cudaMemcpyAsync(cd, nc.data(), sizeof(double) * 2 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
+        DevVec rv = d.vec(true), rhv = d.vec(true);
+        d.mupdate(PV, m, cd, rv.data(), nullptr);
+        PtrArray PH(size_t(m), dev);
+        for (int i = 0; i < m; ++i) PH.set(i, HV[i].data(), d.c.stream);
+        d.mupdate(PH, m, cd, rhv.data(), nullptr);
+        d.c.sync();
+        nV.push_back(std::move(rv));
+        nHV.push_back(std::move(rhv));
+      }
+      V = std::move(nV);
+      HV = std::move(nHV);
+      Hs.clear();
+    }
+    for (auto& t : corr) {
+      orthogonalize(t);
+      const Real nrm = Real(std::sqrt(Real(d.dot(t.data(), t.data()).real())));
+      if (nrm > Real(1e-10)) {
+        d.scal(double(Real(1) / nrm), t.data());
+        DevVec ht = d.vec(false);
+        H.apply(T, t.data(), ht.data());
+        V.push_back(std::move(t));
+        HV.push_back(std::move(ht));
+      }
+    }
+    if (int(Hs.size()) == m && int(V.size()) != m) {
+      // grow the cached projection by the new rows/columns
+      const int m2 = int(V.size());
+      set_ptrs();
+      std::vector<std::vector<C<Real>>> H2(m2, std::vector<C<Real>>(m2));
+      for (int i = 0; i < m; ++i) for (int j = 0; j < m; ++j) H2[i][j] = Hs[i][j];
+      for (int j = 0; j < m2; ++j) {
+        d.update_mdot(0, nullptr, nullptr, PV, m2, HV[j].data(), cd);
+        const double* h = d.c.fetch(cd, 2 * m2);
+        for (int i = std::max(j, m); i < m2; ++i) {
+          H2[i][j] = C<Real>(Real(h[2 * i]), Real(h[2 * i + 1]));
+          if (i != j) H2[j][i] = std::conj(H2[i][j]);
+        }
+      }
+      Hs = std::move(H2);
+    }
+  }
+  return res;
+}
+
+template <class Real>
+Real spectral_function(const Real* alphas, const Real* betas, size_t n, Real norm_phi0, Real omega,
+                       Real E0, Real eta) {
+  if (n == 0) return Real(0);
+  const std::complex<Real> z(omega + E0, eta);
+  std::complex<Real> f = Real(0);
+  for (int i = int(n) - 1; i >= 0; --i) {
+    if (i == int(n) - 1) f = Real(1.0) / (z - alphas[i]);
+    else f = Real(1.0) / (z - alphas[i] - betas[i] * betas[i] * f);
+  }
+  return Real(-1.0 / M_PI * std::imag(norm_phi0 * norm_phi0 * f));
+}
+
+#define QKB_INST(R)                                                                                 \
+  template void reference_uniform_start<R>(uint64_t, std::vector<std::complex<R>>&);               \
+  template LanczosOut<R> lanczos<R>(const Operator&, int, R, const std::complex<R>*,                \
+                                    std::vector<std::complex<R>>*);                                 \
+  template CFOut<R> continued_fraction<R>(const Operator&, const std::complex<R>*, int);            \
+  template std::vector<FTLMOut<R>> ftlm<R>(const Operator&, const std::vector<R>&, int, int);       \
+  template DavidsonOut<R> davidson<R>(const Operator&, int, int, R);                                \
+  template R spectral_function<R>(const R*, const R*, size_t, R, R, R, R);
+QKB_INST(double)
+QKB_INST(float)
+#undef QKB_INST
+
+}  // namespace qkb

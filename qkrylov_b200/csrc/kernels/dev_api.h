@@ -1,0 +1,115 @@
+/* Internal C ABI between the C++ host layer and the CUDA kernels of
+ * libqkrylov_b200.so.  Plain pointers, sizes and streams only; every call
+ * returns 0 or a negative status (QKD_*) and never throws.
+ *
+ * Vector dtypes: complex128 (interleaved double pairs), complex64, float64,
+ * float32.  Real dtypes are only valid for operators whose compiled
+ * coefficients are all real.
+ */
+#ifndef QKRYLOV_B200_DEV_API_H
+#define QKRYLOV_B200_DEV_API_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { QKD_OK = 0, QKD_EINVAL = -1, QKD_ECUDA = -3, QKD_ENOMEM = -4, QKD_ETIMEOUT = -5 };
+typedef enum { QK_C128 = 0, QK_C64 = 1, QK_F64 = 2, QK_F32 = 3 } qk_dtype;
+
+static inline size_t qk_dtype_size(qk_dtype t) {
+  return t == QK_C128 ? 16 : (t == QK_C64 || t == QK_F64) ? 8 : 4;
+}
+static inline int qk_dtype_complex(qk_dtype t) { return t == QK_C128 || t == QK_C64; }
+
+/* One compiled term: valid iff (s & cmask) == cval; value
+ * (wre + i wim) * (-1)^popcount(s & smask). */
+typedef struct { uint64_t cmask, cval, smask; double wre, wim; } qk_term_t;
+/* Terms [first, first+count) share the target s ^ flip. */
+typedef struct { uint64_t flip; uint32_t first, count, check, pad; } qk_group_t;
+/* A run of consecutive rows inside one sector block. */
+typedef struct { uint64_t row0; uint32_t h, lstart, count, pad; } qk_tile_t;
+
+typedef struct {
+  int nbits, L;
+  uint64_t dim;
+  const uint64_t* A; uint64_t nA;         /* block offsets | need key << 56 */
+  const uint32_t* B; uint64_t nB;         /* low ranks | key << 24 */
+  const uint32_t* llist; uint64_t nllist; /* low parts grouped by key */
+  const uint32_t* key_off; uint32_t nkeys;
+  const qk_term_t* terms; uint32_t nterms;
+  const qk_group_t* groups; uint32_t ngroups;
+  int has_diag, all_real;
+} qk_plan_desc;
+
+typedef struct qk_plan qk_plan;
+typedef struct qk_workspace qk_workspace;
+
+int qkd_plan_create(const qk_plan_desc* d, int device, qk_plan** out);
+int qkd_plan_destroy(qk_plan* p);
+uint64_t qkd_plan_dim(const qk_plan* p);
+int qkd_plan_all_real(const qk_plan* p);
+size_t qkd_plan_device_bytes(const qk_plan* p);
+
+/* y = H x (device pointers, n = dim elements of dtype t). */
+int qkd_apply(const qk_plan* p, qk_dtype t, const void* x, void* y, cudaStream_t s);
+/* y = H x and dot_out[0..1] = <x, y> (device memory) in the same pass. */
+int qkd_apply_dot(const qk_plan* p, qk_workspace* w, qk_dtype t, const void* x, void* y,
+                  double* dot_out, cudaStream_t s);
+/* Block form: X, Y hold nvec vectors, vector v at X + v*ldx elements. */
+int qkd_apply_block(const qk_plan* p, qk_dtype t, int nvec, const void* X, size_t ldx, void* Y,
+                    size_t ldy, cudaStream_t s);
+/* diag[i] = <i|H|i> as dtype t. */
+int qkd_diagonal(const qk_plan* p, qk_dtype t, void* diag, cudaStream_t s);
+/* Number of kernel launches issued by this library since load (for the
+ * bench's launch count). */
+uint64_t qkd_launch_count(void);
+
+/* ---------------------------------------------------------------- vectors
+ * Scalars are complex doubles {re, im}.  Reductions accumulate in FP64 and
+ * write their result to `out` (device memory), deterministic for a given
+ * n: each block sums a fixed slice, the last block adds the partials in
+ * block order.  `ws` is a workspace from qkd_workspace_create(). */
+int qkd_workspace_create(int device, qk_workspace** out);
+int qkd_workspace_destroy(qk_workspace* w);
+
+int qkd_fill(qk_dtype t, size_t n, void* x, double re, double im, cudaStream_t s);
+int qkd_copy(qk_dtype t, size_t n, const void* x, void* y, cudaStream_t s);
+int qkd_convert(qk_dtype tin, const void* x, qk_dtype tout, void* y, size_t n, cudaStream_t s);
+/* x *= (re + i im) */
+int qkd_scal(qk_dtype t, size_t n, double re, double im, void* x, cudaStream_t s);
+/* y += (re + i im) x */
+int qkd_axpy(qk_dtype t, size_t n, double re, double im, const void* x, void* y, cudaStream_t s);
+/* y = a x + b y, complex host scalars */
+int qkd_axpby(qk_dtype t, size_t n, double are, double aim, const void* x, double bre, double bim,
+              void* y, cudaStream_t s);
+/* out[0..1] = sum conj(x_i) y_i, written to device memory `out` */
+int qkd_dot(qk_workspace* w, qk_dtype t, size_t n, const void* x, const void* y, double* out,
+            cudaStream_t s);
+/* Optionally update x first:  x <- x - sum_{m<M} a_m U_m  (M <= 4; U and
+ * the complex coefficients a[2M] are HOST arrays), storing x back; then
+ * out[2j..2j+1] = <V_j, x> for j < k (V: DEVICE array of k pointers).  One
+ * pass over U, V and x. */
+int qkd_update_mdot(qk_workspace* w, qk_dtype t, size_t n, int M, const void* const* U,
+                    const double* a, int k, const void* const* V, void* x, double* out,
+                    cudaStream_t s);
+/* x <- x - sum_{j<k} c_j V_j (c: 2k device doubles); if nrm2 != NULL also
+ * writes ||x||^2 of the stored result to nrm2[0] (and 0 to nrm2[1]). */
+int qkd_mupdate(qk_workspace* w, qk_dtype t, size_t n, int k, const void* const* V,
+                const double* c, void* x, double* nrm2, cudaStream_t s);
+/* y = x * scale where scale = 1 / sqrt(nrm2[0]) is read on the device. */
+int qkd_normalize_into(qk_dtype t, size_t n, const double* nrm2, const void* x, void* y,
+                       cudaStream_t s);
+/* Davidson correction t = r / (diag - lambda) with the reference's clamp. */
+int qkd_dav_precond(qk_dtype t, size_t n, const void* diag, double lambda, const void* r, void* out,
+                    cudaStream_t s);
+/* Device scratch of the workspace: 2*kMaxK+16 doubles for small results. */
+double* qkd_workspace_results(qk_workspace* w);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

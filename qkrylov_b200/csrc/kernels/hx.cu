@@ -1,0 +1,319 @@
+// Matrix-free H.x: pull mode, no atomics.
+//
+// Rows are processed in tiles of up to 256 consecutive states of one sector
+// block (fixed high part h), one thread per row.  A thread rebuilds its state
+// s = (h << L) | llist[...] from the sector tables, evaluates every compiled
+// term group of the operator (terms and groups staged in shared memory), and
+// for each group with a valid term gathers x at the target's rank
+// A[t >> L] + B[t & lmask].  Consecutive rows of a tile have consecutive low
+// parts, so for every term that only flips high bits the warp's gathers are
+// consecutive addresses (coalesced); terms that flip low bits stay inside
+// the block, which L1 holds.  Each thread writes only its own y[row].
+#include <algorithm>
+#include <vector>
+
+#include "reduce.cuh"
+#include "../engine/sector.hpp"
+
+struct qk_plan {
+  int device;
+  int nbits, L;
+  uint64_t dim, lmask;
+  uint64_t* A;
+  uint32_t* B;
+  uint32_t* llist;
+  qk_term_t* terms;
+  qk_group_t* groups;
+  qk_tile_t* tiles;
+  uint32_t nterms, ngroups, ntiles;
+  int has_diag, all_real;
+  size_t bytes, smem;
+};
+
+namespace qkd {
+namespace {
+
+constexpr int kTile = 256;
+
+struct DevPlan {
+  int L;
+  uint64_t lmask;
+  const uint64_t* __restrict__ A;
+  const uint32_t* __restrict__ B;
+  const uint32_t* __restrict__ llist;
+  const qk_term_t* __restrict__ terms;
+  const qk_group_t* __restrict__ groups;
+  const qk_tile_t* __restrict__ tiles;
+  uint32_t nterms, ngroups, ntiles;
+  int has_diag;
+};
+
+DevPlan dev(const qk_plan* p) {
+  return DevPlan{p->L, p->lmask, p->A, p->B, p->llist, p->terms, p->groups, p->tiles,
+                 p->nterms, p->ngroups, p->ntiles, p->has_diag};
+}
+
+// Sum of the valid terms of one group on state s: returns false when none is valid.
+template <bool CC, class R>
+__device__ __forceinline__ bool group_coef(const qk_term_t* t, uint32_t first, uint32_t count,
+                                           uint64_t s, R& cr, R& ci) {
+  bool any = false;
+  cr = R(0); ci = R(0);
+  for (uint32_t q = first; q < first + count; ++q) {
+    const qk_term_t term = t[q];
+    if ((s & term.cmask) != term.cval) continue;
+    any = true;
+    const bool neg = __popcll(s & term.smask) & 1;
+    const R wr = R(term.wre);
+    cr += neg ? -wr : wr;
+    if (CC) { const R wi = R(term.wim); ci += neg ? -wi : wi; }
+  }
+  return any;
+}
+
+__device__ __forceinline__ void stage_plan(const DevPlan& p, qk_term_t*& st, qk_group_t*& sg) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  st = reinterpret_cast<qk_term_t*>(smem_raw);
+  sg = reinterpret_cast<qk_group_t*>(smem_raw + size_t(p.nterms) * sizeof(qk_term_t));
+  for (uint32_t i = threadIdx.x; i < p.nterms; i += blockDim.x) st[i] = p.terms[i];
+  for (uint32_t i = threadIdx.x; i < p.ngroups; i += blockDim.x) sg[i] = p.groups[i];
+  __syncthreads();
+}
+
+// y = H x for one row; returns (y_re, y_im) and the row's own x element.
+template <int DT, bool CC>
+__device__ __forceinline__ void row_apply(const DevPlan& p, const qk_term_t* st, const qk_group_t* sg,
+                                          uint64_t row, uint64_t s, const void* x,
+                                          typename VT<DT>::R& yr, typename VT<DT>::R& yi,
+                                          typename VT<DT>::R& xr0, typename VT<DT>::R& xi0) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  yr = R(0); yi = R(0);
+  T::ld(x, row, xr0, xi0);
+  uint32_t g0 = 0;
+  if (p.has_diag) {
+    R cr, ci;
+    if (group_coef<CC, R>(st, sg[0].first, sg[0].count, s, cr, ci)) {
+      yr += cr * xr0;
+      if (T::cplx) {
+        yi += cr * xi0;
+        if (CC) { yr -= ci * xi0; yi += ci * xr0; }
+      }
+    }
+    g0 = 1;
+  }
+  for (uint32_t g = g0; g < p.ngroups; ++g) {
+    const qk_group_t grp = sg[g];
+    R cr, ci;
+    if (!group_coef<CC, R>(st, grp.first, grp.count, s, cr, ci)) continue;
+    const uint64_t t = s ^ grp.flip;
+    const uint64_t a = __ldg(p.A + (t >> p.L));
+    const uint32_t b = __ldg(p.B + (t & p.lmask));
+    // Membership is re-checked for every group (one byte compare), so a
+    // gather index is always a valid row even where the compiler proved the
+    // target stays in the sector.
+    if (uint32_t(a >> 56) != (b >> 24)) continue;
+    const uint64_t col = (a & qkb::kOffsetMask) + (b & qkb::kRankMask);
+    R xr, xi;
+    T::ld(x, col, xr, xi);
+    yr += cr * xr;
+    if (T::cplx) {
+      yi += cr * xi;
+      if (CC) { yr -= ci * xi; yi += ci * xr; }
+    }
+  }
+}
+
+template <int DT, bool CC, bool DOT>
+__global__ void __launch_bounds__(kTile)
+k_hx(DevPlan p, const void* __restrict__ x, void* __restrict__ y, double* partials,
+     unsigned* ticket, double* dot_out) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  qk_term_t* st;
+  qk_group_t* sg;
+  stage_plan(p, st, sg);
+  double dr = 0.0, di = 0.0;
+  for (uint32_t ti = blockIdx.x; ti < p.ntiles; ti += gridDim.x) {
+    const qk_tile_t tile = p.tiles[ti];
+    if (threadIdx.x < tile.count) {
+      const uint64_t row = tile.row0 + threadIdx.x;
+      const uint64_t s = (uint64_t(tile.h) << p.L) | __ldg(p.llist + tile.lstart + threadIdx.x);
+      R yr, yi, xr, xi;
+      row_apply<DT, CC>(p, st, sg, row, s, x, yr, yi, xr, xi);
+      T::st(y, row, yr, yi);
+      if (DOT) {  // <x, Hx> partial: conj(x) * y
+        dr += double(xr) * double(yr) + double(xi) * double(yi);
+        di += double(xr) * double(yi) - double(xi) * double(yr);
+      }
+    }
+  }
+  if (DOT) {
+    __shared__ double sbuf[2 * (kTile / 32)];
+    block_sum2(dr, di, sbuf);
+    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
+    grid_finish(partials, ticket, 1, dot_out);
+  }
+}
+
+template <int DT, bool CC>
+__global__ void __launch_bounds__(kTile) k_diag(DevPlan p, void* __restrict__ d) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  qk_term_t* st;
+  qk_group_t* sg;
+  stage_plan(p, st, sg);
+  for (uint32_t ti = blockIdx.x; ti < p.ntiles; ti += gridDim.x) {
+    const qk_tile_t tile = p.tiles[ti];
+    if (threadIdx.x < tile.count) {
+      const uint64_t row = tile.row0 + threadIdx.x;
+      const uint64_t s = (uint64_t(tile.h) << p.L) | __ldg(p.llist + tile.lstart + threadIdx.x);
+      R cr = R(0), ci = R(0);
+      if (p.has_diag) group_coef<CC, R>(st, sg[0].first, sg[0].count, s, cr, ci);
+      T::st(d, row, cr, ci);
+    }
+  }
+}
+
+template <class K>
+int set_smem(K kernel, size_t smem) {
+  if (smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return QKD_EINVAL;
+    }
+  }
+  return QKD_OK;
+}
+
+unsigned hx_grid(const qk_plan* p) {
+  const unsigned cap = unsigned(sm_count(p->device)) * 8;
+  return std::max(1u, std::min(p->ntiles, cap));
+}
+
+template <int DT, bool CC>
+int launch_apply(const qk_plan* p, const void* x, void* y, cudaStream_t s, qk_workspace* w,
+                 double* dot_out) {
+  const DevPlan d = dev(p);
+  if (dot_out) {
+    auto k = k_hx<DT, CC, true>;
+    if (set_smem(k, p->smem)) return QKD_EINVAL;
+    const unsigned g = std::min<unsigned>(hx_grid(p), kMaxG);
+    k<<<g, kTile, p->smem, s>>>(d, x, y, w->partials, w->ticket, dot_out);
+  } else {
+    auto k = k_hx<DT, CC, false>;
+    if (set_smem(k, p->smem)) return QKD_EINVAL;
+    k<<<hx_grid(p), kTile, p->smem, s>>>(d, x, y, nullptr, nullptr, nullptr);
+  }
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+}  // namespace
+}  // namespace qkd
+
+using namespace qkd;
+
+extern "C" {
+
+int qkd_plan_create(const qk_plan_desc* d, int device, qk_plan** out) {
+  if (!d || !out || d->nbits <= 0 || d->nbits > 64 || d->L < 0 || d->L > d->nbits) return QKD_EINVAL;
+  if (d->nterms > 0 && (!d->terms || !d->groups)) return QKD_EINVAL;
+  // Tiles: runs of <= 256 rows inside each non-empty block.
+  std::vector<qk_tile_t> tiles;
+  for (uint64_t h = 0; h < d->nA; ++h) {
+    const uint32_t need = uint32_t(d->A[h] >> 56);
+    if (need == qkb::kEmptyBlockKey) continue;
+    const uint32_t start = d->key_off[need], size = d->key_off[need + 1] - start;
+    const uint64_t off = d->A[h] & qkb::kOffsetMask;
+    for (uint32_t r = 0; r < size; r += kTile)
+      tiles.push_back(qk_tile_t{off + r, uint32_t(h), start + r, std::min<uint32_t>(kTile, size - r), 0});
+  }
+  if (tiles.size() > 0xFFFFFFFFull) return QKD_EINVAL;
+  auto* p = new qk_plan{};
+  p->device = device;
+  p->nbits = d->nbits; p->L = d->L; p->dim = d->dim;
+  p->lmask = (d->L >= 64) ? ~0ULL : ((1ULL << d->L) - 1);
+  p->nterms = d->nterms; p->ngroups = d->ngroups; p->ntiles = uint32_t(tiles.size());
+  p->has_diag = d->has_diag; p->all_real = d->all_real;
+  p->smem = size_t(d->nterms) * sizeof(qk_term_t) + size_t(d->ngroups) * sizeof(qk_group_t);
+  if (p->smem > 200 * 1024) { delete p; return QKD_EINVAL; }
+  auto up = [&](void** dst, const void* src, size_t bytes) -> bool {
+    if (bytes == 0) { *dst = nullptr; return true; }
+    if (cudaMalloc(dst, bytes) != cudaSuccess) return false;
+    p->bytes += bytes;
+    return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+  };
+  bool ok = up((void**)&p->A, d->A, d->nA * 8) && up((void**)&p->B, d->B, d->nB * 4) &&
+            up((void**)&p->llist, d->llist, d->nllist * 4) &&
+            up((void**)&p->terms, d->terms, size_t(d->nterms) * sizeof(qk_term_t)) &&
+            up((void**)&p->groups, d->groups, size_t(d->ngroups) * sizeof(qk_group_t)) &&
+            up((void**)&p->tiles, tiles.data(), tiles.size() * sizeof(qk_tile_t));
+  if (!ok) {
+    (void)cudaGetLastError();
+    qkd_plan_destroy(p);
+    return QKD_ENOMEM;
+  }
+  *out = p;
+  return QKD_OK;
+}
+
+int qkd_plan_destroy(qk_plan* p) {
+  if (!p) return QKD_OK;
+  cudaFree(p->A); cudaFree(p->B); cudaFree(p->llist);
+  cudaFree(p->terms); cudaFree(p->groups); cudaFree(p->tiles);
+  delete p;
+  return QKD_OK;
+}
+
+uint64_t qkd_plan_dim(const qk_plan* p) { return p ? p->dim : 0; }
+int qkd_plan_all_real(const qk_plan* p) { return p ? p->all_real : 0; }
+size_t qkd_plan_device_bytes(const qk_plan* p) { return p ? p->bytes : 0; }
+
+int qkd_apply(const qk_plan* p, qk_dtype t, const void* x, void* y, cudaStream_t s) {
+  if (!p || !x || !y || x == y) return QKD_EINVAL;
+  if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
+  if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
+  if (p->all_real) { QKD_DISPATCH(t, return launch_apply<DT, false>(p, x, y, s, nullptr, nullptr)); }
+  QKD_DISPATCH(t, return launch_apply<DT, true>(p, x, y, s, nullptr, nullptr));
+  return QKD_OK;
+}
+
+// y = H x and out = <x, y> in one pass.
+int qkd_apply_dot(const qk_plan* p, qk_workspace* w, qk_dtype t, const void* x, void* y,
+                  double* dot_out, cudaStream_t s) {
+  if (!p || !w || !x || !y || x == y || !dot_out) return QKD_EINVAL;
+  if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
+  if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
+  if (p->all_real) { QKD_DISPATCH(t, return launch_apply<DT, false>(p, x, y, s, w, dot_out)); }
+  QKD_DISPATCH(t, return launch_apply<DT, true>(p, x, y, s, w, dot_out));
+  return QKD_OK;
+}
+
+int qkd_apply_block(const qk_plan* p, qk_dtype t, int nvec, const void* X, size_t ldx, void* Y,
+                    size_t ldy, cudaStream_t s) {
+  if (!p || nvec < 0 || !X || !Y) return QKD_EINVAL;
+  const size_t es = qk_dtype_size(t);
+  for (int v = 0; v < nvec; ++v) {
+    const int rc = qkd_apply(p, t, static_cast<const char*>(X) + v * ldx * es, static_cast<char*>(Y) + v * ldy * es, s);
+    if (rc) return rc;
+  }
+  return QKD_OK;
+}
+
+int qkd_diagonal(const qk_plan* p, qk_dtype t, void* diag, cudaStream_t s) {
+  if (!p || !diag) return QKD_EINVAL;
+  if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
+  if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
+  const DevPlan d = dev(p);
+  const unsigned g = hx_grid(p);
+  if (p->all_real) {
+    QKD_DISPATCH(t, { auto k = k_diag<DT, false>; if (set_smem(k, p->smem)) return QKD_EINVAL; k<<<g, kTile, p->smem, s>>>(d, diag); });
+  } else {
+    QKD_DISPATCH(t, { auto k = k_diag<DT, true>; if (set_smem(k, p->smem)) return QKD_EINVAL; k<<<g, kTile, p->smem, s>>>(d, diag); });
+  }
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,401 @@
+// Krylov vector kernels: fills, copies, scalings, axpy, and the FP64
+// reductions (dot, multi-vector dot, block update with norm) under the
+// solvers.  All are bandwidth-bound streams; element loads are 8/16-byte
+// vector loads, grid sizes are fixed multiples of the SM count, and the
+// reductions are deterministic (reduce.cuh).
+#include <algorithm>
+#include <atomic>
+
+#include "reduce.cuh"
+
+namespace qkd {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+int sm_count(int device) {
+  static int cache[64] = {0};
+  if (device < 0 || device >= 64) return 148;
+  if (!cache[device]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0) v = 148;
+    cache[device] = v;
+  }
+  return cache[device];
+}
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int current_device() { int d = 0; cudaGetDevice(&d); return d; }
+
+inline unsigned stream_grid(size_t n, int per_thread = 4) {
+  const size_t need = (n + size_t(kThreads) * per_thread - 1) / (size_t(kThreads) * per_thread);
+  const size_t cap = size_t(sm_count(current_device())) * 8;
+  return unsigned(std::max<size_t>(1, std::min(need, cap)));
+}
+
+inline unsigned reduce_grid(size_t n) {
+  const size_t need = (n + 2047) / 2048;
+  const size_t cap = std::min<size_t>(size_t(sm_count(current_device())) * 4, kMaxG);
+  return unsigned(std::max<size_t>(1, std::min(need, cap)));
+}
+
+template <int DT>
+__global__ void k_fill(size_t n, void* x, double re, double im) {
+  using T = VT<DT>;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    T::st(x, i, typename T::R(re), typename T::R(im));
+}
+
+template <int DI, int DO>
+__global__ void k_convert(size_t n, const void* x, void* y) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    typename VT<DI>::R re, im;
+    VT<DI>::ld(x, i, re, im);
+    VT<DO>::st(y, i, typename VT<DO>::R(re), typename VT<DO>::R(im));
+  }
+}
+
+// y = a x + b y (complex a, b; b = 0 skips reading y)
+template <int DT>
+__global__ void k_axpby(size_t n, double are, double aim, const void* x, double bre, double bim,
+                        void* y, int read_y) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    R xr, xi, yr = 0, yi = 0;
+    T::ld(x, i, xr, xi);
+    if (read_y) T::ld_plain(y, i, yr, yi);
+    R r = R(are) * xr - R(aim) * xi;
+    R m = R(are) * xi + R(aim) * xr;
+    if (read_y) { r += R(bre) * yr - R(bim) * yi; m += R(bre) * yi + R(bim) * yr; }
+    T::st(y, i, r, m);
+  }
+}
+
+// x *= a, in place
+template <int DT>
+__global__ void k_scal(size_t n, double are, double aim, void* x) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    R xr, xi;
+    T::ld_plain(x, i, xr, xi);
+    T::st(x, i, R(are) * xr - R(aim) * xi, R(are) * xi + R(aim) * xr);
+  }
+}
+
+template <int DT>
+__global__ void k_normalize_into(size_t n, const double* nrm2, const void* x, void* y) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  const double sc = 1.0 / sqrt(nrm2[0]);
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    R xr, xi;
+    T::ld(x, i, xr, xi);
+    T::st(y, i, R(double(xr) * sc), R(double(xi) * sc));
+  }
+}
+
+struct UPack { const void* u[4]; double ar[4], ai[4]; };
+
+// Tiled multi-dot.  Each warp owns tiles of 32*E consecutive elements: the x
+// tile stays in registers (after the optional update by U) while the warp
+// streams the matching tile of every V_j and adds the warp-reduced partial
+// of <V_j, x> to its own slot in shared memory.
+template <int DT, int E>
+__global__ void __launch_bounds__(kThreads)
+k_update_mdot(size_t n, int M, UPack U, int k,
+              const void* const* __restrict__ V, void* x, double* partials, unsigned* ticket,
+              double* out) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  extern __shared__ double sacc[];  // [8 warps][k][2]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* wacc = sacc + size_t(warp) * k * 2;
+  for (int j = lane; j < k; j += 32) { wacc[2 * j] = 0.0; wacc[2 * j + 1] = 0.0; }
+  __syncwarp();
+  const size_t tile = size_t(32) * E;
+  const size_t nwarps = size_t(gridDim.x) * (kThreads / 32);
+  for (size_t base = (size_t(blockIdx.x) * (kThreads / 32) + warp) * tile; base < n; base += nwarps * tile) {
+    double xr[E], xi[E];
+    #pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const size_t i = base + size_t(e) * 32 + lane;
+      xr[e] = 0.0; xi[e] = 0.0;
+      if (i < n) {
+        R r, m; T::ld_plain(x, i, r, m); xr[e] = r; xi[e] = m;
+      }
+    }
+    if (M > 0) {
+      #pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        if (m >= M) break;
+        const void* um = U.u[m];
+        const double ar = U.ar[m], ai = U.ai[m];
+        #pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const size_t i = base + size_t(e) * 32 + lane;
+          if (i < n) {
+            R ur, ui; T::ld(um, i, ur, ui);
+            xr[e] -= ar * double(ur) - ai * double(ui);
+            xi[e] -= ar * double(ui) + ai * double(ur);
+          }
+        }
+      }
+      #pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const size_t i = base + size_t(e) * 32 + lane;
+        if (i < n) {
+          T::st(x, i, R(xr[e]), R(xi[e]));
+          xr[e] = double(R(xr[e])); xi[e] = double(R(xi[e]));  // dot the stored values
+        }
+      }
+    }
+    for (int j = 0; j < k; ++j) {
+      const void* vj = V[j];
+      double pr = 0.0, pi = 0.0;
+      #pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const size_t i = base + size_t(e) * 32 + lane;
+        if (i < n) {
+          R vr, vi; T::ld(vj, i, vr, vi);
+          pr += double(vr) * xr[e] + double(vi) * xi[e];
+          pi += double(vr) * xi[e] - double(vi) * xr[e];
+        }
+      }
+      pr = warp_sum(pr);
+      pi = warp_sum(pi);
+      if (lane == 0) { wacc[2 * j] += pr; wacc[2 * j + 1] += pi; }
+    }
+  }
+  __syncthreads();
+  const int G = gridDim.x;
+  for (int j = threadIdx.x; j < k; j += kThreads) {
+    double re = 0.0, im = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) { re += sacc[(size_t(w) * k + j) * 2]; im += sacc[(size_t(w) * k + j) * 2 + 1]; }
+    partials[(size_t(j) * G + blockIdx.x) * 2] = re;
+    partials[(size_t(j) * G + blockIdx.x) * 2 + 1] = im;
+  }
+  grid_finish(partials, ticket, k, out);
+}
+
+// x <- x - sum_j c_j V_j, optional ||x||^2.
+template <int DT, bool NRM>
+__global__ void __launch_bounds__(kThreads)
+k_mupdate(size_t n, int k, const void* const* __restrict__ V, const double* __restrict__ c, void* x,
+          double* partials, unsigned* ticket, double* nrm2) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  extern __shared__ double sc[];  // 2k coefficients, then 2*8 reduction scratch
+  for (int j = threadIdx.x; j < 2 * k; j += kThreads) sc[j] = c[j];
+  __syncthreads();
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n; i += size_t(gridDim.x) * kThreads) {
+    R r0, i0; T::ld_plain(x, i, r0, i0);
+    double xr = r0, xi = i0;
+    for (int j = 0; j < k; ++j) {
+      R vr, vi; T::ld(V[j], i, vr, vi);
+      xr -= sc[2 * j] * double(vr) - sc[2 * j + 1] * double(vi);
+      xi -= sc[2 * j] * double(vi) + sc[2 * j + 1] * double(vr);
+    }
+    const R sr = R(xr), si = R(xi);
+    T::st(x, i, sr, si);
+    if (NRM) acc += double(sr) * double(sr) + double(si) * double(si);
+  }
+  if (NRM) {
+    double im = 0.0;
+    block_sum2(acc, im, sc + 2 * k);
+    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = acc; partials[2 * blockIdx.x + 1] = 0.0; }
+    grid_finish(partials, ticket, 1, nrm2);
+  }
+}
+
+}  // namespace
+}  // namespace qkd
+
+using namespace qkd;
+
+extern "C" {
+
+uint64_t qkd_launch_count(void) { return g_launches.load(); }
+
+int qkd_workspace_create(int device, qk_workspace** out) {
+  if (!out) return QKD_EINVAL;
+  auto* w = new qk_workspace{};
+  w->device = device;
+  w->nsm = sm_count(device);
+  if (cudaMalloc(&w->partials, sizeof(double) * 2 * kMaxK * kMaxG) != cudaSuccess ||
+      cudaMalloc(&w->ticket, sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&w->result, sizeof(double) * (2 * kMaxK + 16)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cudaFree(w->partials); cudaFree(w->ticket); cudaFree(w->result);
+    delete w;
+    return QKD_ENOMEM;
+  }
+  cudaMemset(w->ticket, 0, sizeof(unsigned));
+  cudaMemset(w->result, 0, sizeof(double) * (2 * kMaxK + 16));
+  *out = w;
+  return QKD_OK;
+}
+
+int qkd_workspace_destroy(qk_workspace* w) {
+  if (!w) return QKD_OK;
+  cudaFree(w->partials); cudaFree(w->ticket); cudaFree(w->result);
+  delete w;
+  return QKD_OK;
+}
+
+double* qkd_workspace_results(qk_workspace* w) { return w ? w->result : nullptr; }
+
+int qkd_fill(qk_dtype t, size_t n, void* x, double re, double im, cudaStream_t s) {
+  if (n == 0) return QKD_OK;
+  if (!x) return QKD_EINVAL;
+  QKD_DISPATCH(t, k_fill<DT><<<stream_grid(n), kThreads, 0, s>>>(n, x, re, im));
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+int qkd_copy(qk_dtype t, size_t n, const void* x, void* y, cudaStream_t s) {
+  if (n == 0 || x == y) return QKD_OK;
+  if (!x || !y) return QKD_EINVAL;
+  if (cudaMemcpyAsync(y, x, n * qk_dtype_size(t), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return QKD_ECUDA;
+  }
+  return QKD_OK;
+}
+
+int qkd_convert(qk_dtype tin, const void* x, qk_dtype tout, void* y, size_t n, cudaStream_t s) {
+  if (n == 0) return QKD_OK;
+  if (!x || !y) return QKD_EINVAL;
+  if (tin == tout) return qkd_copy(tin, n, x, y, s);
+  const unsigned g = stream_grid(n);
+#define QKD_CONV(A, B) \
+  if (tin == A && tout == B) { k_convert<A, B><<<g, kThreads, 0, s>>>(n, x, y); QKD_LAUNCH_CHECK(); return QKD_OK; }
+  QKD_CONV(QK_C128, QK_C64) QKD_CONV(QK_C64, QK_C128) QKD_CONV(QK_F64, QK_F32) QKD_CONV(QK_F32, QK_F64)
+  QKD_CONV(QK_F64, QK_C128) QKD_CONV(QK_F32, QK_C64) QKD_CONV(QK_C128, QK_F64) QKD_CONV(QK_C64, QK_F32)
+  QKD_CONV(QK_F32, QK_C128) QKD_CONV(QK_C128, QK_F32) QKD_CONV(QK_F64, QK_C64) QKD_CONV(QK_C64, QK_F64)
+#undef QKD_CONV
+  return QKD_EINVAL;
+}
+
+int qkd_scal(qk_dtype t, size_t n, double re, double im, void* x, cudaStream_t s) {
+  if (n == 0) return QKD_OK;
+  if (!x) return QKD_EINVAL;
+  QKD_DISPATCH(t, k_scal<DT><<<stream_grid(n), kThreads, 0, s>>>(n, re, im, x));
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+int qkd_axpy(qk_dtype t, size_t n, double re, double im, const void* x, void* y, cudaStream_t s) {
+  return qkd_axpby(t, n, re, im, x, 1.0, 0.0, y, s);
+}
+
+int qkd_axpby(qk_dtype t, size_t n, double are, double aim, const void* x, double bre, double bim,
+              void* y, cudaStream_t s) {
+  if (n == 0) return QKD_OK;
+  if (!x || !y) return QKD_EINVAL;
+  const int read_y = (bre != 0.0 || bim != 0.0);
+  QKD_DISPATCH(t, k_axpby<DT><<<stream_grid(n), kThreads, 0, s>>>(n, are, aim, x, bre, bim, y, read_y));
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+int qkd_update_mdot(qk_workspace* w, qk_dtype t, size_t n, int M, const void* const* U,
+                    const double* a, int k, const void* const* V, void* x, double* out,
+                    cudaStream_t s) {
+  if (!w || !x || !out || M < 0 || M > 4 || k < 0 || k > kMaxK || (M > 0 && (!U || !a)) ||
+      (k > 0 && !V))
+    return QKD_EINVAL;
+  if (k == 0 && M == 0) return QKD_OK;
+  UPack up{};
+  for (int m = 0; m < M; ++m) { up.u[m] = U[m]; up.ar[m] = a[2 * m]; up.ai[m] = a[2 * m + 1]; }
+  const unsigned G = std::min<unsigned>(reduce_grid(n), kMaxG);
+  const size_t smem = size_t(kThreads / 32) * std::max(k, 1) * 2 * sizeof(double);
+  if (smem > 48 * 1024) {
+    QKD_DISPATCH(t, cudaFuncSetAttribute(k_update_mdot<DT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  }
+  QKD_DISPATCH(t, k_update_mdot<DT, 8><<<G, kThreads, smem, s>>>(n, M, up, k, V, x, w->partials,
+                                                                 w->ticket, out));
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+int qkd_dot(qk_workspace* w, qk_dtype t, size_t n, const void* x, const void* y, double* out,
+            cudaStream_t s) {
+  // <x, y> = one multi-dot with V = {x}; the pointer array lives in the
+  // workspace's result scratch tail.
+  if (!w || !x || !y || !out) return QKD_EINVAL;
+  const void* host_ptr = x;
+  void** dev_ptrs = reinterpret_cast<void**>(w->result + 2 * kMaxK + 8);
+  if (cudaMemcpyAsync(dev_ptrs, &host_ptr, sizeof(void*), cudaMemcpyHostToDevice, s) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return QKD_ECUDA;
+  }
+  // y is only read: pass it as x with M = 0 (no store happens).
+  return qkd_update_mdot(w, t, n, 0, nullptr, nullptr, 1, reinterpret_cast<const void* const*>(dev_ptrs),
+                         const_cast<void*>(y), out, s);
+}
+
+int qkd_mupdate(qk_workspace* w, qk_dtype t, size_t n, int k, const void* const* V,
+                const double* c, void* x, double* nrm2, cudaStream_t s) {
+  if (!w || !x || k < 0 || k > kMaxK || (k > 0 && (!V || !c))) return QKD_EINVAL;
+  const unsigned G = std::min<unsigned>(reduce_grid(n), kMaxG);
+  const size_t smem = (2 * size_t(k) + 16) * sizeof(double);
+  if (nrm2) {
+    QKD_DISPATCH(t, k_mupdate<DT, true><<<G, kThreads, smem, s>>>(n, k, V, c, x, w->partials, w->ticket, nrm2));
+  } else {
+    if (k == 0) return QKD_OK;
+    QKD_DISPATCH(t, k_mupdate<DT, false><<<G, kThreads, smem, s>>>(n, k, V, c, x, w->partials, w->ticket, nrm2));
+  }
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+int qkd_normalize_into(qk_dtype t, size_t n, const double* nrm2, const void* x, void* y,
+                       cudaStream_t s) {
+  if (n == 0) return QKD_OK;
+  if (!nrm2 || !x || !y) return QKD_EINVAL;
+  QKD_DISPATCH(t, k_normalize_into<DT><<<stream_grid(n), kThreads, 0, s>>>(n, nrm2, x, y));
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- Davidson
+// t_i = r_i / (d_i - lambda), the divisor replaced by +-1e-10 when its modulus
+// is below 1e-10, and the complex division scaled by the divisor's 1-norm
+// (src/solvers/davidson.cpp:171-175).
+namespace qkd {
+namespace {
+template <int DT>
+__global__ void k_dav_precond(size_t n, const void* diag, double lambda, const void* r, void* t) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    R dr, di, rr, ri;
+    T::ld(diag, i, dr, di);
+    T::ld(r, i, rr, ri);
+    R er = dr - R(lambda), ei = di;
+    if (sqrt(er * er + ei * ei) < R(1e-10)) { er = (er >= R(0)) ? R(1e-10) : R(-1e-10); ei = R(0); }
+    const R s = fabs(er) + fabs(ei);
+    const R xr = rr / s, xi = ri / s, yr = er / s, yi = -ei / s;
+    const R den = yr * yr + yi * yi;
+    T::st(t, i, (xr * yr - xi * yi) / den, (xr * yi + xi * yr) / den);
+  }
+}
+}  // namespace
+}  // namespace qkd
+
+extern "C" int qkd_dav_precond(qk_dtype t, size_t n, const void* diag, double lambda, const void* r,
+                               void* out, cudaStream_t s) {
+  if (n == 0) return QKD_OK;
+  if (!diag || !r || !out) return QKD_EINVAL;
+  QKD_DISPATCH(t, qkd::k_dav_precond<DT><<<qkd::stream_grid(n), qkd::kThreads, 0, s>>>(n, diag, lambda, r, out));
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
