@@ -199,6 +199,13 @@ def run_b200(args):
         ms = float(t.item())
     bytes_step = D * 32
     value = world * bytes_step / (ms * 1e-3) / 1e9
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"kernel_only": True, "N": N, "dim": D, "ms_per_step": ms,
+                              "GBs_effective": bytes_step / (ms * 1e-3) / 1e9, "kernel": H.kernel}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     variants = {}
     for name, code, tdt, b in [("c64", qk.DTYPE_C64, torch.complex64, 16), ("f64", qk.DTYPE_F64, torch.float64, 16),
@@ -239,7 +246,7 @@ def run_b200(args):
                        "parallelism": "replicas" if world > 1 else "single-gpu"},
             "roofline": {"bound": "hbm", "achieved": bytes_step / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": bytes_step / (ms * 1e-3) / 1e9 / peak, "traffic": traffic,
-                         "peak_source": peak_kind, "kernel": "k_hx<complex128, real coefficients>"},
+                         "peak_source": peak_kind, "kernel": H.kernel},
             "e2e": {"value": world * bytes_step / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
                     "h2d_bytes_per_step": D * 16, "d2h_bytes_per_step": D * 16, "ms_per_step": e2e_ms,
                     "path": "qkrylov_hamiltonian_apply_complex_f64, pinned host buffers"},
@@ -266,6 +273,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=28)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="time only the complex128 device apply (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

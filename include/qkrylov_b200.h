@@ -30,6 +30,10 @@ const char* qkrylov_b200_last_error(void);
 /* Kernels launched by this library since it was loaded. */
 uint64_t qkrylov_b200_launch_count(void);
 int qkrylov_b200_device_count(void);
+/* 0 (default): H.x uses the specialised two-site exchange kernel wherever
+ * the compiled operator qualifies; 1: the generic kernel everywhere (for
+ * comparisons).  Process-wide. */
+int qkrylov_b200_set_kernel_policy(int policy);
 
 /* Select which of N_up / N_dn a sector conserves after
  * qkrylov_sector_set_hubbard_particles (c_api.h:33), which always sets
@@ -70,6 +74,8 @@ qkrylov_hamiltonian_h qkrylov_hamiltonian_create_ex(qkrylov_basis_h basis, qkryl
 int qkrylov_hamiltonian_precision(qkrylov_hamiltonian_h h);
 int qkrylov_hamiltonian_all_real(qkrylov_hamiltonian_h h);
 uint64_t qkrylov_hamiltonian_device_bytes(qkrylov_hamiltonian_h h);
+/* 1 when this handle's H.x runs the specialised two-site exchange kernel. */
+int qkrylov_hamiltonian_kernel(qkrylov_hamiltonian_h h);
 /* The CUDA stream (cudaStream_t) the library uses on the handle's device. */
 void* qkrylov_hamiltonian_stream(qkrylov_hamiltonian_h h);
 

@@ -415,6 +415,11 @@ class MatrixFreeHamiltonian:
                "apply_device")
 
     @property
+    def kernel(self) -> str:
+        """'spin-exchange' or 'generic': the H.x kernel this operator uses."""
+        return "spin-exchange" if lib().qkrylov_hamiltonian_kernel(self._h) else "generic"
+
+    @property
     def stream(self) -> int:
         return int(lib().qkrylov_hamiltonian_stream(self._h) or 0)
 
@@ -537,6 +542,11 @@ def ftlm(H: MatrixFreeHamiltonian, beta: float, n_random: int = 50, n_steps: int
     r = _FTLMC()
     _check(lib().qkrylov_ftlm(H._h, ctypes.c_float(beta), n_random, n_steps, ctypes.byref(r)), "ftlm")
     return FTLMResult(r.beta, r.partition_function, r.internal_energy, r.specific_heat)
+
+
+def set_kernel_policy(policy: str):
+    """'auto' (specialised kernels where eligible) or 'generic'."""
+    _check(lib().qkrylov_b200_set_kernel_policy({"auto": 0, "generic": 1}[policy]), "set_kernel_policy")
 
 
 def find_gpu():

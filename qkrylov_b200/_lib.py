@@ -72,6 +72,8 @@ PROTOTYPES = {
     "qkrylov_b200_launch_count": (_u64, []),
     "qkrylov_b200_device_count": (_i, []),
     "qkrylov_b200_sector_set_species": (_i, [_vp, _i, _i]),
+    "qkrylov_b200_set_kernel_policy": (_i, [_i]),
+    "qkrylov_hamiltonian_kernel": (_i, [_vp]),
     "qkrylov_b200_site_apply": (_i, [_vp, _cp, _i, _u64, _vp, _vp, _vp]),
     "qkrylov_basis_states": (_i, [_vp, _u64, _u64, _vp]),
     "qkrylov_basis_index_many": (_i, [_vp, _vp, _u64, _vp]),

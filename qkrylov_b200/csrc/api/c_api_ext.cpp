@@ -37,6 +37,12 @@ int qkrylov_b200_device_count(void) {
   return n;
 }
 
+int qkrylov_b200_set_kernel_policy(int policy) {
+  return qkd_set_kernel_policy(policy) == QKD_OK ? QKRYLOV_SUCCESS : QKRYLOV_ERROR_INVALID_ARG;
+}
+
+int qkrylov_hamiltonian_kernel(qkrylov_hamiltonian_h h) { return (h && h->op) ? qkd_plan_kernel(h->op->plan()) : 0; }
+
 int qkrylov_b200_sector_set_species(qkrylov_sector_h sector, int use_nup, int use_ndn) {
   if (!sector) return QKRYLOV_ERROR_INVALID_ARG;
   sector->s.use_nup = use_nup != 0;

@@ -54,6 +54,12 @@ uint64_t qkd_plan_dim(const qk_plan* p);
 int qkd_plan_all_real(const qk_plan* p);
 size_t qkd_plan_device_bytes(const qk_plan* p);
 
+/* 0: use specialised kernels where the operator qualifies (default);
+ * 1: generic kernel only (for comparisons). */
+int qkd_set_kernel_policy(int policy);
+/* 1 when applies of this plan run the specialised two-site spin kernel. */
+int qkd_plan_kernel(const qk_plan* p);
+
 /* y = H x (device pointers, n = dim elements of dtype t). */
 int qkd_apply(const qk_plan* p, qk_dtype t, const void* x, void* y, cudaStream_t s);
 /* y = H x and dot_out[0..1] = <x, y> (device memory) in the same pass. */

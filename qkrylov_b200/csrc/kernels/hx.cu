@@ -15,7 +15,18 @@
 #include "reduce.cuh"
 #include "../engine/sector.hpp"
 
+namespace qkd {
+struct SpinHandle;
+SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes);
+void spin_plan_destroy(SpinHandle* h);
+int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
+               double* dot_out);
+}  // namespace qkd
+
+static int g_kernel_policy = 0;  // 0: specialised kernels where eligible, 1: generic only
+
 struct qk_plan {
+  qkd::SpinHandle* spin = nullptr;
   int device;
   int nbits, L;
   uint64_t dim, lmask;
@@ -254,12 +265,22 @@ int qkd_plan_create(const qk_plan_desc* d, int device, qk_plan** out) {
     qkd_plan_destroy(p);
     return QKD_ENOMEM;
   }
+  p->spin = qkd::spin_plan_create(d, &p->bytes);
   *out = p;
   return QKD_OK;
 }
 
+int qkd_set_kernel_policy(int policy) {
+  if (policy < 0 || policy > 1) return QKD_EINVAL;
+  g_kernel_policy = policy;
+  return QKD_OK;
+}
+
+int qkd_plan_kernel(const qk_plan* p) { return (p && p->spin && g_kernel_policy == 0) ? 1 : 0; }
+
 int qkd_plan_destroy(qk_plan* p) {
   if (!p) return QKD_OK;
+  qkd::spin_plan_destroy(p->spin);
   cudaFree(p->A); cudaFree(p->B); cudaFree(p->llist);
   cudaFree(p->terms); cudaFree(p->groups); cudaFree(p->tiles);
   delete p;
@@ -274,6 +295,7 @@ int qkd_apply(const qk_plan* p, qk_dtype t, const void* x, void* y, cudaStream_t
   if (!p || !x || !y || x == y) return QKD_EINVAL;
   if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
   if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
+  if (p->spin && g_kernel_policy == 0) return qkd::spin_apply(p->spin, t, x, y, s, nullptr, nullptr);
   if (p->all_real) { QKD_DISPATCH(t, return launch_apply<DT, false>(p, x, y, s, nullptr, nullptr)); }
   QKD_DISPATCH(t, return launch_apply<DT, true>(p, x, y, s, nullptr, nullptr));
   return QKD_OK;
@@ -285,6 +307,7 @@ int qkd_apply_dot(const qk_plan* p, qk_workspace* w, qk_dtype t, const void* x, 
   if (!p || !w || !x || !y || x == y || !dot_out) return QKD_EINVAL;
   if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
   if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
+  if (p->spin && g_kernel_policy == 0) return qkd::spin_apply(p->spin, t, x, y, s, w, dot_out);
   if (p->all_real) { QKD_DISPATCH(t, return launch_apply<DT, false>(p, x, y, s, w, dot_out)); }
   QKD_DISPATCH(t, return launch_apply<DT, true>(p, x, y, s, w, dot_out));
   return QKD_OK;

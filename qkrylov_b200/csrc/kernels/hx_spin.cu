@@ -1,0 +1,280 @@
+// H.x specialised for two-site exchange operators in a single-charge sector
+// (spin-1/2 fixed Sz, spinless fermions without strings): the Heisenberg,
+// XXZ and J1-J2 families.
+//
+// Every off-diagonal group flips exactly two bits i < j and is conditioned on
+// both (Sp_i Sm_j, Sm_i Sp_j ...), every diagonal term is a sign-only
+// product (Sz Sz).  Relative to the sector split at bit L a bond is
+//   low      (i, j < L):  target rank = A[h] + B[l ^ F]       one smem lookup
+//   high     (i, j >= L): target rank = A[h ^ F'] + r         validity and base
+//                         depend on h only, so they are computed once per tile
+//                         and the warp's gathers are consecutive addresses
+//   crossing (i < L <= j): A[h ^ F'] + B[l ^ F], two smem lookups.
+// A (u32 offsets) and B (u16 in-class ranks) live in shared memory; the
+// state of a row comes from the coalesced low-part list.  One thread per row,
+// 512 rows per tile.
+#include <algorithm>
+#include <vector>
+
+#include "reduce.cuh"
+#include "../engine/sector.hpp"
+
+namespace qkd {
+
+constexpr int kSpinThreads = 512;
+constexpr int kMaxBonds = 64;
+constexpr int kMaxDiag = 128;
+
+struct SpinBond {
+  uint32_t lo_mask, hi_mask;  // flip split into the low / high part
+  double c[4];                // coefficient for (bit_i, bit_j) = 00, 10, 01, 11
+  uint8_t bi, bj;             // bit positions
+  uint8_t kind;               // 0 low, 1 high, 2 crossing
+  uint8_t valid_mask;         // which combos have a valid term
+};
+
+struct SpinPlan {
+  int L, H;
+  uint64_t dim;
+  int nbonds, ndiag;
+  SpinBond bonds[kMaxBonds];
+  uint32_t diag_smask[kMaxDiag];
+  double diag_w[kMaxDiag];
+  const uint32_t* A32;   // 2^H block offsets (global copy, staged to smem)
+  const uint16_t* B16;   // 2^L in-class ranks (global copy, staged to smem)
+  const uint16_t* lrow;  // llist as u16
+  const qk_tile_t* tiles;
+  uint32_t ntiles;
+  size_t smem;
+};
+
+namespace {
+
+template <int DT, bool DOT>
+__global__ void __launch_bounds__(kSpinThreads)
+k_hx_spin(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y, double* partials,
+          unsigned* ticket, double* dot_out) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  extern __shared__ __align__(16) unsigned char sm[];
+  const SpinPlan& p = *pp;
+  const int nA = 1 << p.H, nB = 1 << p.L;
+  const int nbonds = p.nbonds, ndiag = p.ndiag;
+  const uint64_t dim = p.dim;
+  const uint32_t ntiles = p.ntiles;
+  uint32_t* sA = reinterpret_cast<uint32_t*>(sm);
+  uint16_t* sB = reinterpret_cast<uint16_t*>(sm + size_t(nA) * 4);
+  __shared__ SpinBond sbond[kMaxBonds];
+  __shared__ uint32_t sdm[kMaxDiag];
+  __shared__ R sdw[kMaxDiag];
+  __shared__ uint64_t s_hbase[kMaxBonds];
+  __shared__ R s_hcoef[kMaxBonds];
+  __shared__ int s_hvalid[kMaxBonds];
+  for (int i = threadIdx.x; i < nA; i += blockDim.x) sA[i] = p.A32[i];
+  for (int i = threadIdx.x; i < nB; i += blockDim.x) sB[i] = p.B16[i];
+  for (int i = threadIdx.x; i < nbonds; i += blockDim.x) sbond[i] = p.bonds[i];
+  for (int i = threadIdx.x; i < ndiag; i += blockDim.x) { sdm[i] = p.diag_smask[i]; sdw[i] = R(p.diag_w[i]); }
+  __syncthreads();
+  const int L = p.L;
+  const uint32_t lm = (1u << L) - 1u;
+  double dr = 0.0, di = 0.0;
+  for (uint32_t ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+    const qk_tile_t tile = p.tiles[ti];
+    const uint32_t h = tile.h;
+    if (threadIdx.x < uint32_t(nbonds)) {  // per-tile data of the high bonds
+      const SpinBond b = sbond[threadIdx.x];
+      if (b.kind == 1) {
+        const uint32_t bi = (h >> (b.bi - L)) & 1u, bj = (h >> (b.bj - L)) & 1u;
+        const int combo = int(bi | (bj << 1));
+        s_hvalid[threadIdx.x] = (b.valid_mask >> combo) & 1;
+        s_hcoef[threadIdx.x] = R(b.c[combo]);
+        s_hbase[threadIdx.x] = sA[h ^ b.hi_mask];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < tile.count) {
+      const uint64_t row = tile.row0 + threadIdx.x;
+      const uint64_t rank_in_block = row - sA[h];
+      const uint32_t l = p.lrow[tile.lstart + threadIdx.x];
+      const uint32_t s = (h << L) | l;
+      R xr0, xi0;
+      T::ld(x, row, xr0, xi0);
+      R d = R(0);
+      for (int q = 0; q < ndiag; ++q) d += (__popc(s & sdm[q]) & 1) ? -sdw[q] : sdw[q];
+      R yr = d * xr0, yi = d * xi0;
+      const uint64_t base = sA[h];
+      for (int q = 0; q < nbonds; ++q) {
+        const SpinBond& b = sbond[q];
+        uint64_t col;
+        R c;
+        if (b.kind == 1) {
+          if (!s_hvalid[q]) continue;
+          col = s_hbase[q] + rank_in_block;
+          c = s_hcoef[q];
+        } else {
+          const uint32_t bi = (s >> b.bi) & 1u, bj = (s >> b.bj) & 1u;
+          const int combo = int(bi | (bj << 1));
+          if (!((b.valid_mask >> combo) & 1)) continue;
+          c = R(b.c[combo]);
+          col = (b.kind == 0 ? base : uint64_t(sA[h ^ b.hi_mask])) + sB[l ^ b.lo_mask];
+        }
+        if (col >= dim) continue;  // cannot happen for conserving bonds; keeps every load in bounds
+        R xr, xi;
+        T::ld(x, col, xr, xi);
+        yr += c * xr;
+        if (T::cplx) yi += c * xi;
+      }
+      T::st(y, row, yr, yi);
+      if (DOT) {
+        dr += double(xr0) * double(yr) + double(xi0) * double(yi);
+        di += double(xr0) * double(yi) - double(xi0) * double(yr);
+      }
+    }
+    __syncthreads();
+  }
+  if (DOT) {
+    __shared__ double sbuf[2 * (kSpinThreads / 32)];
+    block_sum2(dr, di, sbuf);
+    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
+    grid_finish(partials, ticket, 1, dot_out);
+  }
+}
+
+}  // namespace
+
+struct SpinHandle {
+  SpinPlan host;
+  SpinPlan* dev = nullptr;
+  void* bufs[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+void spin_plan_destroy(SpinHandle* h) {
+  if (!h) return;
+  for (void* b : h->bufs) cudaFree(b);
+  cudaFree(h->dev);
+  delete h;
+}
+
+// Host side: decide eligibility from the compiled plan and build the
+// specialised tables.  Returns nullptr when the operator does not qualify.
+SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
+  if (!d->all_real || d->nbits > 30 || d->dim >= (1ull << 32) || d->nterms == 0) return nullptr;
+  const int L = d->L, H = d->nbits - d->L;
+  if (L > 15 || H > 15 || L < 1) return nullptr;
+  // single charge: every key is a plain popcount (or 0 without a sector)
+  for (uint64_t l = 0; l < d->nB; ++l) {
+    const uint32_t key = d->B[l] >> 24;
+    if (key == qkb::kInvalidLowKey) return nullptr;
+    if (key != uint32_t(__builtin_popcountll(l)) && key != 0) return nullptr;
+    if ((d->B[l] & qkb::kRankMask) > 0xFFFF) return nullptr;
+  }
+  SpinPlan h{};
+  h.L = L; h.H = H; h.dim = d->dim;
+  uint32_t g0 = 0;
+  if (d->has_diag) {
+    const qk_group_t& g = d->groups[0];
+    if (g.count > uint32_t(kMaxDiag)) return nullptr;
+    for (uint32_t q = g.first; q < g.first + g.count; ++q) {
+      const qk_term_t& t = d->terms[q];
+      if (t.cmask != 0 || (t.smask >> 32)) return nullptr;
+      h.diag_smask[h.ndiag] = uint32_t(t.smask);
+      h.diag_w[h.ndiag] = t.wre;
+      ++h.ndiag;
+    }
+    g0 = 1;
+  }
+  if (d->ngroups - g0 > uint32_t(kMaxBonds)) return nullptr;
+  for (uint32_t gi = g0; gi < d->ngroups; ++gi) {
+    const qk_group_t& g = d->groups[gi];
+    if (__builtin_popcountll(g.flip) != 2 || g.check) return nullptr;
+    SpinBond b{};
+    const int i = __builtin_ctzll(g.flip), j = 63 - __builtin_clzll(g.flip);
+    b.bi = uint8_t(i); b.bj = uint8_t(j);
+    b.lo_mask = uint32_t(g.flip & ((1ull << L) - 1));
+    b.hi_mask = uint32_t(g.flip >> L);
+    b.kind = (j < L) ? 0 : (i >= L ? 1 : 2);
+    for (uint32_t q = g.first; q < g.first + g.count; ++q) {
+      const qk_term_t& t = d->terms[q];
+      if (t.cmask != g.flip || (t.smask & ~g.flip)) return nullptr;
+      const int combo = int(((t.cval >> i) & 1) | (((t.cval >> j) & 1) << 1));
+      const int neg = __builtin_popcountll(t.cval & t.smask) & 1;
+      b.c[combo] += neg ? -t.wre : t.wre;
+      b.valid_mask |= uint8_t(1u << combo);
+    }
+    h.bonds[h.nbonds++] = b;
+  }
+  std::vector<uint32_t> A32(d->nA);
+  std::vector<uint16_t> B16(d->nB), l16(d->nllist);
+  for (uint64_t k = 0; k < d->nA; ++k) A32[k] = uint32_t(d->A[k] & qkb::kOffsetMask);
+  for (uint64_t k = 0; k < d->nB; ++k) B16[k] = uint16_t(d->B[k] & 0xFFFF);
+  for (uint64_t k = 0; k < d->nllist; ++k) l16[k] = uint16_t(d->llist[k]);
+  std::vector<qk_tile_t> tiles;
+  for (uint64_t hh = 0; hh < d->nA; ++hh) {
+    const uint32_t need = uint32_t(d->A[hh] >> 56);
+    if (need == qkb::kEmptyBlockKey) continue;
+    const uint32_t start = d->key_off[need], size = d->key_off[need + 1] - start;
+    const uint64_t off = d->A[hh] & qkb::kOffsetMask;
+    for (uint32_t r = 0; r < size; r += kSpinThreads)
+      tiles.push_back(qk_tile_t{off + r, uint32_t(hh), start + r, std::min<uint32_t>(kSpinThreads, size - r), 0});
+  }
+  h.ntiles = uint32_t(tiles.size());
+  h.smem = size_t(d->nA) * 4 + size_t(d->nB) * 2;
+  if (h.smem > 160 * 1024) return nullptr;
+  auto* out = new SpinHandle;
+  auto up = [&](int slot, const void* src, size_t bytes) {
+    if (cudaMalloc(&out->bufs[slot], bytes) != cudaSuccess) return false;
+    *dev_bytes += bytes;
+    return cudaMemcpy(out->bufs[slot], src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+  };
+  bool ok = up(0, A32.data(), A32.size() * 4) && up(1, B16.data(), B16.size() * 2) &&
+            up(2, l16.data(), l16.size() * 2) && up(3, tiles.data(), tiles.size() * sizeof(qk_tile_t));
+  if (ok) {
+    h.A32 = static_cast<const uint32_t*>(out->bufs[0]);
+    h.B16 = static_cast<const uint16_t*>(out->bufs[1]);
+    h.lrow = static_cast<const uint16_t*>(out->bufs[2]);
+    h.tiles = static_cast<const qk_tile_t*>(out->bufs[3]);
+    out->host = h;
+    ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
+         cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (ok) *dev_bytes += sizeof(SpinPlan);
+  }
+  if (!ok) {
+    (void)cudaGetLastError();
+    spin_plan_destroy(out);
+    return nullptr;
+  }
+  return out;
+}
+
+int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
+               double* dot_out) {
+  const size_t smem = h->host.smem;
+  const unsigned grid = std::max(1u, std::min<unsigned>(h->host.ntiles, unsigned(sm_count(0)) * 2));
+#define QKD_SPIN_LAUNCH(DT)                                                                             \
+  {                                                                                                     \
+    if (dot_out) {                                                                                      \
+      auto k = k_hx_spin<DT, true>;                                                                     \
+      if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) \
+        return QKD_EINVAL;                                                                              \
+      k<<<std::min<unsigned>(grid, kMaxG), kSpinThreads, smem, s>>>(h->dev, x, y, w->partials, w->ticket, \
+                                                                     dot_out);                          \
+    } else {                                                                                            \
+      auto k = k_hx_spin<DT, false>;                                                                    \
+      if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) \
+        return QKD_EINVAL;                                                                              \
+      k<<<grid, kSpinThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);                      \
+    }                                                                                                   \
+  }
+  switch (t) {
+    case QK_C128: QKD_SPIN_LAUNCH(QK_C128); break;
+    case QK_C64: QKD_SPIN_LAUNCH(QK_C64); break;
+    case QK_F64: QKD_SPIN_LAUNCH(QK_F64); break;
+    case QK_F32: QKD_SPIN_LAUNCH(QK_F32); break;
+    default: return QKD_EINVAL;
+  }
+#undef QKD_SPIN_LAUNCH
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+}  // namespace qkd

@@ -140,3 +140,28 @@ def test_headline_size_properties():
     xh = x.cpu().numpy()
     yo = sample_rows("spin", N, dict(use_sz=1, sz2=0), terms, B, rows, xh)
     assert rel(hx.cpu().numpy()[rows], yo) < 1e-13
+
+
+@pytest.mark.parametrize("N,terms", [(16, O.heisenberg_chain(16)), (18, O.j1j2_chain(18, 1.0, 0.37)),
+                                     (14, [(c * 0.5 if "Sz" in f[0][0] else c, f) for c, f in O.heisenberg_chain(14)]),
+                                     (12, O.heisenberg_chain(12, periodic=False))])
+def test_spin_exchange_kernel_equals_generic(N, terms):
+    """The specialised kernel is selected for exchange models and agrees
+    with the generic kernel and the oracle."""
+    sec = dict(use_sz=1, sz2=0)
+    H = ham("spin", N, sec, terms)
+    assert H.kernel == "spin-exchange"
+    x = np.random.default_rng(N).standard_normal(H.dimension) + 1j * np.random.default_rng(N + 1).standard_normal(H.dimension)
+    y_fast = H.apply(x)
+    qk.set_kernel_policy("generic")
+    try:
+        assert H.kernel == "generic"
+        y_gen = H.apply(x)
+    finally:
+        qk.set_kernel_policy("auto")
+    assert rel(y_fast, y_gen) < 1e-14
+    assert rel(y_fast, O.port().hamiltonian("spin", N, sec, terms).apply(x)) < 1e-13
+    Hf = ham("spin", 10, {}, O.heisenberg_chain(10))      # full basis also qualifies
+    assert Hf.kernel == "spin-exchange"
+    xf = np.random.default_rng(0).standard_normal(Hf.dimension) + 0j
+    assert rel(Hf.apply(xf), O.port().hamiltonian("spin", 10, {}, O.heisenberg_chain(10)).apply(xf)) < 1e-13
