@@ -91,6 +91,15 @@ int qkrylov_hamiltonian_diagonal_complex_f64(qkrylov_hamiltonian_h h, double* di
 int qkrylov_hamiltonian_apply_device(qkrylov_hamiltonian_h h, int dtype, const void* x, void* y, void* stream);
 int qkrylov_hamiltonian_diagonal_device(qkrylov_hamiltonian_h h, int dtype, void* diag, void* stream);
 
+/* ------------------------------------------------------ device vector ops
+ * Multi-vector dot out[2j..2j+1] = <V_j, x> = sum_i conj(V_j[i]) x[i] for
+ * j < k (the reorthogonalisation coefficients of vector_ops.hpp:14-30
+ * `dot`, k at once), FP64 accumulation, deterministic.  V: host array of k
+ * device pointers; x, V_j: n elements of dtype on `device`; out: host
+ * array of 2k doubles.  Runs on the library stream and waits for it. */
+int qkrylov_b200_multi_dot(int device, int dtype, size_t n, int k, const void* const* V, const void* x,
+                           double* out);
+
 /* -------------------------------------------------- double-precision solvers */
 typedef struct {
   double energy;

@@ -198,6 +198,29 @@ int qkrylov_hamiltonian_diagonal_device(qkrylov_hamiltonian_h h, int dtype, void
   });
 }
 
+int qkrylov_b200_multi_dot(int device, int dtype, size_t n, int k, const void* const* V, const void* x,
+                           double* out) {
+  if (device < 0 || !valid_dtype(dtype) || k <= 0 || !V || !x || !out) return QKRYLOV_ERROR_INVALID_ARG;
+  for (int j = 0; j < k; ++j)
+    if (!V[j]) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    auto& c = qkb::Context::get(device);
+    qkb::PtrArray P(size_t(k), device);
+    for (int j = 0; j < k; ++j) P.set(size_t(j), V[j], c.stream);
+    qkb::DevVec res(2 * size_t(k), QK_F64, device, false);
+    constexpr int kChunk = 511;
+    for (int j0 = 0; j0 < k; j0 += kChunk) {
+      const int kk = std::min(kChunk, k - j0);
+      qkb::qkd_check(qkd_update_mdot(c.ws, qk_dtype(dtype), n, 0, nullptr, nullptr, kk, P.at(j0),
+                                     const_cast<void*>(x), static_cast<double*>(res.data()) + 2 * j0, c.stream),
+                     "multi-dot");
+    }
+    qkb::cuda_check(cudaMemcpyAsync(out, res.data(), sizeof(double) * 2 * k, cudaMemcpyDeviceToHost, c.stream), "D2H");
+    c.sync();
+    return QKRYLOV_SUCCESS;
+  });
+}
+
 int qkrylov_lanczos_ground_state_f64(qkrylov_hamiltonian_h h, int maxiter, double tol, const double* start,
                                      qkrylov_lanczos_result_f64_t* result, double* evec, double* alphas,
                                      double* betas) {

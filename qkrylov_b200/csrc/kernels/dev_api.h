@@ -112,6 +112,12 @@ int qkd_normalize_into(qk_dtype t, size_t n, const double* nrm2, const void* x, 
 /* Davidson correction t = r / (diag - lambda) with the reference's clamp. */
 int qkd_dav_precond(qk_dtype t, size_t n, const void* diag, double lambda, const void* r, void* out,
                     cudaStream_t s);
+/* Seeded counter-based random vector: kind 0 uniform in [-1, 1) (real and
+ * imaginary parts), kind 1 Rademacher +-1 (real). */
+int qkd_random(qk_dtype t, size_t n, uint64_t seed, int kind, void* x, cudaStream_t s);
+/* x (dtype tx) = sum_{j<k} c_j V_j (dtype tv), c: 2k device doubles. */
+int qkd_combine(qk_dtype tv, size_t n, int k, const void* const* V, const double* c, qk_dtype tx, void* x,
+                cudaStream_t s);
 /* Device scratch of the workspace: 2*kMaxK+16 doubles for small results. */
 double* qkd_workspace_results(qk_workspace* w);
 

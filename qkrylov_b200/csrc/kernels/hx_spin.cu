@@ -37,6 +37,16 @@ struct SpinPlan {
   int L, H;
   uint64_t dim;
   int nbonds, ndiag;
+  // bond classes for the warp-tile kernel
+  int nlow, nhigh, ncross, ndcross;
+  uint32_t low_mask[kMaxBonds], high_mask[kMaxBonds], cross_lo[kMaxBonds], cross_hi[kMaxBonds];
+  uint8_t low_i[kMaxBonds], high_i[kMaxBonds], cross_li[kMaxBonds];
+  double low_c01[kMaxBonds], low_c10[kMaxBonds], high_c01[kMaxBonds], high_c10[kMaxBonds];
+  double cross_c01[kMaxBonds], cross_c10[kMaxBonds];   // c01: low bit 0 / high bit 1
+  uint32_t dcross_mask[kMaxDiag];
+  double dcross_w[kMaxDiag];
+  const double* dhi;     // 2^H: diagonal terms inside the high part
+  const double* dlo;     // aligned with llist: diagonal terms inside the low part
   SpinBond bonds[kMaxBonds];
   uint32_t diag_smask[kMaxDiag];
   double diag_w[kMaxDiag];
@@ -140,12 +150,118 @@ k_hx_spin(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __r
   }
 }
 
+// Warp-tile kernel for charge-conserving exchange bonds (only the 01 <-> 10
+// combinations are valid).  A warp owns 32 consecutive rows of one sector
+// block (lane = row), so the block index h, the diagonal of the high part
+// and the validity and target base of every high bond are warp-uniform; no
+// block-wide barrier is needed after the tables are staged.
+template <int DT, bool DOT>
+__global__ void __launch_bounds__(256)
+k_hx_spin_lean(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
+               double* partials, unsigned* ticket, double* dot_out) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  extern __shared__ __align__(16) unsigned char sm[];
+  const SpinPlan& p = *pp;
+  const int nB = 1 << p.L;
+  const uint64_t dim = p.dim;
+  uint16_t* sB = reinterpret_cast<uint16_t*>(sm);
+  __shared__ uint32_t s_lm[kMaxBonds], s_hm[kMaxBonds], s_clo[kMaxBonds], s_chi[kMaxBonds], s_dm[kMaxDiag];
+  __shared__ uint8_t s_li[kMaxBonds], s_hi[kMaxBonds], s_ci[kMaxBonds];
+  __shared__ R s_l01[kMaxBonds], s_l10[kMaxBonds], s_h01[kMaxBonds], s_h10[kMaxBonds], s_c01[kMaxBonds],
+      s_c10[kMaxBonds], s_dw[kMaxDiag];
+  const int nlow = p.nlow, nhigh = p.nhigh, ncross = p.ncross, ndc = p.ndcross, L = p.L;
+  for (int i = threadIdx.x; i < nB; i += blockDim.x) sB[i] = p.B16[i];
+  for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
+    s_lm[i] = p.low_mask[i]; s_hm[i] = p.high_mask[i]; s_clo[i] = p.cross_lo[i]; s_chi[i] = p.cross_hi[i];
+    s_li[i] = p.low_i[i]; s_hi[i] = p.high_i[i]; s_ci[i] = p.cross_li[i];
+    s_l01[i] = R(p.low_c01[i]); s_l10[i] = R(p.low_c10[i]); s_h01[i] = R(p.high_c01[i]);
+    s_h10[i] = R(p.high_c10[i]); s_c01[i] = R(p.cross_c01[i]); s_c10[i] = R(p.cross_c10[i]);
+  }
+  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { s_dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
+  __syncthreads();
+  const uint32_t* __restrict__ A = p.A32;
+  const int lane = threadIdx.x & 31;
+  const uint32_t wglobal = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  const uint32_t nsub = p.ntiles * (kSpinThreads / 32);  // 32-row sub-tiles of the 512-row tiles
+  double dr = 0.0, di = 0.0;
+  for (uint32_t w = wglobal; w < nsub; w += nwarps) {
+    const qk_tile_t tile = p.tiles[w / (kSpinThreads / 32)];
+    const uint32_t sub = (w % (kSpinThreads / 32)) * 32;
+    if (sub >= tile.count) continue;
+    const uint32_t j = sub + lane;
+    const bool active = j < tile.count;
+    const uint32_t h = tile.h;
+    const uint64_t base = __ldg(A + h);
+    const uint64_t row = tile.row0 + j;
+    const uint64_t rank_in_block = row - base;
+    const uint32_t l = active ? uint32_t(__ldg(p.lrow + tile.lstart + j)) : 0u;
+    R xr0 = R(0), xi0 = R(0);
+    R d = R(0);
+    if (active) {
+      T::ld(x, row, xr0, xi0);
+      d = R(__ldg(p.dhi + h)) + R(__ldg(p.dlo + tile.lstart + j));
+    }
+    const uint32_t s = (h << L) | l;
+    for (int q = 0; q < ndc; ++q) d += (__popc(s & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
+    R yr = d * xr0, yi = d * xi0;
+    if (active) {
+      for (int q = 0; q < nhigh; ++q) {  // warp-uniform
+        const uint32_t m = s_hm[q], v = h & m;
+        if (v == 0 || v == m) continue;
+        const R c = ((v >> s_hi[q]) & 1u) ? s_h10[q] : s_h01[q];
+        const uint64_t col = uint64_t(__ldg(A + (h ^ m))) + rank_in_block;
+        if (col >= dim) continue;  // never taken for charge-conserving bonds; bounds every load
+        R xr, xi;
+        T::ld(x, col, xr, xi);
+        yr += c * xr;
+        if (T::cplx) yi += c * xi;
+      }
+      for (int q = 0; q < nlow; ++q) {
+        const uint32_t m = s_lm[q], v = l & m;
+        if (v == 0 || v == m) continue;
+        const R c = ((v >> s_li[q]) & 1u) ? s_l10[q] : s_l01[q];
+        const uint64_t col = base + sB[l ^ m];
+        if (col >= dim) continue;
+        R xr, xi;
+        T::ld(x, col, xr, xi);
+        yr += c * xr;
+        if (T::cplx) yi += c * xi;
+      }
+      for (int q = 0; q < ncross; ++q) {
+        const uint32_t bl = (l >> s_ci[q]) & 1u, bh = (h & s_chi[q]) ? 1u : 0u;
+        if (bl == bh) continue;
+        const R c = bl ? s_c10[q] : s_c01[q];
+        const uint64_t col = uint64_t(__ldg(A + (h ^ s_chi[q]))) + sB[l ^ s_clo[q]];
+        if (col >= dim) continue;
+        R xr, xi;
+        T::ld(x, col, xr, xi);
+        yr += c * xr;
+        if (T::cplx) yi += c * xi;
+      }
+      T::st(y, row, yr, yi);
+      if (DOT) {
+        dr += double(xr0) * double(yr) + double(xi0) * double(yi);
+        di += double(xr0) * double(yi) - double(xi0) * double(yr);
+      }
+    }
+  }
+  if (DOT) {
+    __shared__ double sbuf[2 * (256 / 32)];
+    block_sum2(dr, di, sbuf);
+    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
+    grid_finish(partials, ticket, 1, dot_out);
+  }
+}
+
 }  // namespace
 
 struct SpinHandle {
   SpinPlan host;
   SpinPlan* dev = nullptr;
-  void* bufs[4] = {nullptr, nullptr, nullptr, nullptr};
+  void* bufs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool lean = false;  // every bond conserves the charge: warp-tile kernel
 };
 
 void spin_plan_destroy(SpinHandle* h) {
@@ -203,6 +319,41 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     }
     h.bonds[h.nbonds++] = b;
   }
+  // Lean classification: only the charge-conserving combinations 01 / 10.
+  bool lean = true;
+  for (int q = 0; q < h.nbonds && lean; ++q) {
+    const SpinBond& b = h.bonds[q];
+    if (b.valid_mask & 0b1001) { lean = false; break; }
+    const uint32_t mi = 1u << b.bi, mj = 1u << b.bj;
+    // c01: bit i = 1, bit j = 0 is combo 1; bit i = 0, bit j = 1 is combo 2
+    if (b.kind == 0) {
+      h.low_mask[h.nlow] = mi | mj; h.low_i[h.nlow] = b.bi;
+      h.low_c10[h.nlow] = b.c[1]; h.low_c01[h.nlow] = b.c[2]; ++h.nlow;
+    } else if (b.kind == 1) {
+      h.high_mask[h.nhigh] = (mi | mj) >> L; h.high_i[h.nhigh] = uint8_t(b.bi - L);
+      h.high_c10[h.nhigh] = b.c[1]; h.high_c01[h.nhigh] = b.c[2]; ++h.nhigh;
+    } else {
+      h.cross_lo[h.ncross] = mi; h.cross_hi[h.ncross] = mj >> L; h.cross_li[h.ncross] = b.bi;
+      // valid when bit i (low) != bit j (high); c10: low bit set
+      h.cross_c10[h.ncross] = b.c[1]; h.cross_c01[h.ncross] = b.c[2]; ++h.ncross;
+    }
+  }
+  std::vector<double> dhi(d->nA, 0.0), dlo(d->nllist, 0.0);
+  if (lean) {
+    const uint32_t lowbits = (1u << L) - 1u;
+    for (int q = 0; q < h.ndiag; ++q) {
+      const uint32_t m = h.diag_smask[q];
+      const double w = h.diag_w[q];
+      if ((m & ~lowbits) == 0) {
+        for (uint64_t k = 0; k < d->nllist; ++k) dlo[k] += (__builtin_popcount(d->llist[k] & m) & 1) ? -w : w;
+      } else if ((m & lowbits) == 0) {
+        for (uint64_t k = 0; k < d->nA; ++k) dhi[k] += (__builtin_popcount(uint32_t(k) & (m >> L)) & 1) ? -w : w;
+      } else {
+        h.dcross_mask[h.ndcross] = m; h.dcross_w[h.ndcross] = w; ++h.ndcross;
+      }
+    }
+  }
+
   std::vector<uint32_t> A32(d->nA);
   std::vector<uint16_t> B16(d->nB), l16(d->nllist);
   for (uint64_t k = 0; k < d->nA; ++k) A32[k] = uint32_t(d->A[k] & qkb::kOffsetMask);
@@ -221,18 +372,22 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
   h.smem = size_t(d->nA) * 4 + size_t(d->nB) * 2;
   if (h.smem > 160 * 1024) return nullptr;
   auto* out = new SpinHandle;
+  out->lean = lean;
   auto up = [&](int slot, const void* src, size_t bytes) {
     if (cudaMalloc(&out->bufs[slot], bytes) != cudaSuccess) return false;
     *dev_bytes += bytes;
     return cudaMemcpy(out->bufs[slot], src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
   };
   bool ok = up(0, A32.data(), A32.size() * 4) && up(1, B16.data(), B16.size() * 2) &&
-            up(2, l16.data(), l16.size() * 2) && up(3, tiles.data(), tiles.size() * sizeof(qk_tile_t));
+            up(2, l16.data(), l16.size() * 2) && up(3, tiles.data(), tiles.size() * sizeof(qk_tile_t)) &&
+            up(4, dhi.data(), dhi.size() * 8) && up(5, dlo.data(), dlo.size() * 8);
   if (ok) {
     h.A32 = static_cast<const uint32_t*>(out->bufs[0]);
     h.B16 = static_cast<const uint16_t*>(out->bufs[1]);
     h.lrow = static_cast<const uint16_t*>(out->bufs[2]);
     h.tiles = static_cast<const qk_tile_t*>(out->bufs[3]);
+    h.dhi = static_cast<const double*>(out->bufs[4]);
+    h.dlo = static_cast<const double*>(out->bufs[5]);
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -246,8 +401,34 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
   return out;
 }
 
+int spin_apply_lean(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
+                    qk_workspace* w, double* dot_out) {
+  const size_t smem = size_t(1u << h->host.L) * 2;
+  const unsigned grid = unsigned(sm_count(0)) * 8;
+#define QKD_LEAN_LAUNCH(DT)                                                                              \
+  {                                                                                                      \
+    if (dot_out) {                                                                                       \
+      k_hx_spin_lean<DT, true><<<std::min<unsigned>(grid, kMaxG), 256, smem, s>>>(h->dev, x, y, w->partials, \
+                                                                                  w->ticket, dot_out);    \
+    } else {                                                                                             \
+      k_hx_spin_lean<DT, false><<<grid, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);        \
+    }                                                                                                    \
+  }
+  switch (t) {
+    case QK_C128: QKD_LEAN_LAUNCH(QK_C128); break;
+    case QK_C64: QKD_LEAN_LAUNCH(QK_C64); break;
+    case QK_F64: QKD_LEAN_LAUNCH(QK_F64); break;
+    case QK_F32: QKD_LEAN_LAUNCH(QK_F32); break;
+    default: return QKD_EINVAL;
+  }
+#undef QKD_LEAN_LAUNCH
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out) {
+  if (h->lean) return spin_apply_lean(h, t, x, y, s, w, dot_out);
   const size_t smem = h->host.smem;
   const unsigned grid = std::max(1u, std::min<unsigned>(h->host.ntiles, unsigned(sm_count(0)) * 2));
 #define QKD_SPIN_LAUNCH(DT)                                                                             \

@@ -399,3 +399,79 @@ extern "C" int qkd_dav_precond(qk_dtype t, size_t n, const void* diag, double la
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
+
+// ------------------------------------------------------ device random vectors
+// Counter-based: element i of stream `seed` is a function of (seed, i) only
+// (SplitMix64 finaliser, Steele-Lea-Flood 2014), so a vector is reproducible
+// for any grid shape.
+namespace qkd {
+namespace {
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ double unit_sym(uint64_t r) {  // uniform in [-1, 1)
+  return double(r >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+template <int DT>
+__global__ void k_random(size_t n, uint64_t seed, int kind, void* x) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  const uint64_t key = mix64(seed ^ 0xD1B54A32D192ED03ull);
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    const uint64_t a = mix64(key + 2 * i), b = mix64(key + 2 * i + 1);
+    if (kind == 0) {
+      T::st(x, i, R(unit_sym(a)), R(T::cplx ? unit_sym(b) : 0.0));
+    } else {  // Rademacher +-1 on the real part
+      T::st(x, i, (a >> 63) ? R(-1) : R(1), R(0));
+    }
+  }
+}
+
+// x (DX) = sum_j c_j V_j (DV), FP64 accumulation, x overwritten.
+template <int DV, int DX>
+__global__ void k_combine(size_t n, int k, const void* const* __restrict__ V, const double* __restrict__ c, void* x) {
+  extern __shared__ double sc[];
+  for (int j = threadIdx.x; j < 2 * k; j += blockDim.x) sc[j] = c[j];
+  __syncthreads();
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    double xr = 0.0, xi = 0.0;
+    for (int j = 0; j < k; ++j) {
+      typename VT<DV>::R vr, vi;
+      VT<DV>::ld(V[j], i, vr, vi);
+      xr += sc[2 * j] * double(vr) - sc[2 * j + 1] * double(vi);
+      xi += sc[2 * j] * double(vi) + sc[2 * j + 1] * double(vr);
+    }
+    VT<DX>::st(x, i, typename VT<DX>::R(xr), typename VT<DX>::R(xi));
+  }
+}
+}  // namespace
+}  // namespace qkd
+
+extern "C" int qkd_random(qk_dtype t, size_t n, uint64_t seed, int kind, void* x, cudaStream_t s) {
+  if (n == 0) return QKD_OK;
+  if (!x || kind < 0 || kind > 1) return QKD_EINVAL;
+  QKD_DISPATCH(t, qkd::k_random<DT><<<qkd::stream_grid(n), qkd::kThreads, 0, s>>>(n, seed, kind, x));
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+extern "C" int qkd_combine(qk_dtype tv, size_t n, int k, const void* const* V, const double* c, qk_dtype tx,
+                           void* x, cudaStream_t s) {
+  if (n == 0) return QKD_OK;
+  if (!V || !c || !x || k <= 0 || k > qkd::kMaxK) return QKD_EINVAL;
+  const size_t smem = 2 * size_t(k) * sizeof(double);
+  const unsigned g = qkd::stream_grid(n, 1);
+#define QKD_COMB(A, B)                                                                          \
+  if (tv == A && tx == B) {                                                                     \
+    qkd::k_combine<A, B><<<g, qkd::kThreads, smem, s>>>(n, k, V, c, x);                         \
+    QKD_LAUNCH_CHECK();                                                                         \
+    return QKD_OK;                                                                              \
+  }
+  QKD_COMB(QK_F32, QK_F64) QKD_COMB(QK_F64, QK_F64) QKD_COMB(QK_F32, QK_F32) QKD_COMB(QK_C64, QK_C128)
+  QKD_COMB(QK_C128, QK_C128) QKD_COMB(QK_C64, QK_C64) QKD_COMB(QK_F64, QK_C128) QKD_COMB(QK_F32, QK_C128)
+#undef QKD_COMB
+  return QKD_EINVAL;
+}

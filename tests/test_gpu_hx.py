@@ -165,3 +165,21 @@ def test_spin_exchange_kernel_equals_generic(N, terms):
     assert Hf.kernel == "spin-exchange"
     xf = np.random.default_rng(0).standard_normal(Hf.dimension) + 0j
     assert rel(Hf.apply(xf), O.port().hamiltonian("spin", 10, {}, O.heisenberg_chain(10)).apply(xf)) < 1e-13
+
+
+def test_multi_dot_device():
+    """qkrylov_b200_multi_dot against torch on all dtypes (FP64 accumulation)."""
+    L = qk.lib()
+    rng = np.random.default_rng(9)
+    for code, tdt, tol in [(qk.DTYPE_C128, torch.complex128, 1e-13), (qk.DTYPE_C64, torch.complex64, 1e-6),
+                           (qk.DTYPE_F64, torch.float64, 1e-13), (qk.DTYPE_F32, torch.float32, 1e-6)]:
+        n, k = 300001, 7
+        V = [torch.tensor(rng.standard_normal(n), device="cuda").to(tdt) for _ in range(k)]
+        x = torch.tensor(rng.standard_normal(n), device="cuda").to(tdt)
+        ptrs = (ctypes.c_void_p * k)(*[v.data_ptr() for v in V])
+        out = np.zeros(2 * k)
+        assert L.qkrylov_b200_multi_dot(torch.cuda.current_device(), code, n, k, ptrs, ctypes.c_void_p(x.data_ptr()),
+                                        out.ctypes.data) == 0
+        got = out[0::2] + 1j * out[1::2]
+        want = np.array([torch.vdot(v.to(torch.complex128), x.to(torch.complex128)).item() for v in V])
+        assert np.abs(got - want).max() <= tol * np.abs(want).max() * 10 + 1e-9
