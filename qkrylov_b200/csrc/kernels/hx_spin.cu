@@ -43,6 +43,10 @@ struct SpinPlan {
   uint8_t low_i[kMaxBonds], high_i[kMaxBonds], cross_li[kMaxBonds];
   double low_c01[kMaxBonds], low_c10[kMaxBonds], high_c01[kMaxBonds], high_c10[kMaxBonds];
   double cross_c01[kMaxBonds], cross_c10[kMaxBonds];   // c01: low bit 0 / high bit 1
+  // merged bond list of the batched kernel (any of low / high / crossing)
+  int nall;
+  uint32_t all_lo[kMaxBonds], all_hi[kMaxBonds], all_ilo[kMaxBonds], all_ihi[kMaxBonds];
+  double all_c01[kMaxBonds], all_c10[kMaxBonds];
   uint32_t dcross_mask[kMaxDiag];
   double dcross_w[kMaxDiag];
   const double* dhi;     // 2^H: diagonal terms inside the high part
@@ -255,6 +259,112 @@ k_hx_spin_lean(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
   }
 }
 
+
+// Batched-gather kernel.  For a warp's 32 rows the block index h is fixed,
+// so for every bond the target block base A[h ^ hi] and the high-part
+// popcount are warp-uniform: lane q computes them for bond q once per tile
+// and the warp reads them from its slice of shared memory.  Per row and
+// bond only the low-part rank B[l ^ lo] is a lane-dependent lookup; the
+// bonds are walked four at a time so four gathers are in flight per lane.
+template <int DT, bool DOT>
+__global__ void __launch_bounds__(256)
+k_hx_spin_batched(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
+                  double* partials, unsigned* ticket, double* dot_out) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  extern __shared__ __align__(16) unsigned char sm[];
+  const SpinPlan& p = *pp;
+  const int nB = 1 << p.L;
+  const uint64_t dim = p.dim;
+  uint16_t* sB = reinterpret_cast<uint16_t*>(sm);
+  __shared__ uint32_t s_lo[kMaxBonds], s_ilo[kMaxBonds], s_dm[kMaxDiag];
+  __shared__ R s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
+  __shared__ uint32_t s_wbase[256 / 32][kMaxBonds];   // per warp: A[h ^ hi] of bond q
+  __shared__ uint8_t s_whv[256 / 32][kMaxBonds];      // per warp: popcount(h & hi), bit-i-in-high flag << 4
+  const int nall = p.nall, ndc = p.ndcross, L = p.L;
+  for (int i = threadIdx.x; i < nB; i += blockDim.x) sB[i] = p.B16[i];
+  for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
+    s_lo[i] = p.all_lo[i]; s_ilo[i] = p.all_ilo[i];
+    s_c01[i] = R(p.all_c01[i]); s_c10[i] = R(p.all_c10[i]);
+  }
+  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { s_dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
+  __syncthreads();
+  const uint32_t* __restrict__ A = p.A32;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t wglobal = blockIdx.x * (blockDim.x >> 5) + wib;
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  const uint32_t nsub = p.ntiles * (kSpinThreads / 32);
+  double dr = 0.0, di = 0.0;
+  for (uint32_t w = wglobal; w < nsub; w += nwarps) {
+    const qk_tile_t tile = p.tiles[w / (kSpinThreads / 32)];
+    const uint32_t sub = (w % (kSpinThreads / 32)) * 32;
+    if (sub >= tile.count) continue;
+    const uint32_t h = tile.h;
+    for (int q = lane; q < nall; q += 32) {
+      const uint32_t hm = p.all_hi[q];
+      s_wbase[wib][q] = __ldg(A + (h ^ hm));
+      s_whv[wib][q] = uint8_t(__popc(h & hm) | ((h & p.all_ihi[q]) ? 16u : 0u));
+    }
+    __syncwarp();
+    const uint32_t j = sub + lane;
+    if (j < tile.count) {
+      const uint64_t row = tile.row0 + j;
+      const uint32_t base = __ldg(A + h);
+      const uint32_t r = uint32_t(row - base);
+      const uint32_t l = uint32_t(__ldg(p.lrow + tile.lstart + j));
+      R xr0, xi0;
+      T::ld(x, row, xr0, xi0);
+      R d = R(__ldg(p.dhi + h)) + R(__ldg(p.dlo + tile.lstart + j));
+      const uint32_t st = (h << L) | l;
+      for (int q = 0; q < ndc; ++q) d += (__popc(st & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
+      R yr = d * xr0, yi = d * xi0;
+      for (int q0 = 0; q0 < nall; q0 += 4) {
+        uint64_t col[4];
+        R c[4];
+        bool ok[4];
+        #pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int q = q0 + u;
+          ok[u] = false; col[u] = 0; c[u] = R(0);
+          if (q < nall) {
+            const uint32_t lo = s_lo[q];
+            const uint32_t hv = s_whv[wib][q];
+            const uint32_t nset = __popc(l & lo) + (hv & 15u);
+            const bool iset = (l & s_ilo[q]) || (hv & 16u);
+            ok[u] = (nset == 1u);
+            c[u] = iset ? s_c10[q] : s_c01[q];
+            col[u] = uint64_t(s_wbase[wib][q]) + (lo ? uint32_t(sB[l ^ lo]) : r);
+            ok[u] = ok[u] && col[u] < dim;  // never false for conserving bonds; bounds every load
+          }
+        }
+        R xr[4], xi[4];
+        #pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          xr[u] = R(0); xi[u] = R(0);
+          if (ok[u]) T::ld(x, col[u], xr[u], xi[u]);
+        }
+        #pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          yr += c[u] * xr[u];
+          if (T::cplx) yi += c[u] * xi[u];
+        }
+      }
+      T::st(y, row, yr, yi);
+      if (DOT) {
+        dr += double(xr0) * double(yr) + double(xi0) * double(yi);
+        di += double(xr0) * double(yi) - double(xi0) * double(yr);
+      }
+    }
+    __syncwarp();
+  }
+  if (DOT) {
+    __shared__ double sbuf[2 * (256 / 32)];
+    block_sum2(dr, di, sbuf);
+    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
+    grid_finish(partials, ticket, 1, dot_out);
+  }
+}
+
 }  // namespace
 
 struct SpinHandle {
@@ -336,6 +446,20 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
       h.cross_lo[h.ncross] = mi; h.cross_hi[h.ncross] = mj >> L; h.cross_li[h.ncross] = b.bi;
       // valid when bit i (low) != bit j (high); c10: low bit set
       h.cross_c10[h.ncross] = b.c[1]; h.cross_c01[h.ncross] = b.c[2]; ++h.ncross;
+    }
+  }
+  if (lean) {
+    for (int q = 0; q < h.nbonds; ++q) {
+      const SpinBond& b = h.bonds[q];
+      const uint64_t mi = 1ull << b.bi, mj = 1ull << b.bj, lowbits = (1ull << L) - 1;
+      const uint64_t m = mi | mj;
+      h.all_lo[h.nall] = uint32_t(m & lowbits);
+      h.all_hi[h.nall] = uint32_t(m >> L);
+      h.all_ilo[h.nall] = uint32_t(mi & lowbits);   // bit i (the lower one) in the low part
+      h.all_ihi[h.nall] = uint32_t((mi & ~lowbits) >> L);
+      h.all_c10[h.nall] = b.c[1];                    // bit i set, bit j clear
+      h.all_c01[h.nall] = b.c[2];
+      ++h.nall;
     }
   }
   std::vector<double> dhi(d->nA, 0.0), dlo(d->nllist, 0.0);
@@ -426,9 +550,37 @@ int spin_apply_lean(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
   return QKD_OK;
 }
 
+int spin_apply_batched(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
+                       qk_workspace* w, double* dot_out) {
+  const size_t smem = size_t(1u << h->host.L) * 2;
+  const unsigned grid = unsigned(sm_count(0)) * 8;
+#define QKD_BATCH_LAUNCH(DT)                                                                               \
+  {                                                                                                        \
+    if (dot_out) {                                                                                         \
+      k_hx_spin_batched<DT, true><<<std::min<unsigned>(grid, kMaxG), 256, smem, s>>>(h->dev, x, y, w->partials, \
+                                                                                     w->ticket, dot_out);    \
+    } else {                                                                                               \
+      k_hx_spin_batched<DT, false><<<grid, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);       \
+    }                                                                                                      \
+  }
+  switch (t) {
+    case QK_C128: QKD_BATCH_LAUNCH(QK_C128); break;
+    case QK_C64: QKD_BATCH_LAUNCH(QK_C64); break;
+    case QK_F64: QKD_BATCH_LAUNCH(QK_F64); break;
+    case QK_F32: QKD_BATCH_LAUNCH(QK_F32); break;
+    default: return QKD_EINVAL;
+  }
+#undef QKD_BATCH_LAUNCH
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+static int g_spin_variant = 2;  // 0 tile kernel, 1 warp-tile kernel, 2 batched-gather kernel
+
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out) {
-  if (h->lean) return spin_apply_lean(h, t, x, y, s, w, dot_out);
+  if (h->lean && g_spin_variant == 2) return spin_apply_batched(h, t, x, y, s, w, dot_out);
+  if (h->lean && g_spin_variant == 1) return spin_apply_lean(h, t, x, y, s, w, dot_out);
   const size_t smem = h->host.smem;
   const unsigned grid = std::max(1u, std::min<unsigned>(h->host.ntiles, unsigned(sm_count(0)) * 2));
 #define QKD_SPIN_LAUNCH(DT)                                                                             \
@@ -458,4 +610,12 @@ int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStre
   return QKD_OK;
 }
 
+int spin_set_variant(int v) {
+  if (v < 0 || v > 2) return QKD_EINVAL;
+  g_spin_variant = v;
+  return QKD_OK;
+}
+
 }  // namespace qkd
+
+extern "C" int qkd_set_spin_variant(int v) { return qkd::spin_set_variant(v); }

@@ -153,13 +153,18 @@ def test_spin_exchange_kernel_equals_generic(N, terms):
     assert H.kernel == "spin-exchange"
     x = np.random.default_rng(N).standard_normal(H.dimension) + 1j * np.random.default_rng(N + 1).standard_normal(H.dimension)
     y_fast = H.apply(x)
-    qk.set_kernel_policy("generic")
+    ys = {}
     try:
+        for pol in ("generic", "exchange-block", "exchange-warp"):
+            qk.set_kernel_policy(pol)
+            ys[pol] = H.apply(x)
+        assert H.kernel == "spin-exchange"
+        qk.set_kernel_policy("generic")
         assert H.kernel == "generic"
-        y_gen = H.apply(x)
     finally:
         qk.set_kernel_policy("auto")
-    assert rel(y_fast, y_gen) < 1e-14
+    for pol, y in ys.items():
+        assert rel(y_fast, y) < 1e-14, pol
     assert rel(y_fast, O.port().hamiltonian("spin", N, sec, terms).apply(x)) < 1e-13
     Hf = ham("spin", 10, {}, O.heisenberg_chain(10))      # full basis also qualifies
     assert Hf.kernel == "spin-exchange"
