@@ -101,6 +101,20 @@ int qkrylov_hamiltonian_diagonal_device(qkrylov_hamiltonian_h h, int dtype, void
 int qkrylov_b200_multi_dot(int device, int dtype, size_t n, int k, const void* const* V, const void* x,
                            double* out);
 
+/* qkrylov_b200_multi_dot for callers that cannot let the library allocate
+ * device memory (their memory is owned by another allocator's pool, or an
+ * allocation or free would stall their streams).  No counterpart in the
+ * reference.  Same inputs, output and arithmetic as qkrylov_b200_multi_dot,
+ * issued on `stream` (NULL: the legacy default stream) and waited for; it
+ * calls no cudaMalloc, cudaFree or allocating routine.  All scratch lives in
+ * one fixed device array of about 129 KB per GPU, held until exit: k is
+ * limited to 16 vectors per call (more is rejected with
+ * QKRYLOV_ERROR_INVALID_ARG), calls share the array and must not overlap on
+ * the GPU, and the first call on a device sets the array up (make it before
+ * any stream capture). */
+int qkrylov_b200_multi_dot_noalloc(int device, int dtype, size_t n, int k, const void* const* V, const void* x,
+                                   double* out, void* stream);
+
 /* -------------------------------------------------- double-precision solvers */
 typedef struct {
   double energy;

@@ -90,6 +90,7 @@ PROTOTYPES = {
     "qkrylov_hamiltonian_apply_device": (_i, [_vp, _i, _vp, _vp, _vp]),
     "qkrylov_hamiltonian_diagonal_device": (_i, [_vp, _i, _vp, _vp]),
     "qkrylov_b200_multi_dot": (_i, [_i, _i, _sz, _i, _vp, _vp, _vp]),
+    "qkrylov_b200_multi_dot_noalloc": (_i, [_i, _i, _sz, _i, _vp, _vp, _vp, _vp]),
     "qkrylov_lanczos_ground_state_f64": (_i, [_vp, _i, _d, _vp, _vp, _vp, _vp, _vp]),
     "qkrylov_davidson_lowest_f64": (_i, [_vp, _i, _i, _d, _vp, _vp, _vp]),
     "qkrylov_continued_fraction_coeffs_f64": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
