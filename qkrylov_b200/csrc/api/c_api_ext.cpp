@@ -38,10 +38,11 @@ int qkrylov_b200_device_count(void) {
 }
 
 int qkrylov_b200_set_kernel_policy(int policy) {
-  // 0 auto, 1 generic only, 2 / 3: exchange kernel with block tiles / warp tiles
-  if (policy < 0 || policy > 3) return QKRYLOV_ERROR_INVALID_ARG;
+  // 0 auto, 1 generic only, 2 / 3 / 4: exchange kernel with block tiles /
+  // warp tiles / batched gathers
+  if (policy < 0 || policy > 4) return QKRYLOV_ERROR_INVALID_ARG;
   qkd_set_kernel_policy(policy == 1 ? 1 : 0);
-  qkd_set_spin_variant(policy == 2 ? 0 : policy == 3 ? 1 : 2);
+  qkd_set_spin_variant(policy == 2 ? 0 : policy == 3 ? 1 : policy == 4 ? 2 : 3);
   return QKRYLOV_SUCCESS;
 }
 

@@ -1,6 +1,7 @@
 #include "solvers.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <numeric>
 #include <random>
@@ -173,6 +174,140 @@ LanczosOut<Real> lanczos(const Operator& H, int maxiter, Real tol, const std::co
     d.download<Real>(r, *ritz);
   }
   return res;
+}
+
+
+namespace {
+double now_s() {
+  using clk = std::chrono::steady_clock;
+  return std::chrono::duration<double>(clk::now().time_since_epoch()).count();
+}
+}  // namespace
+
+CoreOut lanczos_core(const Operator& H, qk_dtype T, const void* start, int maxiter, double tol_dE, double tol_res,
+                     qk_dtype tout, void* ritz, double t0) {
+  CoreOut res;
+  const uint64_t dim = H.dim();
+  if (dim == 0) return res;
+  Dev d(H, T);
+  const int lim = int(std::min<uint64_t>(uint64_t(std::max(maxiter, 0)), dim));
+  std::vector<DevVec> V;
+  PtrArray P(size_t(lim) + 3, H.device());
+  DevVec w = d.vec();
+  DevVec coef(size_t(2) * (lim + 4), QK_F64, H.device());
+  double* cd = static_cast<double*>(coef.data());
+  V.push_back(d.vec(false));
+  qkd_check(qkd_copy(T, dim, start, V[0].data(), d.c.stream), "copy");
+  {
+    const double n0 = std::sqrt(d.dot(V[0].data(), V[0].data()).real());
+    if (n0 == 0.0) throw std::invalid_argument("qkrylov_b200: zero start vector");
+    d.scal(1.0 / n0, V[0].data());
+  }
+  P.set(0, V[0].data(), d.c.stream);
+  std::vector<double>& a = res.alphas;
+  std::vector<double>& b = res.betas;
+  double e_old = 1e300;
+  for (int iter = 0; iter < lim; ++iter) {
+    res.iterations = iter + 1;
+    const int k = int(V.size()) - 1;
+    H.apply_dot(T, V[k].data(), w.data(), d.c.dres(0));
+    const double alpha = d.c.fetch(d.c.dres(0), 1)[0];
+    a.push_back(alpha);
+    const void* U[2] = {V[k].data(), k > 0 ? V[k - 1].data() : nullptr};
+    const double co[4] = {alpha, 0.0, k > 0 ? b.back() : 0.0, 0.0};
+    P.set(k + 1, w.data(), d.c.stream);
+    d.update_mdot(k > 0 ? 2 : 1, U, co, P, k + 2, w.data(), cd);
+    d.mupdate(P, k + 1, cd, w.data(), cd + 2 * (k + 2));
+    const double* hh = d.c.fetch(cd + 2 * (k + 1), 4);
+    double after = hh[2];
+    if (after < 0.25 * hh[0]) {
+      d.update_mdot(0, nullptr, nullptr, P, k + 1, w.data(), cd);
+      d.mupdate(P, k + 1, cd, w.data(), cd + 2 * (k + 2));
+      after = d.c.fetch(cd + 2 * (k + 2), 1)[0];
+    }
+    const double beta = std::sqrt(after);
+    std::vector<double> z;
+    const double e = tridiag_ground<double>(a, b, int(a.size()), &z);
+    const double rest = beta * std::abs(z.back());
+    res.trace.push_back({iter + 1, e, now_s() - t0, rest});
+    res.energy = e;
+    res.resid_est = rest;
+    if (beta < 1e-15 || rest <= tol_res * std::abs(e) || (iter > 0 && std::abs(e - e_old) < tol_dE * std::abs(e))) {
+      res.converged = true;
+      break;
+    }
+    e_old = e;
+    if (iter + 1 == lim) break;
+    b.push_back(beta);
+    V.push_back(d.vec(false));
+    d.scale_into(1.0 / beta, w.data(), V.back().data());
+    P.set(k + 1, V.back().data(), d.c.stream);
+  }
+  if (ritz) {
+    std::vector<double> z;
+    const int m = int(a.size());
+    tridiag_ground<double>(a, b, m, &z);
+    std::vector<double> cz(2 * size_t(m), 0.0);
+    for (int i = 0; i < m; ++i) cz[2 * i] = z[i];
+    cuda_check(cudaMemcpyAsync(cd, cz.data(), sizeof(double) * 2 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
+    constexpr int kChunk = 511;
+    // ritz = sum_i z_i V_i assembled in dtype tout (chunks accumulate through
+    // a temporary when m exceeds one launch)
+    if (m <= kChunk) {
+      qkd_check(qkd_combine(T, dim, m, P.data(), cd, tout, ritz, d.c.stream), "combine");
+    } else {
+      throw std::invalid_argument("qkrylov_b200: Ritz assembly over more than 511 vectors is not supported");
+    }
+    Dev dout(H, tout);
+    const double nr = std::sqrt(dout.dot(ritz, ritz).real());
+    if (nr > 0) dout.scal(1.0 / nr, ritz);
+  }
+  return res;
+}
+
+MixedOut lanczos_mixed(const Operator& H, const void* start_low, uint64_t seed, int maxiter, double tol_res,
+                       void* psi_out) {
+  MixedOut out;
+  const uint64_t dim = H.dim();
+  if (dim == 0) return out;
+  const bool real = H.all_real();
+  const qk_dtype lo = real ? QK_F32 : QK_C64, hi = real ? QK_F64 : QK_C128;
+  const double t0 = now_s();
+  Dev dl(H, lo), dh(H, hi);
+  DevVec s0 = dl.vec(false);
+  if (start_low) qkd_check(qkd_copy(lo, dim, start_low, s0.data(), dl.c.stream), "copy");
+  else qkd_check(qkd_random(lo, dim, seed, 0, s0.data(), dl.c.stream), "random");
+  DevVec psi = dh.vec(false);
+  // Phase 1: FP32 vectors until the Ritz value is settled to FP32 accuracy.
+  auto p1 = lanczos_core(H, lo, s0.data(), maxiter, 1e-8, 1e-5, hi, psi.data(), t0);
+  out.iters_low = p1.iterations;
+  out.trace = p1.trace;
+  out.seconds_low = now_s() - t0;
+  // Phase 2: FP64 restarts from the current Ritz vector, each checked by an
+  // explicit FP64 residual.
+  DevVec r = dh.vec(false);
+  PtrArray P(1, H.device());
+  P.set(0, r.data(), dh.c.stream);
+  double e = p1.energy;
+  for (int rs = 0; rs < 8; ++rs) {
+    auto p2 = lanczos_core(H, hi, psi.data(), maxiter, 0.0, 0.1 * tol_res, hi, psi.data(), t0);
+    out.iters_high += p2.iterations;
+    for (auto te : p2.trace) { te.iteration += out.iters_low; out.trace.push_back(te); }
+    e = p2.energy;
+    H.apply(hi, psi.data(), r.data());
+    const void* U[1] = {psi.data()};
+    const double co[2] = {e, 0.0};
+    dh.update_mdot(1, U, co, P, 1, r.data(), dh.c.dres(0));
+    const double rn = std::sqrt(dh.c.fetch(dh.c.dres(0), 1)[0]);
+    out.residual = rn / std::abs(e);
+    out.restarts = rs + 1;
+    if (out.residual <= tol_res) { out.converged = true; break; }
+  }
+  out.energy = e;
+  out.seconds_high = now_s() - t0 - out.seconds_low;
+  if (psi_out) qkd_check(qkd_copy(hi, dim, psi.data(), psi_out, dh.c.stream), "copy");
+  dh.c.sync();
+  return out;
 }
 
 template <class Real>

@@ -59,6 +59,37 @@ template <class Real>
 LanczosOut<Real> lanczos(const Operator& H, int maxiter, Real tol,
                          const std::complex<Real>* start, std::vector<std::complex<Real>>* ritz);
 
+// Lanczos with full reorthogonalisation on device vectors of any dtype,
+// scalars (alpha, beta, reorthogonalisation coefficients, tridiagonal) in
+// FP64 on the host.  `start` (dtype t, dim elements) is copied, not
+// modified.  Stops when |E_k - E_{k-1}| < tol_dE |E_k|, when the residual estimate
+// beta_k |z_k| falls below tol_res * |E_k|, at breakdown, or at maxiter.  If
+// ritz is given it receives the normalised Ritz vector in dtype tout.
+struct TraceEntry { int iteration; double energy; double seconds; double resid_est; };
+struct CoreOut {
+  double energy = 0, resid_est = 0;
+  int iterations = 0;
+  bool converged = false;
+  std::vector<double> alphas, betas;
+  std::vector<TraceEntry> trace;
+};
+CoreOut lanczos_core(const Operator& H, qk_dtype t, const void* start, int maxiter, double tol_dE,
+                     double tol_res, qk_dtype tout, void* ritz, double t0_seconds);
+
+// Mixed precision: phase 1 on FP32 vectors (FP64 scalars), then FP64
+// Lanczos restarted from the FP32 Ritz vector until the explicit FP64
+// residual ||H psi - E psi|| / |E| <= tol_res.  Real operators use real
+// vectors (float32 / float64), complex ones complex64 / complex128.
+struct MixedOut {
+  double energy = 0, residual = 0;
+  int iters_low = 0, iters_high = 0, restarts = 0;
+  bool converged = false;
+  double seconds_low = 0, seconds_high = 0;
+  std::vector<TraceEntry> trace;  // both phases, seconds from the start
+};
+MixedOut lanczos_mixed(const Operator& H, const void* start_low, uint64_t seed, int maxiter, double tol_res,
+                       void* psi_out_high);
+
 // src/solvers/dynamics.cpp:12-59
 template <class Real>
 CFOut<Real> continued_fraction(const Operator& H, const std::complex<Real>* phi0, int n_iter);

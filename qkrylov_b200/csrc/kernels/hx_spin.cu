@@ -47,6 +47,13 @@ struct SpinPlan {
   int nall;
   uint32_t all_lo[kMaxBonds], all_hi[kMaxBonds], all_ilo[kMaxBonds], all_ihi[kMaxBonds];
   double all_c01[kMaxBonds], all_c10[kMaxBonds];
+  // per-part target lists of the list kernel
+  const uint32_t* loff;    // nllist + 1 offsets into lent (by llist position)
+  const uint32_t* lent;    // (in-class rank of l ^ m) << 8 | coefficient index
+  const uint32_t* hoff;    // 2^H + 1 offsets into hent
+  const uint2* hent;       // (A[h ^ m], coefficient index)
+  double coef[2 * kMaxBonds];
+  int ncoef;
   uint32_t dcross_mask[kMaxDiag];
   double dcross_w[kMaxDiag];
   const double* dhi;     // 2^H: diagonal terms inside the high part
@@ -365,12 +372,120 @@ k_hx_spin_batched(const SpinPlan* __restrict__ pp, const void* __restrict__ x, v
   }
 }
 
+
+// List kernel: for each low part l (and each high part h) the valid bond
+// targets are precomputed, so a row visits only the bonds it actually has.
+// Low-bond targets live in a small table shared by every block of the same
+// charge class (rank of l ^ m inside the class); high-bond target bases are
+// per h and warp-uniform.  Crossing bonds (few) are evaluated directly.
+template <int DT, bool DOT>
+__global__ void __launch_bounds__(256)
+k_hx_spin_list(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
+               double* partials, unsigned* ticket, double* dot_out) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  extern __shared__ __align__(16) unsigned char sm[];
+  const SpinPlan& p = *pp;
+  const int nB = 1 << p.L;
+  const uint64_t dim = p.dim;
+  uint16_t* sB = reinterpret_cast<uint16_t*>(sm);
+  __shared__ R s_coef[2 * kMaxBonds];
+  __shared__ uint32_t s_clo[kMaxBonds], s_chi[kMaxBonds], s_dm[kMaxDiag];
+  __shared__ uint8_t s_ci[kMaxBonds];
+  __shared__ R s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
+  __shared__ uint32_t s_cbase[256 / 32][kMaxBonds];
+  const int ncross = p.ncross, ndc = p.ndcross, L = p.L;
+  for (int i = threadIdx.x; i < nB; i += blockDim.x) sB[i] = p.B16[i];
+  for (int i = threadIdx.x; i < 2 * kMaxBonds; i += blockDim.x) s_coef[i] = R(p.coef[i]);
+  for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
+    s_clo[i] = p.cross_lo[i]; s_chi[i] = p.cross_hi[i]; s_ci[i] = p.cross_li[i];
+    s_c01[i] = R(p.cross_c01[i]); s_c10[i] = R(p.cross_c10[i]);
+  }
+  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { s_dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
+  __syncthreads();
+  const uint32_t* __restrict__ A = p.A32;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t wglobal = blockIdx.x * (blockDim.x >> 5) + wib;
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  const uint32_t nsub = p.ntiles * (kSpinThreads / 32);
+  double dr = 0.0, di = 0.0;
+  for (uint32_t w = wglobal; w < nsub; w += nwarps) {
+    const qk_tile_t tile = p.tiles[w / (kSpinThreads / 32)];
+    const uint32_t sub = (w % (kSpinThreads / 32)) * 32;
+    if (sub >= tile.count) continue;
+    const uint32_t h = tile.h;
+    for (int q = lane; q < ncross; q += 32) s_cbase[wib][q] = __ldg(A + (h ^ s_chi[q]));
+    __syncwarp();
+    const uint32_t hbeg = __ldg(p.hoff + h), hend = __ldg(p.hoff + h + 1);
+    const uint32_t j = sub + lane;
+    if (j < tile.count) {
+      const uint64_t row = tile.row0 + j;
+      const uint32_t base = __ldg(A + h);
+      const uint32_t r = uint32_t(row - base);
+      const uint32_t pos = tile.lstart + j;
+      const uint32_t l = uint32_t(__ldg(p.lrow + pos));
+      R xr0, xi0;
+      T::ld(x, row, xr0, xi0);
+      R d = R(__ldg(p.dhi + h)) + R(__ldg(p.dlo + pos));
+      const uint32_t st = (h << L) | l;
+      for (int q = 0; q < ndc; ++q) d += (__popc(st & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
+      R yr = d * xr0, yi = d * xi0;
+      // high bonds: warp-uniform list, consecutive lanes gather consecutive rows
+      for (uint32_t e = hbeg; e < hend; ++e) {
+        const uint2 ent = __ldg(p.hent + e);
+        const uint64_t col = uint64_t(ent.x) + r;
+        if (col >= dim) continue;  // never taken; bounds every load
+        R xr, xi;
+        T::ld(x, col, xr, xi);
+        const R c = s_coef[ent.y];
+        yr += c * xr;
+        if (T::cplx) yi += c * xi;
+      }
+      // low bonds: the row's own list
+      const uint32_t lbeg = __ldg(p.loff + pos), lend = __ldg(p.loff + pos + 1);
+      for (uint32_t e = lbeg; e < lend; ++e) {
+        const uint32_t ent = __ldg(p.lent + e);
+        const uint64_t col = uint64_t(base) + (ent >> 8);
+        if (col >= dim) continue;
+        R xr, xi;
+        T::ld(x, col, xr, xi);
+        const R c = s_coef[ent & 0xFFu];
+        yr += c * xr;
+        if (T::cplx) yi += c * xi;
+      }
+      for (int q = 0; q < ncross; ++q) {
+        const uint32_t bl = (l >> s_ci[q]) & 1u, bh = (h & s_chi[q]) ? 1u : 0u;
+        if (bl == bh) continue;
+        const R c = bl ? s_c10[q] : s_c01[q];
+        const uint64_t col = uint64_t(s_cbase[wib][q]) + sB[l ^ s_clo[q]];
+        if (col >= dim) continue;
+        R xr, xi;
+        T::ld(x, col, xr, xi);
+        yr += c * xr;
+        if (T::cplx) yi += c * xi;
+      }
+      T::st(y, row, yr, yi);
+      if (DOT) {
+        dr += double(xr0) * double(yr) + double(xi0) * double(yi);
+        di += double(xr0) * double(yi) - double(xi0) * double(yr);
+      }
+    }
+    __syncwarp();
+  }
+  if (DOT) {
+    __shared__ double sbuf[2 * (256 / 32)];
+    block_sum2(dr, di, sbuf);
+    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
+    grid_finish(partials, ticket, 1, dot_out);
+  }
+}
+
 }  // namespace
 
 struct SpinHandle {
   SpinPlan host;
   SpinPlan* dev = nullptr;
-  void* bufs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  void* bufs[10] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool lean = false;  // every bond conserves the charge: warp-tile kernel
 };
 
@@ -478,6 +593,43 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     }
   }
 
+  // coefficient table and per-part target lists (list kernel)
+  std::vector<uint32_t> loff, lent, hoff;
+  std::vector<uint2> hent;
+  if (lean) {
+    auto coef_index = [&](double c) -> uint32_t {
+      for (int k = 0; k < h.ncoef; ++k) if (h.coef[k] == c) return uint32_t(k);
+      h.coef[h.ncoef] = c;
+      return uint32_t(h.ncoef++);
+    };
+    loff.assign(d->nllist + 1, 0);
+    for (uint64_t pos = 0; pos < d->nllist; ++pos) {
+      const uint32_t l = d->llist[pos];
+      loff[pos] = uint32_t(lent.size());
+      for (int q = 0; q < h.nlow; ++q) {
+        const uint32_t m = h.low_mask[q], v = l & m;
+        if (v == 0 || v == m) continue;
+        const double c = ((v >> h.low_i[q]) & 1u) ? h.low_c10[q] : h.low_c01[q];
+        lent.push_back(((d->B[l ^ m] & 0xFFFFu) << 8) | coef_index(c));
+      }
+    }
+    loff[d->nllist] = uint32_t(lent.size());
+    hoff.assign(d->nA + 1, 0);
+    for (uint64_t hh = 0; hh < d->nA; ++hh) {
+      hoff[hh] = uint32_t(hent.size());
+      if (uint32_t(d->A[hh] >> 56) == qkb::kEmptyBlockKey) continue;
+      for (int q = 0; q < h.nhigh; ++q) {
+        const uint32_t m = h.high_mask[q], v = uint32_t(hh) & m;
+        if (v == 0 || v == m) continue;
+        const double c = ((v >> h.high_i[q]) & 1u) ? h.high_c10[q] : h.high_c01[q];
+        hent.push_back(make_uint2(uint32_t(d->A[hh ^ m] & qkb::kOffsetMask), coef_index(c)));
+      }
+    }
+    hoff[d->nA] = uint32_t(hent.size());
+    if (lent.empty()) lent.push_back(0);
+    if (hent.empty()) hent.push_back(make_uint2(0, 0));
+  }
+
   std::vector<uint32_t> A32(d->nA);
   std::vector<uint16_t> B16(d->nB), l16(d->nllist);
   for (uint64_t k = 0; k < d->nA; ++k) A32[k] = uint32_t(d->A[k] & qkb::kOffsetMask);
@@ -504,7 +656,9 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
   };
   bool ok = up(0, A32.data(), A32.size() * 4) && up(1, B16.data(), B16.size() * 2) &&
             up(2, l16.data(), l16.size() * 2) && up(3, tiles.data(), tiles.size() * sizeof(qk_tile_t)) &&
-            up(4, dhi.data(), dhi.size() * 8) && up(5, dlo.data(), dlo.size() * 8);
+            up(4, dhi.data(), dhi.size() * 8) && up(5, dlo.data(), dlo.size() * 8) &&
+            (!lean || (up(6, loff.data(), loff.size() * 4) && up(7, lent.data(), lent.size() * 4) &&
+                       up(8, hoff.data(), hoff.size() * 4) && up(9, hent.data(), hent.size() * sizeof(uint2))));
   if (ok) {
     h.A32 = static_cast<const uint32_t*>(out->bufs[0]);
     h.B16 = static_cast<const uint16_t*>(out->bufs[1]);
@@ -512,6 +666,10 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.tiles = static_cast<const qk_tile_t*>(out->bufs[3]);
     h.dhi = static_cast<const double*>(out->bufs[4]);
     h.dlo = static_cast<const double*>(out->bufs[5]);
+    h.loff = static_cast<const uint32_t*>(out->bufs[6]);
+    h.lent = static_cast<const uint32_t*>(out->bufs[7]);
+    h.hoff = static_cast<const uint32_t*>(out->bufs[8]);
+    h.hent = static_cast<const uint2*>(out->bufs[9]);
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -575,10 +733,36 @@ int spin_apply_batched(const SpinHandle* h, qk_dtype t, const void* x, void* y, 
   return QKD_OK;
 }
 
-static int g_spin_variant = 2;  // 0 tile kernel, 1 warp-tile kernel, 2 batched-gather kernel
+int spin_apply_list(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
+                    qk_workspace* w, double* dot_out) {
+  const size_t smem = size_t(1u << h->host.L) * 2;
+  const unsigned grid = unsigned(sm_count(0)) * 8;
+#define QKD_LIST_LAUNCH(DT)                                                                              \
+  {                                                                                                      \
+    if (dot_out) {                                                                                       \
+      k_hx_spin_list<DT, true><<<std::min<unsigned>(grid, kMaxG), 256, smem, s>>>(h->dev, x, y, w->partials, \
+                                                                                  w->ticket, dot_out);    \
+    } else {                                                                                             \
+      k_hx_spin_list<DT, false><<<grid, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);        \
+    }                                                                                                    \
+  }
+  switch (t) {
+    case QK_C128: QKD_LIST_LAUNCH(QK_C128); break;
+    case QK_C64: QKD_LIST_LAUNCH(QK_C64); break;
+    case QK_F64: QKD_LIST_LAUNCH(QK_F64); break;
+    case QK_F32: QKD_LIST_LAUNCH(QK_F32); break;
+    default: return QKD_EINVAL;
+  }
+#undef QKD_LIST_LAUNCH
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+static int g_spin_variant = 3;  // 0 block tiles, 1 warp tiles, 2 batched gathers, 3 target lists
 
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out) {
+  if (h->lean && g_spin_variant == 3) return spin_apply_list(h, t, x, y, s, w, dot_out);
   if (h->lean && g_spin_variant == 2) return spin_apply_batched(h, t, x, y, s, w, dot_out);
   if (h->lean && g_spin_variant == 1) return spin_apply_lean(h, t, x, y, s, w, dot_out);
   const size_t smem = h->host.smem;
@@ -611,7 +795,7 @@ int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStre
 }
 
 int spin_set_variant(int v) {
-  if (v < 0 || v > 2) return QKD_EINVAL;
+  if (v < 0 || v > 3) return QKD_EINVAL;
   g_spin_variant = v;
   return QKD_OK;
 }
