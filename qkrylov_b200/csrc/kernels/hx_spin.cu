@@ -52,6 +52,8 @@ struct SpinPlan {
   const uint32_t* lent;    // (in-class rank of l ^ m) << 8 | coefficient index
   const uint32_t* hoff;    // 2^H + 1 offsets into hent
   const uint2* hent;       // (A[h ^ m], coefficient index)
+  const uint32_t* hlst;    // 2^H: llist position of block h's first low part
+  uint32_t max_block;      // largest block size
   double coef[2 * kMaxBonds];
   int ncoef;
   uint32_t dcross_mask[kMaxDiag];
@@ -480,12 +482,115 @@ k_hx_spin_list(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
   }
 }
 
+
+// Block-staged list kernel: one CTA owns a whole sector block h at a time.
+// It stages x_h in shared memory, so every low-bond gather (targets inside
+// the block) is a shared-memory load; high-bond targets are whole rows of
+// other blocks at the same in-block rank, read coalesced from global; the
+// few crossing bonds gather from global.
+template <int DT, bool DOT>
+__global__ void __launch_bounds__(256)
+k_hx_spin_staged(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
+                 double* partials, unsigned* ticket, double* dot_out) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  extern __shared__ __align__(16) unsigned char sm[];
+  const SpinPlan& p = *pp;
+  const int nB = 1 << p.L;
+  const uint64_t dim = p.dim;
+  uint16_t* sB = reinterpret_cast<uint16_t*>(sm);
+  R* sxr = reinterpret_cast<R*>(sm + ((size_t(nB) * 2 + 15) & ~size_t(15)));
+  R* sxi = sxr + p.max_block;
+  __shared__ R s_coef[2 * kMaxBonds];
+  __shared__ uint32_t s_clo[kMaxBonds], s_chi[kMaxBonds], s_dm[kMaxDiag], s_cbase[kMaxBonds];
+  __shared__ uint8_t s_ci[kMaxBonds];
+  __shared__ R s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
+  const int ncross = p.ncross, ndc = p.ndcross, L = p.L;
+  for (int i = threadIdx.x; i < nB; i += blockDim.x) sB[i] = p.B16[i];
+  for (int i = threadIdx.x; i < 2 * kMaxBonds; i += blockDim.x) s_coef[i] = R(p.coef[i]);
+  for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
+    s_clo[i] = p.cross_lo[i]; s_chi[i] = p.cross_hi[i]; s_ci[i] = p.cross_li[i];
+    s_c01[i] = R(p.cross_c01[i]); s_c10[i] = R(p.cross_c10[i]);
+  }
+  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { s_dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
+  const uint32_t* __restrict__ A = p.A32;
+  const uint32_t nA = 1u << p.H;
+  double dr = 0.0, di = 0.0;
+  for (uint32_t h = blockIdx.x; h < nA; h += gridDim.x) {
+    const uint32_t base = __ldg(A + h);
+    const uint32_t size = (h + 1 < nA ? __ldg(A + h + 1) : uint32_t(dim)) - base;
+    if (size == 0) continue;
+    __syncthreads();  // previous block's readers are done with sx
+    for (uint32_t r = threadIdx.x; r < size; r += blockDim.x) {
+      R xr, xi;
+      T::ld(x, uint64_t(base) + r, xr, xi);
+      sxr[r] = xr;
+      if (T::cplx) sxi[r] = xi;
+    }
+    for (int q = threadIdx.x; q < ncross; q += blockDim.x) s_cbase[q] = __ldg(A + (h ^ s_chi[q]));
+    __syncthreads();
+    const uint32_t hbeg = __ldg(p.hoff + h), hend = __ldg(p.hoff + h + 1);
+    const uint32_t lst = __ldg(p.hlst + h);
+    const R dh = R(__ldg(p.dhi + h));
+    for (uint32_t r = threadIdx.x; r < size; r += blockDim.x) {
+      const uint32_t pos = lst + r;
+      const uint32_t l = uint32_t(__ldg(p.lrow + pos));
+      const R xr0 = sxr[r], xi0 = T::cplx ? sxi[r] : R(0);
+      R d = dh + R(__ldg(p.dlo + pos));
+      const uint32_t st = (h << L) | l;
+      for (int q = 0; q < ndc; ++q) d += (__popc(st & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
+      R yr = d * xr0, yi = d * xi0;
+      for (uint32_t e = hbeg; e < hend; ++e) {
+        const uint2 ent = __ldg(p.hent + e);
+        const uint64_t col = uint64_t(ent.x) + r;
+        if (col >= dim) continue;  // never taken; bounds every load
+        R xr, xi;
+        T::ld(x, col, xr, xi);
+        const R c = s_coef[ent.y];
+        yr += c * xr;
+        if (T::cplx) yi += c * xi;
+      }
+      const uint32_t lbeg = __ldg(p.loff + pos), lend = __ldg(p.loff + pos + 1);
+      for (uint32_t e = lbeg; e < lend; ++e) {
+        const uint32_t ent = __ldg(p.lent + e);
+        const uint32_t k = ent >> 8;
+        if (k >= size) continue;
+        const R c = s_coef[ent & 0xFFu];
+        yr += c * sxr[k];
+        if (T::cplx) yi += c * sxi[k];
+      }
+      for (int q = 0; q < ncross; ++q) {
+        const uint32_t bl = (l >> s_ci[q]) & 1u, bh = (h & s_chi[q]) ? 1u : 0u;
+        if (bl == bh) continue;
+        const R c = bl ? s_c10[q] : s_c01[q];
+        const uint64_t col = uint64_t(s_cbase[q]) + sB[l ^ s_clo[q]];
+        if (col >= dim) continue;
+        R xr, xi;
+        T::ld(x, col, xr, xi);
+        yr += c * xr;
+        if (T::cplx) yi += c * xi;
+      }
+      T::st(y, uint64_t(base) + r, yr, yi);
+      if (DOT) {
+        dr += double(xr0) * double(yr) + double(xi0) * double(yi);
+        di += double(xr0) * double(yi) - double(xi0) * double(yr);
+      }
+    }
+  }
+  if (DOT) {
+    __shared__ double sbuf[2 * (256 / 32)];
+    block_sum2(dr, di, sbuf);
+    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
+    grid_finish(partials, ticket, 1, dot_out);
+  }
+}
+
 }  // namespace
 
 struct SpinHandle {
   SpinPlan host;
   SpinPlan* dev = nullptr;
-  void* bufs[10] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  void* bufs[11] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool lean = false;  // every bond conserves the charge: warp-tile kernel
 };
 
@@ -594,7 +699,7 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
   }
 
   // coefficient table and per-part target lists (list kernel)
-  std::vector<uint32_t> loff, lent, hoff;
+  std::vector<uint32_t> loff, lent, hoff, hlst;
   std::vector<uint2> hent;
   if (lean) {
     auto coef_index = [&](double c) -> uint32_t {
@@ -626,6 +731,13 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
       }
     }
     hoff[d->nA] = uint32_t(hent.size());
+    hlst.assign(d->nA, 0);
+    for (uint64_t hh = 0; hh < d->nA; ++hh) {
+      const uint32_t need = uint32_t(d->A[hh] >> 56);
+      if (need == qkb::kEmptyBlockKey) continue;
+      hlst[hh] = d->key_off[need];
+      h.max_block = std::max<uint32_t>(h.max_block, d->key_off[need + 1] - d->key_off[need]);
+    }
     if (lent.empty()) lent.push_back(0);
     if (hent.empty()) hent.push_back(make_uint2(0, 0));
   }
@@ -658,7 +770,8 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
             up(2, l16.data(), l16.size() * 2) && up(3, tiles.data(), tiles.size() * sizeof(qk_tile_t)) &&
             up(4, dhi.data(), dhi.size() * 8) && up(5, dlo.data(), dlo.size() * 8) &&
             (!lean || (up(6, loff.data(), loff.size() * 4) && up(7, lent.data(), lent.size() * 4) &&
-                       up(8, hoff.data(), hoff.size() * 4) && up(9, hent.data(), hent.size() * sizeof(uint2))));
+                       up(8, hoff.data(), hoff.size() * 4) && up(9, hent.data(), hent.size() * sizeof(uint2)) &&
+                       up(10, hlst.data(), hlst.size() * 4)));
   if (ok) {
     h.A32 = static_cast<const uint32_t*>(out->bufs[0]);
     h.B16 = static_cast<const uint16_t*>(out->bufs[1]);
@@ -670,6 +783,7 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.lent = static_cast<const uint32_t*>(out->bufs[7]);
     h.hoff = static_cast<const uint32_t*>(out->bufs[8]);
     h.hent = static_cast<const uint2*>(out->bufs[9]);
+    h.hlst = static_cast<const uint32_t*>(out->bufs[10]);
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -758,11 +872,63 @@ int spin_apply_list(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
   return QKD_OK;
 }
 
-static int g_spin_variant = 3;  // 0 block tiles, 1 warp tiles, 2 batched gathers, 3 target lists
+int spin_apply_staged(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
+                      qk_workspace* w, double* dot_out) {
+  const size_t es = (t == QK_C128 || t == QK_F64) ? 8 : 4;
+  const size_t planes = (t == QK_C128 || t == QK_C64) ? 2 : 1;
+  const size_t smem = ((size_t(1u << h->host.L) * 2 + 15) & ~size_t(15)) + es * planes * h->host.max_block;
+  if (smem > 200 * 1024) return QKD_EINVAL;
+  // Persistent grid: exactly the CTAs that fit at once (a second wave would
+  // only start after the first finished its whole share).
+  auto resident = [&](auto kern) {
+    int nb = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 256, smem) != cudaSuccess || nb < 1) {
+      (void)cudaGetLastError();
+      nb = 1;
+    }
+    return unsigned(nb);
+  };
+  unsigned per_sm = 1;
+  switch (t) {
+    case QK_C128: per_sm = resident(k_hx_spin_staged<QK_C128, true>); break;
+    case QK_C64: per_sm = resident(k_hx_spin_staged<QK_C64, true>); break;
+    case QK_F64: per_sm = resident(k_hx_spin_staged<QK_F64, true>); break;
+    default: per_sm = resident(k_hx_spin_staged<QK_F32, true>); break;
+  }
+  const unsigned grid = std::min<unsigned>(1u << h->host.H, unsigned(sm_count(0)) * per_sm);
+#define QKD_STAGED_LAUNCH(DT)                                                                             \
+  {                                                                                                       \
+    auto kd = k_hx_spin_staged<DT, true>;                                                                 \
+    auto kn = k_hx_spin_staged<DT, false>;                                                                \
+    if (cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||  \
+        cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)    \
+      return QKD_EINVAL;                                                                                  \
+    if (dot_out) kd<<<std::min<unsigned>(grid, kMaxG), 256, smem, s>>>(h->dev, x, y, w->partials, w->ticket, \
+                                                                       dot_out);                          \
+    else kn<<<grid, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);                             \
+  }
+  switch (t) {
+    case QK_C128: QKD_STAGED_LAUNCH(QK_C128); break;
+    case QK_C64: QKD_STAGED_LAUNCH(QK_C64); break;
+    case QK_F64: QKD_STAGED_LAUNCH(QK_F64); break;
+    case QK_F32: QKD_STAGED_LAUNCH(QK_F32); break;
+    default: return QKD_EINVAL;
+  }
+#undef QKD_STAGED_LAUNCH
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+static int g_spin_variant = 4;  // 0 block tiles, 1 warp tiles, 2 batched gathers, 3 target lists, 4 staged blocks
 
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out) {
-  if (h->lean && g_spin_variant == 3) return spin_apply_list(h, t, x, y, s, w, dot_out);
+  if (h->lean && g_spin_variant == 4) {
+    const int rc = spin_apply_staged(h, t, x, y, s, w, dot_out);
+    if (rc != QKD_EINVAL) return rc;  // block too large for shared memory: use the list kernel
+  }
+  if (h->lean && g_spin_variant >= 3) return spin_apply_list(h, t, x, y, s, w, dot_out);
   if (h->lean && g_spin_variant == 2) return spin_apply_batched(h, t, x, y, s, w, dot_out);
   if (h->lean && g_spin_variant == 1) return spin_apply_lean(h, t, x, y, s, w, dot_out);
   const size_t smem = h->host.smem;
@@ -795,7 +961,7 @@ int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStre
 }
 
 int spin_set_variant(int v) {
-  if (v < 0 || v > 3) return QKD_EINVAL;
+  if (v < 0 || v > 4) return QKD_EINVAL;
   g_spin_variant = v;
   return QKD_OK;
 }
