@@ -191,6 +191,18 @@ def run_b200(args):
         return ms, launches
 
     peak, peak_kind = peaks()
+    if args.kernel_only:
+        qk.set_kernel_policy(args.policy)
+        code, tdt, b = {"c128": (qk.DTYPE_C128, torch.complex128, 32), "c64": (qk.DTYPE_C64, torch.complex64, 16),
+                        "f64": (qk.DTYPE_F64, torch.float64, 16), "f32": (qk.DTYPE_F32, torch.float32, 8)}[args.kernel_dtype]
+        ms, _ = time_apply(code, tdt, b, args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"kernel_only": True, "N": N, "dim": D, "dtype": args.kernel_dtype, "policy": args.policy,
+                              "ms_per_step": ms, "GBs_effective": D * b / (ms * 1e-3) / 1e9, "kernel": H.kernel}),
+                  flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     with ClockSampler(local) as clk:
         ms, launches = time_apply(qk.DTYPE_C128, torch.complex128, 32, args.steps, args.warmup)
     if dist:
@@ -199,13 +211,6 @@ def run_b200(args):
         ms = float(t.item())
     bytes_step = D * 32
     value = world * bytes_step / (ms * 1e-3) / 1e9
-    if args.kernel_only:
-        if rank == 0:
-            print(json.dumps({"kernel_only": True, "N": N, "dim": D, "ms_per_step": ms,
-                              "GBs_effective": bytes_step / (ms * 1e-3) / 1e9, "kernel": H.kernel}), flush=True)
-        if dist:
-            dist.destroy_process_group()
-        return
 
     variants = {}
     for name, code, tdt, b in [("c64", qk.DTYPE_C64, torch.complex64, 16), ("f64", qk.DTYPE_F64, torch.float64, 16),
@@ -274,7 +279,10 @@ def main():
     ap.add_argument("--n", type=int, default=28)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel-only", action="store_true",
-                    help="time only the complex128 device apply (profiling runs)")
+                    help="time only the device apply (profiling runs)")
+    ap.add_argument("--kernel-dtype", default="c128", choices=["c128", "c64", "f64", "f32"],
+                    help="vector type of --kernel-only")
+    ap.add_argument("--policy", default="auto", help="H.x kernel policy of --kernel-only (qkrylov_b200.set_kernel_policy)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
