@@ -375,6 +375,70 @@ k_hx_spin_batched(const SpinPlan* __restrict__ pp, const void* __restrict__ x, v
 }
 
 
+
+// Batched gathers of the list kernels: up to kBatch list entries are loaded,
+// then all their x gathers are issued, then accumulated, so kBatch loads are
+// in flight per lane instead of one dependent chain per bond.
+constexpr int kBatch = 8;
+
+template <int DT>
+__device__ __forceinline__ void gather_high(const uint2* __restrict__ hent, uint32_t hbeg, uint32_t hend,
+                                            uint32_t r, uint64_t dim, const void* __restrict__ x,
+                                            const typename VT<DT>::R* coef, typename VT<DT>::R& yr,
+                                            typename VT<DT>::R& yi) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  for (uint32_t e0 = hbeg; e0 < hend; e0 += kBatch) {
+    uint2 ent[kBatch];
+    #pragma unroll
+    for (int u = 0; u < kBatch; ++u) ent[u] = (e0 + u < hend) ? __ldg(hent + e0 + u) : make_uint2(0xFFFFFFFFu, 0u);
+    R xr[kBatch], xi[kBatch];
+    #pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      xr[u] = R(0); xi[u] = R(0);
+      const uint64_t col = uint64_t(ent[u].x) + r;
+      if (e0 + u < hend && col < dim) T::ld(x, col, xr[u], xi[u]);
+    }
+    #pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      if (e0 + u < hend) {
+        const R c = coef[ent[u].y];
+        yr += c * xr[u];
+        if (T::cplx) yi += c * xi[u];
+      }
+    }
+  }
+}
+
+template <int DT>
+__device__ __forceinline__ void gather_low(const uint32_t* __restrict__ lent, uint32_t lbeg, uint32_t lend,
+                                           uint32_t base, uint64_t dim, const void* __restrict__ x,
+                                           const typename VT<DT>::R* coef, typename VT<DT>::R& yr,
+                                           typename VT<DT>::R& yi) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  for (uint32_t e0 = lbeg; e0 < lend; e0 += kBatch) {
+    uint32_t ent[kBatch];
+    #pragma unroll
+    for (int u = 0; u < kBatch; ++u) ent[u] = (e0 + u < lend) ? __ldg(lent + e0 + u) : 0u;
+    R xr[kBatch], xi[kBatch];
+    #pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      xr[u] = R(0); xi[u] = R(0);
+      const uint64_t col = uint64_t(base) + (ent[u] >> 8);
+      if (e0 + u < lend && col < dim) T::ld(x, col, xr[u], xi[u]);
+    }
+    #pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      if (e0 + u < lend) {
+        const R c = coef[ent[u] & 0xFFu];
+        yr += c * xr[u];
+        if (T::cplx) yi += c * xi[u];
+      }
+    }
+  }
+}
+
 // List kernel: for each low part l (and each high part h) the valid bond
 // targets are precomputed, so a row visits only the bonds it actually has.
 // Low-bond targets live in a small table shared by every block of the same
@@ -432,29 +496,12 @@ k_hx_spin_list(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       const uint32_t st = (h << L) | l;
       for (int q = 0; q < ndc; ++q) d += (__popc(st & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
       R yr = d * xr0, yi = d * xi0;
-      // high bonds: warp-uniform list, consecutive lanes gather consecutive rows
-      for (uint32_t e = hbeg; e < hend; ++e) {
-        const uint2 ent = __ldg(p.hent + e);
-        const uint64_t col = uint64_t(ent.x) + r;
-        if (col >= dim) continue;  // never taken; bounds every load
-        R xr, xi;
-        T::ld(x, col, xr, xi);
-        const R c = s_coef[ent.y];
-        yr += c * xr;
-        if (T::cplx) yi += c * xi;
-      }
-      // low bonds: the row's own list
+      // high bonds: warp-uniform list, consecutive lanes gather consecutive
+      // rows; eight entries, then their eight gathers, are in flight at once
+      gather_high<DT>(p.hent, hbeg, hend, r, dim, x, s_coef, yr, yi);
+      // low bonds: the row's own list, batched the same way
       const uint32_t lbeg = __ldg(p.loff + pos), lend = __ldg(p.loff + pos + 1);
-      for (uint32_t e = lbeg; e < lend; ++e) {
-        const uint32_t ent = __ldg(p.lent + e);
-        const uint64_t col = uint64_t(base) + (ent >> 8);
-        if (col >= dim) continue;
-        R xr, xi;
-        T::ld(x, col, xr, xi);
-        const R c = s_coef[ent & 0xFFu];
-        yr += c * xr;
-        if (T::cplx) yi += c * xi;
-      }
+      gather_low<DT>(p.lent, lbeg, lend, base, dim, x, s_coef, yr, yi);
       for (int q = 0; q < ncross; ++q) {
         const uint32_t bl = (l >> s_ci[q]) & 1u, bh = (h & s_chi[q]) ? 1u : 0u;
         if (bl == bh) continue;
@@ -496,17 +543,14 @@ k_hx_spin_staged(const SpinPlan* __restrict__ pp, const void* __restrict__ x, vo
   using R = typename T::R;
   extern __shared__ __align__(16) unsigned char sm[];
   const SpinPlan& p = *pp;
-  const int nB = 1 << p.L;
   const uint64_t dim = p.dim;
-  uint16_t* sB = reinterpret_cast<uint16_t*>(sm);
-  R* sxr = reinterpret_cast<R*>(sm + ((size_t(nB) * 2 + 15) & ~size_t(15)));
+  R* sxr = reinterpret_cast<R*>(sm);
   R* sxi = sxr + p.max_block;
   __shared__ R s_coef[2 * kMaxBonds];
   __shared__ uint32_t s_clo[kMaxBonds], s_chi[kMaxBonds], s_dm[kMaxDiag], s_cbase[kMaxBonds];
   __shared__ uint8_t s_ci[kMaxBonds];
   __shared__ R s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
   const int ncross = p.ncross, ndc = p.ndcross, L = p.L;
-  for (int i = threadIdx.x; i < nB; i += blockDim.x) sB[i] = p.B16[i];
   for (int i = threadIdx.x; i < 2 * kMaxBonds; i += blockDim.x) s_coef[i] = R(p.coef[i]);
   for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
     s_clo[i] = p.cross_lo[i]; s_chi[i] = p.cross_hi[i]; s_ci[i] = p.cross_li[i];
@@ -540,30 +584,27 @@ k_hx_spin_staged(const SpinPlan* __restrict__ pp, const void* __restrict__ x, vo
       const uint32_t st = (h << L) | l;
       for (int q = 0; q < ndc; ++q) d += (__popc(st & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
       R yr = d * xr0, yi = d * xi0;
-      for (uint32_t e = hbeg; e < hend; ++e) {
-        const uint2 ent = __ldg(p.hent + e);
-        const uint64_t col = uint64_t(ent.x) + r;
-        if (col >= dim) continue;  // never taken; bounds every load
-        R xr, xi;
-        T::ld(x, col, xr, xi);
-        const R c = s_coef[ent.y];
-        yr += c * xr;
-        if (T::cplx) yi += c * xi;
-      }
+      gather_high<DT>(p.hent, hbeg, hend, r, dim, x, s_coef, yr, yi);
       const uint32_t lbeg = __ldg(p.loff + pos), lend = __ldg(p.loff + pos + 1);
-      for (uint32_t e = lbeg; e < lend; ++e) {
-        const uint32_t ent = __ldg(p.lent + e);
-        const uint32_t k = ent >> 8;
-        if (k >= size) continue;
-        const R c = s_coef[ent & 0xFFu];
-        yr += c * sxr[k];
-        if (T::cplx) yi += c * sxi[k];
+      for (uint32_t e0 = lbeg; e0 < lend; e0 += kBatch) {
+        uint32_t ent[kBatch];
+        #pragma unroll
+        for (int u = 0; u < kBatch; ++u) ent[u] = (e0 + u < lend) ? __ldg(p.lent + e0 + u) : 0xFFFFFFFFu;
+        #pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+          const uint32_t k = ent[u] >> 8;
+          if (e0 + u < lend && k < size) {
+            const R c = s_coef[ent[u] & 0xFFu];
+            yr += c * sxr[k];
+            if (T::cplx) yi += c * sxi[k];
+          }
+        }
       }
       for (int q = 0; q < ncross; ++q) {
         const uint32_t bl = (l >> s_ci[q]) & 1u, bh = (h & s_chi[q]) ? 1u : 0u;
         if (bl == bh) continue;
         const R c = bl ? s_c10[q] : s_c01[q];
-        const uint64_t col = uint64_t(s_cbase[q]) + sB[l ^ s_clo[q]];
+        const uint64_t col = uint64_t(s_cbase[q]) + __ldg(p.B16 + (l ^ s_clo[q]));
         if (col >= dim) continue;
         R xr, xi;
         T::ld(x, col, xr, xi);
@@ -876,7 +917,7 @@ int spin_apply_staged(const SpinHandle* h, qk_dtype t, const void* x, void* y, c
                       qk_workspace* w, double* dot_out) {
   const size_t es = (t == QK_C128 || t == QK_F64) ? 8 : 4;
   const size_t planes = (t == QK_C128 || t == QK_C64) ? 2 : 1;
-  const size_t smem = ((size_t(1u << h->host.L) * 2 + 15) & ~size_t(15)) + es * planes * h->host.max_block;
+  const size_t smem = es * planes * h->host.max_block;
   if (smem > 200 * 1024) return QKD_EINVAL;
   // Persistent grid: exactly the CTAs that fit at once (a second wave would
   // only start after the first finished its whole share).
