@@ -59,6 +59,20 @@ template <> struct VT<QK_F32> {
 void count_launch();
 int sm_count(int device);
 
+// Grid of a persistent (grid-stride) kernel: exactly the CTAs that are
+// resident at once, so no CTA starts its whole share after another wave.
+template <class K>
+inline unsigned resident_grid(K kernel, int threads, size_t smem, unsigned cap) {
+  int dev = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1) {
+    (void)cudaGetLastError();
+    per_sm = 1;
+  }
+  const unsigned g = unsigned(sm_count(dev)) * unsigned(per_sm);
+  return g < cap ? g : cap;
+}
+
 }  // namespace qkd
 
 #define QKD_LAUNCH_CHECK()                         \

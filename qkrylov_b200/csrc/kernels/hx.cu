@@ -197,9 +197,9 @@ int set_smem(K kernel, size_t smem) {
   return QKD_OK;
 }
 
-unsigned hx_grid(const qk_plan* p) {
-  const unsigned cap = unsigned(sm_count(p->device)) * 8;
-  return std::max(1u, std::min(p->ntiles, cap));
+template <class K>
+unsigned hx_grid(const qk_plan* p, K kernel) {
+  return std::max(1u, resident_grid(kernel, kTile, p->smem, std::max(1u, p->ntiles)));
 }
 
 template <int DT, bool CC>
@@ -209,12 +209,12 @@ int launch_apply(const qk_plan* p, const void* x, void* y, cudaStream_t s, qk_wo
   if (dot_out) {
     auto k = k_hx<DT, CC, true>;
     if (set_smem(k, p->smem)) return QKD_EINVAL;
-    const unsigned g = std::min<unsigned>(hx_grid(p), kMaxG);
+    const unsigned g = std::min<unsigned>(hx_grid(p, k), kMaxG);
     k<<<g, kTile, p->smem, s>>>(d, x, y, w->partials, w->ticket, dot_out);
   } else {
     auto k = k_hx<DT, CC, false>;
     if (set_smem(k, p->smem)) return QKD_EINVAL;
-    k<<<hx_grid(p), kTile, p->smem, s>>>(d, x, y, nullptr, nullptr, nullptr);
+    k<<<hx_grid(p, k), kTile, p->smem, s>>>(d, x, y, nullptr, nullptr, nullptr);
   }
   QKD_LAUNCH_CHECK();
   return QKD_OK;
@@ -329,11 +329,10 @@ int qkd_diagonal(const qk_plan* p, qk_dtype t, void* diag, cudaStream_t s) {
   if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
   if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
   const DevPlan d = dev(p);
-  const unsigned g = hx_grid(p);
   if (p->all_real) {
-    QKD_DISPATCH(t, { auto k = k_diag<DT, false>; if (set_smem(k, p->smem)) return QKD_EINVAL; k<<<g, kTile, p->smem, s>>>(d, diag); });
+    QKD_DISPATCH(t, { auto k = k_diag<DT, false>; if (set_smem(k, p->smem)) return QKD_EINVAL; k<<<hx_grid(p, k), kTile, p->smem, s>>>(d, diag); });
   } else {
-    QKD_DISPATCH(t, { auto k = k_diag<DT, true>; if (set_smem(k, p->smem)) return QKD_EINVAL; k<<<g, kTile, p->smem, s>>>(d, diag); });
+    QKD_DISPATCH(t, { auto k = k_diag<DT, true>; if (set_smem(k, p->smem)) return QKD_EINVAL; k<<<hx_grid(p, k), kTile, p->smem, s>>>(d, diag); });
   }
   QKD_LAUNCH_CHECK();
   return QKD_OK;

@@ -536,7 +536,7 @@ k_hx_spin_list(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
 // other blocks at the same in-block rank, read coalesced from global; the
 // few crossing bonds gather from global.
 template <int DT, bool DOT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k_hx_spin_staged(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
                  double* partials, unsigned* ticket, double* dot_out) {
   using T = VT<DT>;
@@ -841,14 +841,14 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
 int spin_apply_lean(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
                     qk_workspace* w, double* dot_out) {
   const size_t smem = size_t(1u << h->host.L) * 2;
-  const unsigned grid = unsigned(sm_count(0)) * 8;
 #define QKD_LEAN_LAUNCH(DT)                                                                              \
   {                                                                                                      \
     if (dot_out) {                                                                                       \
-      k_hx_spin_lean<DT, true><<<std::min<unsigned>(grid, kMaxG), 256, smem, s>>>(h->dev, x, y, w->partials, \
-                                                                                  w->ticket, dot_out);    \
+      const unsigned g = resident_grid(k_hx_spin_lean<DT, true>, 256, smem, kMaxG);                      \
+      k_hx_spin_lean<DT, true><<<g, 256, smem, s>>>(h->dev, x, y, w->partials, w->ticket, dot_out);      \
     } else {                                                                                             \
-      k_hx_spin_lean<DT, false><<<grid, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);        \
+      const unsigned g = resident_grid(k_hx_spin_lean<DT, false>, 256, smem, 1u << 20);                  \
+      k_hx_spin_lean<DT, false><<<g, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);           \
     }                                                                                                    \
   }
   switch (t) {
@@ -866,14 +866,14 @@ int spin_apply_lean(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
 int spin_apply_batched(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
                        qk_workspace* w, double* dot_out) {
   const size_t smem = size_t(1u << h->host.L) * 2;
-  const unsigned grid = unsigned(sm_count(0)) * 8;
 #define QKD_BATCH_LAUNCH(DT)                                                                               \
   {                                                                                                        \
     if (dot_out) {                                                                                         \
-      k_hx_spin_batched<DT, true><<<std::min<unsigned>(grid, kMaxG), 256, smem, s>>>(h->dev, x, y, w->partials, \
-                                                                                     w->ticket, dot_out);    \
+      const unsigned g = resident_grid(k_hx_spin_batched<DT, true>, 256, smem, kMaxG);                     \
+      k_hx_spin_batched<DT, true><<<g, 256, smem, s>>>(h->dev, x, y, w->partials, w->ticket, dot_out);     \
     } else {                                                                                               \
-      k_hx_spin_batched<DT, false><<<grid, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);       \
+      const unsigned g = resident_grid(k_hx_spin_batched<DT, false>, 256, smem, 1u << 20);                 \
+      k_hx_spin_batched<DT, false><<<g, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);          \
     }                                                                                                      \
   }
   switch (t) {
@@ -891,14 +891,14 @@ int spin_apply_batched(const SpinHandle* h, qk_dtype t, const void* x, void* y, 
 int spin_apply_list(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
                     qk_workspace* w, double* dot_out) {
   const size_t smem = size_t(1u << h->host.L) * 2;
-  const unsigned grid = unsigned(sm_count(0)) * 8;
 #define QKD_LIST_LAUNCH(DT)                                                                              \
   {                                                                                                      \
     if (dot_out) {                                                                                       \
-      k_hx_spin_list<DT, true><<<std::min<unsigned>(grid, kMaxG), 256, smem, s>>>(h->dev, x, y, w->partials, \
-                                                                                  w->ticket, dot_out);    \
+      const unsigned g = resident_grid(k_hx_spin_list<DT, true>, 256, smem, kMaxG);                      \
+      k_hx_spin_list<DT, true><<<g, 256, smem, s>>>(h->dev, x, y, w->partials, w->ticket, dot_out);      \
     } else {                                                                                             \
-      k_hx_spin_list<DT, false><<<grid, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);        \
+      const unsigned g = resident_grid(k_hx_spin_list<DT, false>, 256, smem, 1u << 20);                  \
+      k_hx_spin_list<DT, false><<<g, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);           \
     }                                                                                                    \
   }
   switch (t) {
@@ -973,7 +973,7 @@ int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStre
   if (h->lean && g_spin_variant == 2) return spin_apply_batched(h, t, x, y, s, w, dot_out);
   if (h->lean && g_spin_variant == 1) return spin_apply_lean(h, t, x, y, s, w, dot_out);
   const size_t smem = h->host.smem;
-  const unsigned grid = std::max(1u, std::min<unsigned>(h->host.ntiles, unsigned(sm_count(0)) * 2));
+  const unsigned grid = std::max(1u, std::min<unsigned>(h->host.ntiles, unsigned(sm_count(0)) * 1));
 #define QKD_SPIN_LAUNCH(DT)                                                                             \
   {                                                                                                     \
     if (dot_out) {                                                                                      \
