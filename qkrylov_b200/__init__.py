@@ -548,7 +548,7 @@ def set_kernel_policy(policy: str):
     """'auto' (specialised kernels where eligible), 'generic', or the earlier
     exchange-kernel variants 'exchange-block' / 'exchange-warp'."""
     codes = {"auto": 0, "generic": 1, "exchange-block": 2, "exchange-warp": 3, "exchange-batched": 4,
-             "exchange-list": 5}
+             "exchange-list": 5, "exchange-staged": 6}
     _check(lib().qkrylov_b200_set_kernel_policy(codes[policy]), "set_kernel_policy")
 
 

@@ -626,6 +626,142 @@ k_hx_spin_staged(const SpinPlan* __restrict__ pp, const void* __restrict__ x, vo
   }
 }
 
+
+// Block-owner kernel: a 512-thread CTA owns one sector block h at a time and
+// each thread keeps register accumulators for its rows r = tid + 512 k.
+// x_h is staged in shared memory (all low-bond targets), every valid high
+// bond is a block-wide coalesced AXPY from another block at the same
+// in-block rank with kOwnRows independent loads per thread in flight, and
+// the few crossing bonds gather from global memory.
+constexpr int kOwnThreads = 512;
+constexpr int kOwnRows = 8;  // blocks up to 4096 rows
+
+template <int DT, bool DOT>
+__global__ void __launch_bounds__(kOwnThreads, 2)
+k_hx_spin_owner(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
+                double* partials, unsigned* ticket, double* dot_out) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  extern __shared__ __align__(16) unsigned char sm[];
+  const SpinPlan& p = *pp;
+  const uint64_t dim = p.dim;
+  R* sxr = reinterpret_cast<R*>(sm);
+  R* sxi = sxr + p.max_block;
+  __shared__ R s_coef[2 * kMaxBonds];
+  __shared__ uint32_t s_clo[kMaxBonds], s_chi[kMaxBonds], s_dm[kMaxDiag], s_cbase[kMaxBonds];
+  __shared__ uint8_t s_ci[kMaxBonds];
+  __shared__ R s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
+  __shared__ uint2 s_hent[kMaxBonds];
+  const int ncross = p.ncross, ndc = p.ndcross, L = p.L;
+  for (int i = threadIdx.x; i < 2 * kMaxBonds; i += blockDim.x) s_coef[i] = R(p.coef[i]);
+  for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
+    s_clo[i] = p.cross_lo[i]; s_chi[i] = p.cross_hi[i]; s_ci[i] = p.cross_li[i];
+    s_c01[i] = R(p.cross_c01[i]); s_c10[i] = R(p.cross_c10[i]);
+  }
+  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { s_dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
+  const uint32_t* __restrict__ A = p.A32;
+  const uint32_t nA = 1u << p.H;
+  double dr = 0.0, di = 0.0;
+  for (uint32_t h = blockIdx.x; h < nA; h += gridDim.x) {
+    const uint32_t base = __ldg(A + h);
+    const uint32_t size = (h + 1 < nA ? __ldg(A + h + 1) : uint32_t(dim)) - base;
+    if (size == 0) continue;
+    const uint32_t hbeg = __ldg(p.hoff + h), nh = __ldg(p.hoff + h + 1) - hbeg;
+    __syncthreads();  // the previous block is finished with the staging
+    // stage x_h: kOwnRows independent coalesced loads per thread
+    {
+      R ar[kOwnRows], ai[kOwnRows];
+      #pragma unroll
+      for (int k = 0; k < kOwnRows; ++k) {
+        const uint32_t r = threadIdx.x + k * kOwnThreads;
+        ar[k] = R(0); ai[k] = R(0);
+        if (r < size) T::ld(x, uint64_t(base) + r, ar[k], ai[k]);
+      }
+      #pragma unroll
+      for (int k = 0; k < kOwnRows; ++k) {
+        const uint32_t r = threadIdx.x + k * kOwnThreads;
+        if (r < size) { sxr[r] = ar[k]; if (T::cplx) sxi[r] = ai[k]; }
+      }
+    }
+    for (int q = threadIdx.x; q < ncross; q += blockDim.x) s_cbase[q] = __ldg(A + (h ^ s_chi[q]));
+    for (uint32_t e = threadIdx.x; e < nh && e < uint32_t(kMaxBonds); e += blockDim.x) s_hent[e] = __ldg(p.hent + hbeg + e);
+    __syncthreads();
+    const uint32_t lst = __ldg(p.hlst + h);
+    const R dh = R(__ldg(p.dhi + h));
+    // diagonal, low bonds (shared memory) and crossing bonds, row by row
+    R yr[kOwnRows], yi[kOwnRows];
+    #pragma unroll
+    for (int k = 0; k < kOwnRows; ++k) {
+      const uint32_t r = threadIdx.x + k * kOwnThreads;
+      yr[k] = R(0); yi[k] = R(0);
+      if (r >= size) continue;
+      const uint32_t pos = lst + r;
+      const uint32_t l = uint32_t(__ldg(p.lrow + pos));
+      R d = dh + R(__ldg(p.dlo + pos));
+      const uint32_t st = (h << L) | l;
+      for (int q = 0; q < ndc; ++q) d += (__popc(st & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
+      yr[k] = d * sxr[r];
+      yi[k] = T::cplx ? d * sxi[r] : R(0);
+      const uint32_t lbeg = __ldg(p.loff + pos), lend = __ldg(p.loff + pos + 1);
+      for (uint32_t e = lbeg; e < lend; ++e) {
+        const uint32_t ent = __ldg(p.lent + e);
+        const uint32_t kk = ent >> 8;
+        if (kk >= size) continue;
+        const R c = s_coef[ent & 0xFFu];
+        yr[k] += c * sxr[kk];
+        if (T::cplx) yi[k] += c * sxi[kk];
+      }
+      for (int q = 0; q < ncross; ++q) {
+        const uint32_t bl = (l >> s_ci[q]) & 1u, bh = (h & s_chi[q]) ? 1u : 0u;
+        if (bl == bh) continue;
+        const R c = bl ? s_c10[q] : s_c01[q];
+        const uint64_t col = uint64_t(s_cbase[q]) + __ldg(p.B16 + (l ^ s_clo[q]));
+        if (col >= dim) continue;
+        R xr, xi;
+        T::ld(x, col, xr, xi);
+        yr[k] += c * xr;
+        if (T::cplx) yi[k] += c * xi;
+      }
+    }
+    // high bonds: block-wide AXPYs from other blocks at the same rank
+    for (uint32_t e = 0; e < nh; ++e) {
+      const uint2 ent = (e < uint32_t(kMaxBonds)) ? s_hent[e] : __ldg(p.hent + hbeg + e);
+      const R c = s_coef[ent.y];
+      R xr[kOwnRows], xi[kOwnRows];
+      #pragma unroll
+      for (int k = 0; k < kOwnRows; ++k) {
+        const uint32_t r = threadIdx.x + k * kOwnThreads;
+        xr[k] = R(0); xi[k] = R(0);
+        const uint64_t col = uint64_t(ent.x) + r;
+        if (r < size && col < dim) T::ld(x, col, xr[k], xi[k]);
+      }
+      #pragma unroll
+      for (int k = 0; k < kOwnRows; ++k) {
+        yr[k] += c * xr[k];
+        if (T::cplx) yi[k] += c * xi[k];
+      }
+    }
+    #pragma unroll
+    for (int k = 0; k < kOwnRows; ++k) {
+      const uint32_t r = threadIdx.x + k * kOwnThreads;
+      if (r < size) {
+        T::st(y, uint64_t(base) + r, yr[k], yi[k]);
+        if (DOT) {
+          const double x0r = double(sxr[r]), x0i = T::cplx ? double(sxi[r]) : 0.0;
+          dr += x0r * double(yr[k]) + x0i * double(yi[k]);
+          di += x0r * double(yi[k]) - x0i * double(yr[k]);
+        }
+      }
+    }
+  }
+  if (DOT) {
+    __shared__ double sbuf[2 * (kOwnThreads / 32)];
+    block_sum2(dr, di, sbuf);
+    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
+    grid_finish(partials, ticket, 1, dot_out);
+  }
+}
+
 }  // namespace
 
 struct SpinHandle {
@@ -961,11 +1097,46 @@ int spin_apply_staged(const SpinHandle* h, qk_dtype t, const void* x, void* y, c
   return QKD_OK;
 }
 
-static int g_spin_variant = 4;  // 0 block tiles, 1 warp tiles, 2 batched gathers, 3 target lists, 4 staged blocks
+int spin_apply_owner(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
+                     qk_workspace* w, double* dot_out) {
+  if (h->host.max_block > uint32_t(kOwnThreads * kOwnRows)) return QKD_EINVAL;
+  const size_t es = (t == QK_C128 || t == QK_F64) ? 8 : 4;
+  const size_t planes = (t == QK_C128 || t == QK_C64) ? 2 : 1;
+  const size_t smem = es * planes * h->host.max_block;
+  if (smem > 200 * 1024) return QKD_EINVAL;
+#define QKD_OWNER_LAUNCH(DT)                                                                              \
+  {                                                                                                       \
+    auto kd = k_hx_spin_owner<DT, true>;                                                                  \
+    auto kn = k_hx_spin_owner<DT, false>;                                                                 \
+    if (cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||  \
+        cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)    \
+      return QKD_EINVAL;                                                                                  \
+    const unsigned cap = 1u << h->host.H;                                                                 \
+    if (dot_out) kd<<<resident_grid(kd, kOwnThreads, smem, std::min<unsigned>(cap, kMaxG)), kOwnThreads, smem, s>>>( \
+        h->dev, x, y, w->partials, w->ticket, dot_out);                                                   \
+    else kn<<<resident_grid(kn, kOwnThreads, smem, cap), kOwnThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr); \
+  }
+  switch (t) {
+    case QK_C128: QKD_OWNER_LAUNCH(QK_C128); break;
+    case QK_C64: QKD_OWNER_LAUNCH(QK_C64); break;
+    case QK_F64: QKD_OWNER_LAUNCH(QK_F64); break;
+    case QK_F32: QKD_OWNER_LAUNCH(QK_F32); break;
+    default: return QKD_EINVAL;
+  }
+#undef QKD_OWNER_LAUNCH
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+static int g_spin_variant = 5;  // 0 block tiles, 1 warp tiles, 2 batched, 3 lists, 4 staged, 5 block owner
 
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out) {
-  if (h->lean && g_spin_variant == 4) {
+  if (h->lean && g_spin_variant == 5) {
+    const int rc = spin_apply_owner(h, t, x, y, s, w, dot_out);
+    if (rc != QKD_EINVAL) return rc;
+  }
+  if (h->lean && g_spin_variant >= 4) {
     const int rc = spin_apply_staged(h, t, x, y, s, w, dot_out);
     if (rc != QKD_EINVAL) return rc;  // block too large for shared memory: use the list kernel
   }
@@ -1002,7 +1173,7 @@ int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStre
 }
 
 int spin_set_variant(int v) {
-  if (v < 0 || v > 4) return QKD_EINVAL;
+  if (v < 0 || v > 5) return QKD_EINVAL;
   g_spin_variant = v;
   return QKD_OK;
 }

@@ -155,7 +155,8 @@ def test_spin_exchange_kernel_equals_generic(N, terms):
     y_fast = H.apply(x)
     ys = {}
     try:
-        for pol in ("generic", "exchange-block", "exchange-warp", "exchange-batched", "exchange-list"):
+        for pol in ("generic", "exchange-block", "exchange-warp", "exchange-batched", "exchange-list",
+                    "exchange-staged"):
             qk.set_kernel_policy(pol)
             ys[pol] = H.apply(x)
         assert H.kernel == "spin-exchange"
