@@ -628,13 +628,98 @@ k_hx_spin_staged(const SpinPlan* __restrict__ pp, const void* __restrict__ x, vo
 
 
 // Block-owner kernel: a 512-thread CTA owns one sector block h at a time and
-// each thread keeps register accumulators for its rows r = tid + 512 k.
+// each thread keeps register accumulators for its rows r = tid + 512 k,
+// k < K, with K (1, 2, 4 or 8) the smallest that covers the block.
 // x_h is staged in shared memory (all low-bond targets), every valid high
 // bond is a block-wide coalesced AXPY from another block at the same
-// in-block rank with kOwnRows independent loads per thread in flight, and
-// the few crossing bonds gather from global memory.
+// in-block rank with K independent loads per thread in flight, and the few
+// crossing bonds gather from global memory.
 constexpr int kOwnThreads = 512;
 constexpr int kOwnRows = 8;  // blocks up to 4096 rows
+
+struct OwnShared {
+  uint32_t clo[kMaxBonds], chi[kMaxBonds], dm[kMaxDiag], cbase[kMaxBonds];
+  uint8_t ci[kMaxBonds];
+  uint2 hent[kMaxBonds];
+};
+
+template <int DT, int K>
+__device__ __forceinline__ void own_block(const SpinPlan& p, const OwnShared& S, const typename VT<DT>::R* coef,
+                                          const typename VT<DT>::R* c01, const typename VT<DT>::R* c10,
+                                          const typename VT<DT>::R* dw, const typename VT<DT>::R* sxr,
+                                          const typename VT<DT>::R* sxi, uint32_t h, uint32_t base, uint32_t size,
+                                          uint32_t hbeg, uint32_t nh, const void* __restrict__ x,
+                                          void* __restrict__ y, bool dot, double& dr, double& di) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  const uint64_t dim = p.dim;
+  const int ncross = p.ncross, ndc = p.ndcross, L = p.L;
+  const uint32_t lst = __ldg(p.hlst + h);
+  const R dh = R(__ldg(p.dhi + h));
+  R yr[K], yi[K];
+  #pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const uint32_t r = threadIdx.x + k * kOwnThreads;
+    yr[k] = R(0); yi[k] = R(0);
+    if (r >= size) continue;
+    const uint32_t pos = lst + r;
+    const uint32_t l = uint32_t(__ldg(p.lrow + pos));
+    R d = dh + R(__ldg(p.dlo + pos));
+    const uint32_t st = (h << L) | l;
+    for (int q = 0; q < ndc; ++q) d += (__popc(st & S.dm[q]) & 1) ? -dw[q] : dw[q];
+    yr[k] = d * sxr[r];
+    yi[k] = T::cplx ? d * sxi[r] : R(0);
+    const uint32_t lbeg = __ldg(p.loff + pos), lend = __ldg(p.loff + pos + 1);
+    for (uint32_t e = lbeg; e < lend; ++e) {
+      const uint32_t ent = __ldg(p.lent + e);
+      const uint32_t kk = ent >> 8;
+      if (kk >= size) continue;
+      const R c = coef[ent & 0xFFu];
+      yr[k] += c * sxr[kk];
+      if (T::cplx) yi[k] += c * sxi[kk];
+    }
+    for (int q = 0; q < ncross; ++q) {
+      const uint32_t bl = (l >> S.ci[q]) & 1u, bh = (h & S.chi[q]) ? 1u : 0u;
+      if (bl == bh) continue;
+      const R c = bl ? c10[q] : c01[q];
+      const uint64_t col = uint64_t(S.cbase[q]) + __ldg(p.B16 + (l ^ S.clo[q]));
+      if (col >= dim) continue;
+      R xr, xi;
+      T::ld(x, col, xr, xi);
+      yr[k] += c * xr;
+      if (T::cplx) yi[k] += c * xi;
+    }
+  }
+  for (uint32_t e = 0; e < nh; ++e) {
+    const uint2 ent = (e < uint32_t(kMaxBonds)) ? S.hent[e] : __ldg(p.hent + hbeg + e);
+    const R c = coef[ent.y];
+    R xr[K], xi[K];
+    #pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const uint32_t r = threadIdx.x + k * kOwnThreads;
+      xr[k] = R(0); xi[k] = R(0);
+      const uint64_t col = uint64_t(ent.x) + r;
+      if (r < size && col < dim) T::ld(x, col, xr[k], xi[k]);
+    }
+    #pragma unroll
+    for (int k = 0; k < K; ++k) {
+      yr[k] += c * xr[k];
+      if (T::cplx) yi[k] += c * xi[k];
+    }
+  }
+  #pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const uint32_t r = threadIdx.x + k * kOwnThreads;
+    if (r < size) {
+      T::st(y, uint64_t(base) + r, yr[k], yi[k]);
+      if (dot) {
+        const double x0r = double(sxr[r]), x0i = T::cplx ? double(sxi[r]) : 0.0;
+        dr += x0r * double(yr[k]) + x0i * double(yi[k]);
+        di += x0r * double(yi[k]) - x0i * double(yr[k]);
+      }
+    }
+  }
+}
 
 template <int DT, bool DOT>
 __global__ void __launch_bounds__(kOwnThreads, 2)
@@ -647,18 +732,15 @@ k_hx_spin_owner(const SpinPlan* __restrict__ pp, const void* __restrict__ x, voi
   const uint64_t dim = p.dim;
   R* sxr = reinterpret_cast<R*>(sm);
   R* sxi = sxr + p.max_block;
-  __shared__ R s_coef[2 * kMaxBonds];
-  __shared__ uint32_t s_clo[kMaxBonds], s_chi[kMaxBonds], s_dm[kMaxDiag], s_cbase[kMaxBonds];
-  __shared__ uint8_t s_ci[kMaxBonds];
-  __shared__ R s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
-  __shared__ uint2 s_hent[kMaxBonds];
-  const int ncross = p.ncross, ndc = p.ndcross, L = p.L;
+  __shared__ OwnShared S;
+  __shared__ R s_coef[2 * kMaxBonds], s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
+  const int ncross = p.ncross;
   for (int i = threadIdx.x; i < 2 * kMaxBonds; i += blockDim.x) s_coef[i] = R(p.coef[i]);
   for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
-    s_clo[i] = p.cross_lo[i]; s_chi[i] = p.cross_hi[i]; s_ci[i] = p.cross_li[i];
+    S.clo[i] = p.cross_lo[i]; S.chi[i] = p.cross_hi[i]; S.ci[i] = p.cross_li[i];
     s_c01[i] = R(p.cross_c01[i]); s_c10[i] = R(p.cross_c10[i]);
   }
-  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { s_dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
+  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { S.dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
   const uint32_t* __restrict__ A = p.A32;
   const uint32_t nA = 1u << p.H;
   double dr = 0.0, di = 0.0;
@@ -668,91 +750,23 @@ k_hx_spin_owner(const SpinPlan* __restrict__ pp, const void* __restrict__ x, voi
     if (size == 0) continue;
     const uint32_t hbeg = __ldg(p.hoff + h), nh = __ldg(p.hoff + h + 1) - hbeg;
     __syncthreads();  // the previous block is finished with the staging
-    // stage x_h: kOwnRows independent coalesced loads per thread
-    {
-      R ar[kOwnRows], ai[kOwnRows];
-      #pragma unroll
-      for (int k = 0; k < kOwnRows; ++k) {
-        const uint32_t r = threadIdx.x + k * kOwnThreads;
-        ar[k] = R(0); ai[k] = R(0);
-        if (r < size) T::ld(x, uint64_t(base) + r, ar[k], ai[k]);
-      }
-      #pragma unroll
-      for (int k = 0; k < kOwnRows; ++k) {
-        const uint32_t r = threadIdx.x + k * kOwnThreads;
-        if (r < size) { sxr[r] = ar[k]; if (T::cplx) sxi[r] = ai[k]; }
-      }
+    for (uint32_t r = threadIdx.x; r < size; r += kOwnThreads) {
+      R a, b;
+      T::ld(x, uint64_t(base) + r, a, b);
+      sxr[r] = a;
+      if (T::cplx) sxi[r] = b;
     }
-    for (int q = threadIdx.x; q < ncross; q += blockDim.x) s_cbase[q] = __ldg(A + (h ^ s_chi[q]));
-    for (uint32_t e = threadIdx.x; e < nh && e < uint32_t(kMaxBonds); e += blockDim.x) s_hent[e] = __ldg(p.hent + hbeg + e);
+    for (int q = threadIdx.x; q < ncross; q += blockDim.x) S.cbase[q] = __ldg(A + (h ^ S.chi[q]));
+    for (uint32_t e = threadIdx.x; e < nh && e < uint32_t(kMaxBonds); e += blockDim.x) S.hent[e] = __ldg(p.hent + hbeg + e);
     __syncthreads();
-    const uint32_t lst = __ldg(p.hlst + h);
-    const R dh = R(__ldg(p.dhi + h));
-    // diagonal, low bonds (shared memory) and crossing bonds, row by row
-    R yr[kOwnRows], yi[kOwnRows];
-    #pragma unroll
-    for (int k = 0; k < kOwnRows; ++k) {
-      const uint32_t r = threadIdx.x + k * kOwnThreads;
-      yr[k] = R(0); yi[k] = R(0);
-      if (r >= size) continue;
-      const uint32_t pos = lst + r;
-      const uint32_t l = uint32_t(__ldg(p.lrow + pos));
-      R d = dh + R(__ldg(p.dlo + pos));
-      const uint32_t st = (h << L) | l;
-      for (int q = 0; q < ndc; ++q) d += (__popc(st & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
-      yr[k] = d * sxr[r];
-      yi[k] = T::cplx ? d * sxi[r] : R(0);
-      const uint32_t lbeg = __ldg(p.loff + pos), lend = __ldg(p.loff + pos + 1);
-      for (uint32_t e = lbeg; e < lend; ++e) {
-        const uint32_t ent = __ldg(p.lent + e);
-        const uint32_t kk = ent >> 8;
-        if (kk >= size) continue;
-        const R c = s_coef[ent & 0xFFu];
-        yr[k] += c * sxr[kk];
-        if (T::cplx) yi[k] += c * sxi[kk];
-      }
-      for (int q = 0; q < ncross; ++q) {
-        const uint32_t bl = (l >> s_ci[q]) & 1u, bh = (h & s_chi[q]) ? 1u : 0u;
-        if (bl == bh) continue;
-        const R c = bl ? s_c10[q] : s_c01[q];
-        const uint64_t col = uint64_t(s_cbase[q]) + __ldg(p.B16 + (l ^ s_clo[q]));
-        if (col >= dim) continue;
-        R xr, xi;
-        T::ld(x, col, xr, xi);
-        yr[k] += c * xr;
-        if (T::cplx) yi[k] += c * xi;
-      }
-    }
-    // high bonds: block-wide AXPYs from other blocks at the same rank
-    for (uint32_t e = 0; e < nh; ++e) {
-      const uint2 ent = (e < uint32_t(kMaxBonds)) ? s_hent[e] : __ldg(p.hent + hbeg + e);
-      const R c = s_coef[ent.y];
-      R xr[kOwnRows], xi[kOwnRows];
-      #pragma unroll
-      for (int k = 0; k < kOwnRows; ++k) {
-        const uint32_t r = threadIdx.x + k * kOwnThreads;
-        xr[k] = R(0); xi[k] = R(0);
-        const uint64_t col = uint64_t(ent.x) + r;
-        if (r < size && col < dim) T::ld(x, col, xr[k], xi[k]);
-      }
-      #pragma unroll
-      for (int k = 0; k < kOwnRows; ++k) {
-        yr[k] += c * xr[k];
-        if (T::cplx) yi[k] += c * xi[k];
-      }
-    }
-    #pragma unroll
-    for (int k = 0; k < kOwnRows; ++k) {
-      const uint32_t r = threadIdx.x + k * kOwnThreads;
-      if (r < size) {
-        T::st(y, uint64_t(base) + r, yr[k], yi[k]);
-        if (DOT) {
-          const double x0r = double(sxr[r]), x0i = T::cplx ? double(sxi[r]) : 0.0;
-          dr += x0r * double(yr[k]) + x0i * double(yi[k]);
-          di += x0r * double(yi[k]) - x0i * double(yr[k]);
-        }
-      }
-    }
+    if (size <= kOwnThreads)
+      own_block<DT, 1>(p, S, s_coef, s_c01, s_c10, s_dw, sxr, sxi, h, base, size, hbeg, nh, x, y, DOT, dr, di);
+    else if (size <= 2 * kOwnThreads)
+      own_block<DT, 2>(p, S, s_coef, s_c01, s_c10, s_dw, sxr, sxi, h, base, size, hbeg, nh, x, y, DOT, dr, di);
+    else if (size <= 4 * kOwnThreads)
+      own_block<DT, 4>(p, S, s_coef, s_c01, s_c10, s_dw, sxr, sxi, h, base, size, hbeg, nh, x, y, DOT, dr, di);
+    else
+      own_block<DT, 8>(p, S, s_coef, s_c01, s_c10, s_dw, sxr, sxi, h, base, size, hbeg, nh, x, y, DOT, dr, di);
   }
   if (DOT) {
     __shared__ double sbuf[2 * (kOwnThreads / 32)];
