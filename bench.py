@@ -94,6 +94,21 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+# ncu summary of the default kernel on this workload (complex128, N=28);
+# its dram_bytes_per_launch line is the roofline's measured traffic.
+PROFILE = os.path.join(ROOT, "profiles", "hx_spin_owner_heisenberg_n28_c128.md")
+
+
+def profiled_traffic():
+    import re
+    try:
+        with open(PROFILE) as f:
+            m = re.search(r"^dram_bytes_per_launch:\s*(\d+)", f.read(), re.M)
+        return int(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
 def heisenberg_opsum(qk, N, dtype):
     os_ = qk.OpSum(dtype=dtype)
     for i in range(N):
@@ -236,11 +251,7 @@ def run_b200(args):
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / ke2e
 
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "hx_heisenberg_n28_c128.json")
-    if os.path.exists(prof):
-        with open(prof) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+    traffic = profiled_traffic() if N == 28 else None
 
     line = {"metric": "Hx effective HBM GB/s (Heisenberg N=28 Sz=0)", "value": value, "unit": "GB/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
