@@ -31,11 +31,11 @@ const char* qkrylov_b200_last_error(void);
 uint64_t qkrylov_b200_launch_count(void);
 int qkrylov_b200_device_count(void);
 /* 0 (default): H.x uses the specialised two-site exchange kernel (one CTA
- * per sector block, register row accumulators, per-part target lists)
- * wherever the compiled operator qualifies; 1: the generic kernel
- * everywhere; 2-6: earlier exchange-kernel variants (block tiles, warp
- * tiles, batched gathers, target lists, staged blocks).  For comparisons;
- * process-wide. */
+ * per sector block, x of the block staged in shared memory, per-row class
+ * tables) wherever the compiled operator qualifies; 1: the generic kernel
+ * everywhere; 2-7: earlier exchange-kernel variants (block tiles, warp
+ * tiles, batched gathers, target lists, staged blocks, block owner with
+ * register row accumulators).  For comparisons; process-wide. */
 int qkrylov_b200_set_kernel_policy(int policy);
 
 /* Select which of N_up / N_dn a sector conserves after

@@ -33,6 +33,12 @@ struct SpinBond {
   uint8_t valid_mask;         // which combos have a valid term
 };
 
+struct RowBlock {
+  uint32_t base, size, lst, ebeg;  // block offset, rows, llist position, first entry in bent
+  uint32_t nh, combo;              // high entries; sign pattern of the crossing Sz Sz terms
+  double dh;                       // diagonal terms inside the high part
+};
+
 struct SpinPlan {
   int L, H;
   uint64_t dim;
@@ -69,6 +75,17 @@ struct SpinPlan {
   const qk_tile_t* tiles;
   uint32_t ntiles;
   size_t smem;
+  // class and block tables of the row kernel
+  const uint2* rrec;     // per llist position: first 4-entry group; groups per low class, 4 bits each
+  const uint2* lgrp;     // 4 in-class ranks (u16) per group; padding entries name the zero slot
+  const uint16_t* crk;   // [pos][cpad]: (low-side bit << 15) | partner in-class rank
+  const double* dtab;    // [combo][pos]: low-part diagonal plus the crossing Sz Sz terms
+  const RowBlock* brec;  // per sector block
+  const uint2* bent;     // per block: high entries (base, coef) then crossing (base, coef | bit_h << 16)
+  double lcls[4];        // coefficient of each low class
+  int ncls, cpad, ncombo;
+  uint32_t zero_slot, nllist;
+  bool rows_ok;
 };
 
 namespace {
@@ -776,12 +793,202 @@ k_hx_spin_owner(const SpinPlan* __restrict__ pp, const void* __restrict__ x, voi
   }
 }
 
+// Row kernel.  A CTA owns one sector block h at a time (grid-stride over
+// blocks) and stages x_h in shared memory; each thread then walks the rows
+// r = tid, tid + 256, ... of the block.  Everything a row needs that does
+// not depend on h is precomputed per class position, and everything that
+// depends on h only comes from one block record and its entry list, so the
+// row body is loads and FMAs:
+//   y[r] = (dh + dtab[combo][pos]) x_h[r]                  diagonal
+//        + sum_c lc_c sum_j x_h[k_cj]    (u16 row lists)   low bonds
+//        + sum_q [bit_l != bit_h] c_q x[cb_q + rk_q]       crossing bonds
+//        + sum_e c_e x[hb_e + r]         (coalesced)       high bonds
+// The low list of a row is grouped by coefficient class and padded to
+// groups of four with the index of a zero slot behind the staged block, so
+// a row reads 4 targets per 8-byte load.  The next block's record is loaded
+// while the current block runs and its x is prefetched into L2.
+// Index arithmetic is 32-bit (dim < 2^32 is a precondition of the plan).
+// All gathers stay in bounds by construction: list ranks are in-class ranks
+// of the row's own class, partner blocks of a high bond have the block's
+// size, and crossing ranks are in-class ranks of the partner's class; the
+// plan builder checks the high-bond sizes.
+constexpr int kRowThreads = 256;
+constexpr int kRowCoef = 32, kRowEnt = 48, kRowCross = 16, kRowCls = 4;
+
+__device__ __forceinline__ void sld(const double2* s, uint32_t k, double& re, double& im) {
+  const double2 v = s[k]; re = v.x; im = v.y;
+}
+__device__ __forceinline__ void sld(const float2* s, uint32_t k, float& re, float& im) {
+  const float2 v = s[k]; re = v.x; im = v.y;
+}
+__device__ __forceinline__ void sld(const double* s, uint32_t k, double& re, double& im) { re = s[k]; im = 0; }
+__device__ __forceinline__ void sld(const float* s, uint32_t k, float& re, float& im) { re = s[k]; im = 0; }
+__device__ __forceinline__ void szero(double2& v) { v = make_double2(0.0, 0.0); }
+__device__ __forceinline__ void szero(float2& v) { v = make_float2(0.f, 0.f); }
+__device__ __forceinline__ void szero(double& v) { v = 0.0; }
+__device__ __forceinline__ void szero(float& v) { v = 0.f; }
+
+// L2 prefetch of [lo, hi) rounded inward to 16-byte boundaries (bulk
+// prefetch operands must be 16-byte aligned and sized), in 32 KB pieces.
+__device__ __forceinline__ void l2_prefetch(const void* lo, const void* hi) {
+  uintptr_t a = (reinterpret_cast<uintptr_t>(lo) + 15) & ~uintptr_t(15);
+  const uintptr_t b = reinterpret_cast<uintptr_t>(hi) & ~uintptr_t(15);
+  for (; a < b; a += 32768) {
+    const uint32_t n = uint32_t(b - a < 32768 ? b - a : 32768);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(n) : "memory");
+  }
+}
+
+__device__ __forceinline__ RowBlock load_block(const RowBlock* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  const uint4 a = __ldg(q), b = __ldg(q + 1);
+  RowBlock r;
+  r.base = a.x; r.size = a.y; r.lst = a.z; r.ebeg = a.w;
+  r.nh = b.x; r.combo = b.y;
+  r.dh = __hiloint2double(int(b.w), int(b.z));
+  return r;
+}
+
+template <int DT, bool DOT>
+__global__ void __launch_bounds__(kRowThreads, DT == QK_C128 ? 3 : 4)
+k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
+               double* partials, unsigned* ticket, double* dot_out) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  using E = typename T::E;
+  extern __shared__ __align__(16) unsigned char sm[];
+  const SpinPlan& p = *pp;
+  E* sx = reinterpret_cast<E*>(sm);
+  const E* __restrict__ xg = reinterpret_cast<const E*>(x);
+  __shared__ R s_coef[kRowCoef], s_lc[kRowCls], s_ec[kRowEnt];
+  __shared__ uint32_t s_eb[kRowEnt], s_ebit[kRowCross];
+  for (int i = threadIdx.x; i < kRowCoef; i += blockDim.x) s_coef[i] = R(p.coef[i]);
+  if (threadIdx.x < kRowCls) s_lc[threadIdx.x] = R(p.lcls[threadIdx.x]);
+  if (threadIdx.x == 0) szero(sx[p.zero_slot]);
+  const uint32_t nA = 1u << p.H;
+  const uint32_t nll = p.nllist;
+  const int ncross = p.ncross, ncls = p.ncls;
+  const uint32_t cw = uint32_t(p.cpad) >> 1;  // crossing words (two u16 each) per row
+  const uint32_t xbytes = uint32_t(sizeof(E));
+  double dr = 0.0, di = 0.0;
+  RowBlock nxt;
+  if (blockIdx.x < nA) nxt = load_block(p.brec + blockIdx.x);
+  for (uint32_t h = blockIdx.x; h < nA; h += gridDim.x) {
+    const RowBlock cur = nxt;
+    const uint32_t hn = h + gridDim.x;
+    if (hn < nA) nxt = load_block(p.brec + hn);
+    if (cur.size == 0) continue;
+    const uint32_t base = cur.base, size = cur.size, nh = cur.nh;
+    __syncthreads();  // the previous block is finished with the staging and the entry tables
+    for (uint32_t r = threadIdx.x; r < size; r += kRowThreads) sx[r] = __ldg(xg + base + r);
+    if (threadIdx.x < nh + uint32_t(ncross)) {
+      const uint2 e = __ldg(p.bent + cur.ebeg + threadIdx.x);
+      s_eb[threadIdx.x] = e.x;
+      s_ec[threadIdx.x] = s_coef[e.y & 0xFFFFu];
+      if (threadIdx.x >= nh) s_ebit[threadIdx.x - nh] = e.y >> 16;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && hn < nA && nxt.size) {
+      const char* xb = reinterpret_cast<const char*>(x);
+      l2_prefetch(xb + size_t(nxt.base) * xbytes, xb + size_t(nxt.base + nxt.size) * xbytes);
+    }
+    const R dh = R(cur.dh);
+    const double* __restrict__ dcol = p.dtab + size_t(cur.combo) * nll;
+    const uint32_t* __restrict__ ckw = reinterpret_cast<const uint32_t*>(p.crk);
+    const int nh8 = nh < 8 ? int(nh) : 8;
+    for (uint32_t r = threadIdx.x; r < size; r += kRowThreads) {
+      const uint32_t pos = cur.lst + r;
+      // Independent loads first so their latencies overlap: the row record,
+      // the diagonal, the first crossing pair and up to 8 high-bond values
+      // (coalesced); then the shared-memory low-bond groups.
+      const uint2 rec = __ldg(p.rrec + pos);
+      const double dt = __ldg(dcol + pos);
+      const uint32_t two0 = ncross ? __ldg(ckw + pos * cw) : 0u;
+      R hr[8], hi[8];
+      #pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        hr[e] = R(0); hi[e] = R(0);
+        if (e < nh8) T::ld(x, s_eb[e] + r, hr[e], hi[e]);
+      }
+      R cr[2], ci[2];
+      #pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        cr[u] = R(0); ci[u] = R(0);
+        const uint32_t ent = u ? (two0 >> 16) : (two0 & 0xFFFFu);
+        if (u < ncross && (ent >> 15) != s_ebit[u]) T::ld(x, s_eb[nh + u] + (ent & 0x7FFFu), cr[u], ci[u]);
+      }
+      R x0r, x0i;
+      sld(sx, r, x0r, x0i);
+      const R d = dh + R(dt);
+      R ar = d * x0r, ai = T::cplx ? d * x0i : R(0);
+      const uint2* __restrict__ g = p.lgrp + rec.x;
+      for (int c = 0; c < ncls; ++c) {
+        const uint32_t ng = (rec.y >> (4 * c)) & 0xFu;
+        R sr = R(0), si = R(0);
+        for (uint32_t k = 0; k < ng; ++k) {
+          const uint2 q = __ldg(g + k);
+          R vr, vi;
+          sld(sx, q.x & 0xFFFFu, vr, vi); sr += vr; if (T::cplx) si += vi;
+          sld(sx, q.x >> 16, vr, vi);     sr += vr; if (T::cplx) si += vi;
+          sld(sx, q.y & 0xFFFFu, vr, vi); sr += vr; if (T::cplx) si += vi;
+          sld(sx, q.y >> 16, vr, vi);     sr += vr; if (T::cplx) si += vi;
+        }
+        g += ng;
+        ar += s_lc[c] * sr;
+        if (T::cplx) ai += s_lc[c] * si;
+      }
+      #pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const R c = u < ncross ? s_ec[nh + u] : R(0);
+        ar += c * cr[u];
+        if (T::cplx) ai += c * ci[u];
+      }
+      for (int q = 2; q < ncross; q += 2) {
+        const uint32_t two = __ldg(ckw + pos * cw + (q >> 1));
+        #pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const uint32_t ent = u ? (two >> 16) : (two & 0xFFFFu);
+          if (q + u < ncross && (ent >> 15) != s_ebit[q + u]) {
+            R vr, vi;
+            T::ld(x, s_eb[nh + q + u] + (ent & 0x7FFFu), vr, vi);
+            ar += s_ec[nh + q + u] * vr;
+            if (T::cplx) ai += s_ec[nh + q + u] * vi;
+          }
+        }
+      }
+      #pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const R c = e < nh8 ? s_ec[e] : R(0);
+        ar += c * hr[e];
+        if (T::cplx) ai += c * hi[e];
+      }
+      for (uint32_t e = 8; e < nh; ++e) {
+        R vr, vi;
+        T::ld(x, s_eb[e] + r, vr, vi);
+        ar += s_ec[e] * vr;
+        if (T::cplx) ai += s_ec[e] * vi;
+      }
+      T::st(y, base + r, ar, ai);
+      if (DOT) {
+        dr += double(x0r) * double(ar) + double(x0i) * double(ai);
+        di += double(x0r) * double(ai) - double(x0i) * double(ar);
+      }
+    }
+  }
+  if (DOT) {
+    __shared__ double sbuf[2 * (kRowThreads / 32)];
+    block_sum2(dr, di, sbuf);
+    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
+    grid_finish(partials, ticket, 1, dot_out);
+  }
+}
+
 }  // namespace
 
 struct SpinHandle {
   SpinPlan host;
   SpinPlan* dev = nullptr;
-  void* bufs[11] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  void* bufs[17] = {};
   bool lean = false;  // every bond conserves the charge: warp-tile kernel
 };
 
@@ -933,6 +1140,118 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     if (hent.empty()) hent.push_back(make_uint2(0, 0));
   }
 
+  // Row-kernel tables.  Eligibility: at most kRowCls distinct low-bond
+  // coefficients and 15 groups of four per class and row, few enough
+  // coefficients and per-block entries for the shared tables, the combined
+  // diagonal table at most 16 MB, a free u16 index for the zero slot, and
+  // every high-bond partner block of the same size as the block (which is
+  // what keeps the coalesced high-bond loads in bounds).
+  std::vector<uint2> rrec, lgrp, bent;
+  std::vector<uint16_t> crk;
+  std::vector<double> dtab;
+  std::vector<RowBlock> brec;
+  if (lean) {
+    const uint32_t lowbits = (1u << L) - 1u;
+    h.cpad = h.ncross ? (h.ncross + 1) & ~1 : 0;
+    h.ncombo = 1 << h.ndcross;
+    h.nllist = uint32_t(d->nllist);
+    h.zero_slot = h.max_block;
+    h.rows_ok = h.nhigh + h.ncross <= kRowEnt && h.ncross <= kRowCross && h.ndcross <= 6 &&
+                d->nllist * uint64_t(h.ncombo) * 8 <= (16ull << 20) && h.max_block < 0xFFFFu;
+    // low coefficient classes (by coefficient index of the list entries)
+    int cls_of[2 * kMaxBonds];
+    for (int k = 0; k < 2 * kMaxBonds; ++k) cls_of[k] = -1;
+    for (uint32_t e = 0; e < loff[d->nllist] && h.rows_ok; ++e) {
+      const uint32_t ci = lent[e] & 0xFFu;
+      if (cls_of[ci] >= 0) continue;
+      if (h.ncls == kRowCls) { h.rows_ok = false; break; }
+      cls_of[ci] = h.ncls;
+      h.lcls[h.ncls++] = h.coef[ci];
+    }
+    for (uint64_t hh = 0; hh < d->nA && h.rows_ok; ++hh) {
+      if (uint32_t(d->A[hh] >> 56) == qkb::kEmptyBlockKey) continue;
+      const uint32_t need = uint32_t(d->A[hh] >> 56), size = d->key_off[need + 1] - d->key_off[need];
+      for (int q = 0; q < h.nhigh; ++q) {
+        const uint32_t m = h.high_mask[q], v = uint32_t(hh) & m;
+        if (v == 0 || v == m) continue;
+        const uint32_t need2 = uint32_t(d->A[hh ^ m] >> 56);
+        if (need2 == qkb::kEmptyBlockKey || d->key_off[need2 + 1] - d->key_off[need2] != size) h.rows_ok = false;
+      }
+    }
+    if (h.rows_ok) {
+      rrec.resize(d->nllist);
+      std::vector<uint16_t> bucket[kRowCls];
+      for (uint64_t pos = 0; pos < d->nllist && h.rows_ok; ++pos) {
+        for (auto& b : bucket) b.clear();
+        for (uint32_t e = loff[pos]; e < loff[pos + 1]; ++e)
+          bucket[cls_of[lent[e] & 0xFFu]].push_back(uint16_t(lent[e] >> 8));
+        uint32_t counts = 0;
+        rrec[pos].x = uint32_t(lgrp.size());
+        for (int c = 0; c < h.ncls; ++c) {
+          auto& b = bucket[c];
+          while (b.size() % 4) b.push_back(uint16_t(h.zero_slot));
+          const uint32_t ng = uint32_t(b.size() / 4);
+          if (ng > 15) { h.rows_ok = false; break; }
+          counts |= ng << (4 * c);
+          for (uint32_t k = 0; k < ng; ++k)
+            lgrp.push_back(make_uint2(uint32_t(b[4 * k]) | (uint32_t(b[4 * k + 1]) << 16),
+                                      uint32_t(b[4 * k + 2]) | (uint32_t(b[4 * k + 3]) << 16)));
+        }
+        rrec[pos].y = counts;
+      }
+      if (lgrp.empty()) lgrp.push_back(make_uint2(0, 0));
+    }
+    if (h.rows_ok) {
+      crk.assign(std::max<uint64_t>(2, d->nllist * uint64_t(h.cpad)), 0);
+      for (uint64_t pos = 0; pos < d->nllist; ++pos) {
+        const uint32_t l = d->llist[pos];
+        for (int q = 0; q < h.ncross; ++q) {
+          const uint32_t bl = (l >> h.cross_li[q]) & 1u;
+          crk[pos * h.cpad + q] = uint16_t((bl << 15) | (d->B[l ^ h.cross_lo[q]] & 0x7FFFu));
+        }
+      }
+      dtab.assign(d->nllist * uint64_t(h.ncombo), 0.0);
+      for (int c = 0; c < h.ncombo; ++c)
+        for (uint64_t pos = 0; pos < d->nllist; ++pos) {
+          const uint32_t l = d->llist[pos];
+          double v = dlo[pos];
+          for (int q = 0; q < h.ndcross; ++q) {
+            const uint32_t par = ((c >> q) ^ __builtin_popcount(l & h.dcross_mask[q] & lowbits)) & 1u;
+            v += par ? -h.dcross_w[q] : h.dcross_w[q];
+          }
+          dtab[c * d->nllist + pos] = v;
+        }
+      auto coef_index = [&](double c) -> uint32_t {
+        for (int k = 0; k < h.ncoef; ++k) if (h.coef[k] == c) return uint32_t(k);
+        h.coef[h.ncoef] = c;
+        return uint32_t(h.ncoef++);
+      };
+      brec.resize(d->nA);
+      for (uint64_t hh = 0; hh < d->nA; ++hh) {
+        RowBlock& b = brec[hh];
+        const uint32_t need = uint32_t(d->A[hh] >> 56);
+        b.base = uint32_t(d->A[hh] & qkb::kOffsetMask);
+        b.size = need == qkb::kEmptyBlockKey ? 0 : d->key_off[need + 1] - d->key_off[need];
+        b.lst = hlst[hh];
+        b.ebeg = uint32_t(bent.size());
+        b.nh = hoff[hh + 1] - hoff[hh];
+        b.dh = dhi[hh];
+        b.combo = 0;
+        for (int q = 0; q < h.ndcross; ++q)
+          b.combo |= uint32_t(__builtin_popcount(uint32_t(hh) & (h.dcross_mask[q] >> L)) & 1) << q;
+        for (uint32_t e = hoff[hh]; e < hoff[hh + 1]; ++e) bent.push_back(hent[e]);
+        for (int q = 0; q < h.ncross; ++q) {
+          const uint32_t bh = (uint32_t(hh) & h.cross_hi[q]) ? 1u : 0u;
+          // valid rows have the opposite low bit: c01 (low 0, high 1) or c10
+          const uint32_t ci = coef_index(bh ? h.cross_c01[q] : h.cross_c10[q]);
+          bent.push_back(make_uint2(uint32_t(d->A[hh ^ h.cross_hi[q]] & qkb::kOffsetMask), ci | (bh << 16)));
+        }
+      }
+      if (bent.empty()) bent.push_back(make_uint2(0, 0));
+      if (h.ncoef > kRowCoef) h.rows_ok = false;
+    }
+  }
+
   std::vector<uint32_t> A32(d->nA);
   std::vector<uint16_t> B16(d->nB), l16(d->nllist);
   for (uint64_t k = 0; k < d->nA; ++k) A32[k] = uint32_t(d->A[k] & qkb::kOffsetMask);
@@ -962,7 +1281,12 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
             up(4, dhi.data(), dhi.size() * 8) && up(5, dlo.data(), dlo.size() * 8) &&
             (!lean || (up(6, loff.data(), loff.size() * 4) && up(7, lent.data(), lent.size() * 4) &&
                        up(8, hoff.data(), hoff.size() * 4) && up(9, hent.data(), hent.size() * sizeof(uint2)) &&
-                       up(10, hlst.data(), hlst.size() * 4)));
+                       up(10, hlst.data(), hlst.size() * 4))) &&
+            (!h.rows_ok || (up(11, rrec.data(), rrec.size() * sizeof(uint2)) &&
+                            up(12, lgrp.data(), lgrp.size() * sizeof(uint2)) && up(13, crk.data(), crk.size() * 2) &&
+                            up(14, dtab.data(), dtab.size() * 8) &&
+                            up(15, brec.data(), brec.size() * sizeof(RowBlock)) &&
+                            up(16, bent.data(), bent.size() * sizeof(uint2))));
   if (ok) {
     h.A32 = static_cast<const uint32_t*>(out->bufs[0]);
     h.B16 = static_cast<const uint16_t*>(out->bufs[1]);
@@ -975,6 +1299,12 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.hoff = static_cast<const uint32_t*>(out->bufs[8]);
     h.hent = static_cast<const uint2*>(out->bufs[9]);
     h.hlst = static_cast<const uint32_t*>(out->bufs[10]);
+    h.rrec = static_cast<const uint2*>(out->bufs[11]);
+    h.lgrp = static_cast<const uint2*>(out->bufs[12]);
+    h.crk = static_cast<const uint16_t*>(out->bufs[13]);
+    h.dtab = static_cast<const double*>(out->bufs[14]);
+    h.brec = static_cast<const RowBlock*>(out->bufs[15]);
+    h.bent = static_cast<const uint2*>(out->bufs[16]);
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1142,11 +1472,46 @@ int spin_apply_owner(const SpinHandle* h, qk_dtype t, const void* x, void* y, cu
   return QKD_OK;
 }
 
-static int g_spin_variant = 5;  // 0 block tiles, 1 warp tiles, 2 batched, 3 lists, 4 staged, 5 block owner
+int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
+                    qk_workspace* w, double* dot_out) {
+  if (!h->host.rows_ok) return QKD_EINVAL;
+  const size_t es = (t == QK_C128) ? 16 : (t == QK_F32 ? 4 : 8);
+  const size_t smem = es * (h->host.max_block + 1);  // staged block and the zero slot
+  if (smem > 200 * 1024) return QKD_EINVAL;
+#define QKD_ROWS_LAUNCH(DT)                                                                               \
+  {                                                                                                       \
+    auto kd = k_hx_spin_rows<DT, true>;                                                                   \
+    auto kn = k_hx_spin_rows<DT, false>;                                                                  \
+    if (cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||  \
+        cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)    \
+      return QKD_EINVAL;                                                                                  \
+    const unsigned cap = 1u << h->host.H;                                                                 \
+    if (dot_out) kd<<<resident_grid(kd, kRowThreads, smem, std::min<unsigned>(cap, kMaxG)), kRowThreads, smem, s>>>( \
+        h->dev, x, y, w->partials, w->ticket, dot_out);                                                   \
+    else kn<<<resident_grid(kn, kRowThreads, smem, cap), kRowThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr); \
+  }
+  switch (t) {
+    case QK_C128: QKD_ROWS_LAUNCH(QK_C128); break;
+    case QK_C64: QKD_ROWS_LAUNCH(QK_C64); break;
+    case QK_F64: QKD_ROWS_LAUNCH(QK_F64); break;
+    case QK_F32: QKD_ROWS_LAUNCH(QK_F32); break;
+    default: return QKD_EINVAL;
+  }
+#undef QKD_ROWS_LAUNCH
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+// 0 block tiles, 1 warp tiles, 2 batched, 3 lists, 4 staged, 5 block owner, 6 rows
+static int g_spin_variant = 6;
 
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out) {
-  if (h->lean && g_spin_variant == 5) {
+  if (h->lean && g_spin_variant == 6) {
+    const int rc = spin_apply_rows(h, t, x, y, s, w, dot_out);
+    if (rc != QKD_EINVAL) return rc;
+  }
+  if (h->lean && g_spin_variant >= 5) {
     const int rc = spin_apply_owner(h, t, x, y, s, w, dot_out);
     if (rc != QKD_EINVAL) return rc;
   }
@@ -1187,7 +1552,7 @@ int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStre
 }
 
 int spin_set_variant(int v) {
-  if (v < 0 || v > 5) return QKD_EINVAL;
+  if (v < 0 || v > 6) return QKD_EINVAL;
   g_spin_variant = v;
   return QKD_OK;
 }

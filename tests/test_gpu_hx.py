@@ -156,7 +156,7 @@ def test_spin_exchange_kernel_equals_generic(N, terms):
     ys = {}
     try:
         for pol in ("generic", "exchange-block", "exchange-warp", "exchange-batched", "exchange-list",
-                    "exchange-staged"):
+                    "exchange-staged", "exchange-owner"):
             qk.set_kernel_policy(pol)
             ys[pol] = H.apply(x)
         assert H.kernel == "spin-exchange"
