@@ -806,7 +806,7 @@ k_hx_spin_owner(const SpinPlan* __restrict__ pp, const void* __restrict__ x, voi
 // The low list of a row is grouped by coefficient class and padded to
 // groups of four with the index of a zero slot behind the staged block, so
 // a row reads 4 targets per 8-byte load.  The next block's record is loaded
-// while the current block runs and its x is prefetched into L2.
+// while the current block runs.
 // Index arithmetic is 32-bit (dim < 2^32 is a precondition of the plan).
 // All gathers stay in bounds by construction: list ranks are in-class ranks
 // of the row's own class, partner blocks of a high bond have the block's
@@ -814,6 +814,7 @@ k_hx_spin_owner(const SpinPlan* __restrict__ pp, const void* __restrict__ x, voi
 // plan builder checks the high-bond sizes.
 constexpr int kRowThreads = 256;
 constexpr int kRowCoef = 32, kRowEnt = 48, kRowCross = 16, kRowCls = 4;
+template <int DT> constexpr int kRowBatch = DT == QK_C128 ? 1 : 4;  // rows per thread and pass
 
 __device__ __forceinline__ void sld(const double2* s, uint32_t k, double& re, double& im) {
   const double2 v = s[k]; re = v.x; im = v.y;
@@ -827,17 +828,6 @@ __device__ __forceinline__ void szero(double2& v) { v = make_double2(0.0, 0.0); 
 __device__ __forceinline__ void szero(float2& v) { v = make_float2(0.f, 0.f); }
 __device__ __forceinline__ void szero(double& v) { v = 0.0; }
 __device__ __forceinline__ void szero(float& v) { v = 0.f; }
-
-// L2 prefetch of [lo, hi) rounded inward to 16-byte boundaries (bulk
-// prefetch operands must be 16-byte aligned and sized), in 32 KB pieces.
-__device__ __forceinline__ void l2_prefetch(const void* lo, const void* hi) {
-  uintptr_t a = (reinterpret_cast<uintptr_t>(lo) + 15) & ~uintptr_t(15);
-  const uintptr_t b = reinterpret_cast<uintptr_t>(hi) & ~uintptr_t(15);
-  for (; a < b; a += 32768) {
-    const uint32_t n = uint32_t(b - a < 32768 ? b - a : 32768);
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(n) : "memory");
-  }
-}
 
 __device__ __forceinline__ RowBlock load_block(const RowBlock* p) {
   const uint4* q = reinterpret_cast<const uint4*>(p);
@@ -869,7 +859,6 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
   const uint32_t nll = p.nllist;
   const int ncross = p.ncross, ncls = p.ncls;
   const uint32_t cw = uint32_t(p.cpad) >> 1;  // crossing words (two u16 each) per row
-  const uint32_t xbytes = uint32_t(sizeof(E));
   double dr = 0.0, di = 0.0;
   RowBlock nxt;
   if (blockIdx.x < nA) nxt = load_block(p.brec + blockIdx.x);
@@ -888,90 +877,122 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       if (threadIdx.x >= nh) s_ebit[threadIdx.x - nh] = e.y >> 16;
     }
     __syncthreads();
-    if (threadIdx.x == 0 && hn < nA && nxt.size) {
-      const char* xb = reinterpret_cast<const char*>(x);
-      l2_prefetch(xb + size_t(nxt.base) * xbytes, xb + size_t(nxt.base + nxt.size) * xbytes);
-    }
     const R dh = R(cur.dh);
     const double* __restrict__ dcol = p.dtab + size_t(cur.combo) * nll;
     const uint32_t* __restrict__ ckw = reinterpret_cast<const uint32_t*>(p.crk);
+    // block-uniform entries in registers: the first 8 high bonds, 2 crossing
     const int nh8 = nh < 8 ? int(nh) : 8;
-    for (uint32_t r = threadIdx.x; r < size; r += kRowThreads) {
-      const uint32_t pos = cur.lst + r;
-      // Independent loads first so their latencies overlap: the row record,
-      // the diagonal, the first crossing pair and up to 8 high-bond values
-      // (coalesced); then the shared-memory low-bond groups.
-      const uint2 rec = __ldg(p.rrec + pos);
-      const double dt = __ldg(dcol + pos);
-      const uint32_t two0 = ncross ? __ldg(ckw + pos * cw) : 0u;
-      R hr[8], hi[8];
+    uint32_t eb[8];
+    R ec[8];
+    #pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      eb[e] = e < nh8 ? s_eb[e] : 0u;
+      ec[e] = e < nh8 ? s_ec[e] : R(0);
+    }
+    uint32_t cb[2], cbit[2];
+    R cc[2];
+    #pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      cb[u] = u < ncross ? s_eb[nh + u] : 0u;
+      cbit[u] = u < ncross ? s_ebit[u] : 2u;  // 2: never equal to a low bit, never valid
+      cc[u] = u < ncross ? s_ec[nh + u] : R(0);
+    }
+    constexpr int K = kRowBatch<DT>;
+    for (uint32_t r0 = threadIdx.x; r0 < size; r0 += K * kRowThreads) {
+      // K rows r0 + k * 256 per thread.  Loads that do not depend on each
+      // other are issued together: row records, diagonals, crossing pairs,
+      // then all high-bond values; the shared-memory low groups come last.
+      uint32_t rk[K], pos[K];
+      bool ok[K];
+      uint2 rec[K];
+      double dt[K];
+      uint32_t two[K];
+      #pragma unroll
+      for (int k = 0; k < K; ++k) {
+        rk[k] = r0 + k * kRowThreads;
+        ok[k] = rk[k] < size;
+        pos[k] = cur.lst + (ok[k] ? rk[k] : 0u);
+        rec[k] = __ldg(p.rrec + pos[k]);
+        dt[k] = __ldg(dcol + pos[k]);
+        two[k] = ncross ? __ldg(ckw + pos[k] * cw) : 0u;
+      }
+      R ar[K], ai[K];
+      #pragma unroll
+      for (int k = 0; k < K; ++k) { ar[k] = R(0); ai[k] = R(0); }
       #pragma unroll
       for (int e = 0; e < 8; ++e) {
-        hr[e] = R(0); hi[e] = R(0);
-        if (e < nh8) T::ld(x, s_eb[e] + r, hr[e], hi[e]);
-      }
-      R cr[2], ci[2];
-      #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        cr[u] = R(0); ci[u] = R(0);
-        const uint32_t ent = u ? (two0 >> 16) : (two0 & 0xFFFFu);
-        if (u < ncross && (ent >> 15) != s_ebit[u]) T::ld(x, s_eb[nh + u] + (ent & 0x7FFFu), cr[u], ci[u]);
-      }
-      R x0r, x0i;
-      sld(sx, r, x0r, x0i);
-      const R d = dh + R(dt);
-      R ar = d * x0r, ai = T::cplx ? d * x0i : R(0);
-      const uint2* __restrict__ g = p.lgrp + rec.x;
-      for (int c = 0; c < ncls; ++c) {
-        const uint32_t ng = (rec.y >> (4 * c)) & 0xFu;
-        R sr = R(0), si = R(0);
-        for (uint32_t k = 0; k < ng; ++k) {
-          const uint2 q = __ldg(g + k);
-          R vr, vi;
-          sld(sx, q.x & 0xFFFFu, vr, vi); sr += vr; if (T::cplx) si += vi;
-          sld(sx, q.x >> 16, vr, vi);     sr += vr; if (T::cplx) si += vi;
-          sld(sx, q.y & 0xFFFFu, vr, vi); sr += vr; if (T::cplx) si += vi;
-          sld(sx, q.y >> 16, vr, vi);     sr += vr; if (T::cplx) si += vi;
-        }
-        g += ng;
-        ar += s_lc[c] * sr;
-        if (T::cplx) ai += s_lc[c] * si;
-      }
-      #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const R c = u < ncross ? s_ec[nh + u] : R(0);
-        ar += c * cr[u];
-        if (T::cplx) ai += c * ci[u];
-      }
-      for (int q = 2; q < ncross; q += 2) {
-        const uint32_t two = __ldg(ckw + pos * cw + (q >> 1));
         #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const uint32_t ent = u ? (two >> 16) : (two & 0xFFFFu);
-          if (q + u < ncross && (ent >> 15) != s_ebit[q + u]) {
+        for (int k = 0; k < K; ++k) {
+          if (e < nh8 && ok[k]) {
             R vr, vi;
-            T::ld(x, s_eb[nh + q + u] + (ent & 0x7FFFu), vr, vi);
-            ar += s_ec[nh + q + u] * vr;
-            if (T::cplx) ai += s_ec[nh + q + u] * vi;
+            T::ld(x, eb[e] + rk[k], vr, vi);
+            ar[k] += ec[e] * vr;
+            if (T::cplx) ai[k] += ec[e] * vi;
           }
         }
       }
       #pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const R c = e < nh8 ? s_ec[e] : R(0);
-        ar += c * hr[e];
-        if (T::cplx) ai += c * hi[e];
+      for (int k = 0; k < K; ++k) {
+        #pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const uint32_t ent = u ? (two[k] >> 16) : (two[k] & 0xFFFFu);
+          if (ok[k] && (ent >> 15) != cbit[u]) {
+            R vr, vi;
+            T::ld(x, cb[u] + (ent & 0x7FFFu), vr, vi);
+            ar[k] += cc[u] * vr;
+            if (T::cplx) ai[k] += cc[u] * vi;
+          }
+        }
       }
-      for (uint32_t e = 8; e < nh; ++e) {
-        R vr, vi;
-        T::ld(x, s_eb[e] + r, vr, vi);
-        ar += s_ec[e] * vr;
-        if (T::cplx) ai += s_ec[e] * vi;
-      }
-      T::st(y, base + r, ar, ai);
-      if (DOT) {
-        dr += double(x0r) * double(ar) + double(x0i) * double(ai);
-        di += double(x0r) * double(ai) - double(x0i) * double(ar);
+      #pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (!ok[k]) continue;
+        const uint32_t r = rk[k];
+        for (uint32_t e = 8; e < nh; ++e) {
+          R vr, vi;
+          T::ld(x, s_eb[e] + r, vr, vi);
+          ar[k] += s_ec[e] * vr;
+          if (T::cplx) ai[k] += s_ec[e] * vi;
+        }
+        for (int q = 2; q < ncross; q += 2) {
+          const uint32_t tw = __ldg(ckw + pos[k] * cw + (q >> 1));
+          #pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const uint32_t ent = u ? (tw >> 16) : (tw & 0xFFFFu);
+            if (q + u < ncross && (ent >> 15) != s_ebit[q + u]) {
+              R vr, vi;
+              T::ld(x, s_eb[nh + q + u] + (ent & 0x7FFFu), vr, vi);
+              ar[k] += s_ec[nh + q + u] * vr;
+              if (T::cplx) ai[k] += s_ec[nh + q + u] * vi;
+            }
+          }
+        }
+        const uint2* __restrict__ g = p.lgrp + rec[k].x;
+        for (int c = 0; c < ncls; ++c) {
+          const uint32_t ng = (rec[k].y >> (4 * c)) & 0xFu;
+          R sr = R(0), si = R(0);
+          for (uint32_t j = 0; j < ng; ++j) {
+            const uint2 q = __ldg(g + j);
+            R vr, vi;
+            sld(sx, q.x & 0xFFFFu, vr, vi); sr += vr; if (T::cplx) si += vi;
+            sld(sx, q.x >> 16, vr, vi);     sr += vr; if (T::cplx) si += vi;
+            sld(sx, q.y & 0xFFFFu, vr, vi); sr += vr; if (T::cplx) si += vi;
+            sld(sx, q.y >> 16, vr, vi);     sr += vr; if (T::cplx) si += vi;
+          }
+          g += ng;
+          ar[k] += s_lc[c] * sr;
+          if (T::cplx) ai[k] += s_lc[c] * si;
+        }
+        R x0r, x0i;
+        sld(sx, r, x0r, x0i);
+        const R d = dh + R(dt[k]);
+        ar[k] += d * x0r;
+        if (T::cplx) ai[k] += d * x0i;
+        T::st(y, base + r, ar[k], ai[k]);
+        if (DOT) {
+          dr += double(x0r) * double(ar[k]) + double(x0i) * double(ai[k]);
+          di += double(x0r) * double(ai[k]) - double(x0i) * double(ar[k]);
+        }
       }
     }
   }
