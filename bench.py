@@ -12,6 +12,8 @@ tables, term tables and repeated gathers are not counted).
   e2e    the same apply through the C ABI entry point with host buffers
          (qkrylov_hamiltonian_apply_complex_f64): H2D of x, kernel, D2H of y
   variants  the same kernel on complex64 / float64 / float32 vectors
+  time_to_e0  plain FP64 GPU Lanczos vs FP32-vector Lanczos + FP64
+         refinement, both to the explicit residual 1e-10 (wall seconds)
 
 --impl reference times the reference's own CPU implementation (its
 unchanged sources, oracle/_ref, OpenMP on all host cores) on a bounded
@@ -144,6 +146,30 @@ def cpu_reference_gbs(N=24, steps=3, use_ref=True):
                 seconds_per_apply=t)
 
 
+def time_to_e0(qk, N, tol=1e-10, seed=1):
+    """Plain FP64 GPU Lanczos vs the mixed-precision form on the Heisenberg
+    chain, both from a GPU random start, both stopped at the explicit FP64
+    residual ||H psi - E psi|| / |E| <= tol; each form runs twice and the
+    second (warm) run is reported."""
+    H = qk.MatrixFreeHamiltonian(qk.SpinHalfBasis(N, sz=0), qk.SpinHalfSite(), heisenberg_opsum(qk, N, np.float64),
+                                 dtype=np.float64)
+    out = {"workload": f"heisenberg_chain_N{N}_Sz0", "dim": H.dimension, "tol_residual": tol,
+           "start": f"GPU uniform [-1,1) from seed {seed}"}
+    for name, fn in (("plain_fp64", qk.lanczos_fp64), ("mixed", qk.lanczos_mixed)):
+        r = None
+        for _ in range(2):
+            t0 = time.perf_counter()
+            r = fn(H, seed=seed, tol=tol)
+            wall = time.perf_counter() - t0
+        out[name] = {"seconds": wall, "energy": r.energy, "residual": r.residual, "converged": r.converged,
+                     "iterations_fp32": r.iterations_low, "iterations_fp64": r.iterations_high,
+                     "restarts": r.restarts}
+    out["dE_mixed_vs_plain"] = abs(out["mixed"]["energy"] - out["plain_fp64"]["energy"])
+    out["speedup_mixed"] = out["plain_fp64"]["seconds"] / out["mixed"]["seconds"]
+    del H
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -269,6 +295,12 @@ def run_b200(args):
             "variants": variants,
             "gpu_launches": launches,
             "clocks": clk.summary()}
+    if rank == 0 and not args.no_solvers:
+        try:
+            torch.cuda.empty_cache()
+            line["time_to_e0"] = time_to_e0(qk, N)
+        except Exception as e:  # reported, never silently replaced
+            line["time_to_e0"] = {"error": str(e)}
     if rank == 0 and not args.no_cpu_baseline:
         try:
             cb = cpu_reference_gbs(N=24, steps=2)
@@ -289,6 +321,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=28)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-solvers", action="store_true", help="skip the time-to-E0 Lanczos comparison")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time only the device apply (profiling runs)")
     ap.add_argument("--kernel-dtype", default="c128", choices=["c128", "c64", "f64", "f32"],

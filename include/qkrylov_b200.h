@@ -148,6 +148,46 @@ double qkrylov_evaluate_spectral_function_f64(const double* alphas, const double
 int qkrylov_ftlm_sweep_f64(qkrylov_hamiltonian_h h, int n_beta, const double* betas, int n_random, int n_steps,
                            double* Z_out, double* U_out, double* Cv_out);
 
+/* ------------------------------------------------ mixed-precision Lanczos
+ * No counterpart in the reference.  Lanczos with full reorthogonalisation
+ * whose vectors and H.x are FP32 (float32 for a real operator, complex64
+ * otherwise) while alpha, beta, the reorthogonalisation coefficients, the
+ * norms and the tridiagonal eigensolve are FP64.  It stops when the Ritz
+ * value settles (|dE| < 1e-8 |E|) or the residual estimate beta_k |z_k|
+ * drops below 1e-5 |E|; FP64 Lanczos (float64 / complex128 vectors) then
+ * restarts from that Ritz vector until the explicit FP64 residual
+ * ||H psi - E psi|| / |E| <= tol, at most 8 restarts of up to maxiter
+ * (<= 511) steps each.
+ *   start: NULL for a random start generated on the GPU from `seed`
+ *          (uniform in [-1, 1)), else dimension() elements of the FP32
+ *          vector type, in host memory, or in device memory of the
+ *          operator's GPU when start_on_device is non-zero.
+ *   psi_out: NULL, or host memory for the normalised FP64 ground state.
+ *   trace_*: NULL, or trace_cap entries receiving (iteration, Ritz value,
+ *          seconds since the call started) for every step of both phases. */
+typedef struct {
+  double energy;
+  double residual;      /* explicit ||H psi - E psi|| / |E| of psi_out */
+  double seconds_low;   /* wall time of the FP32 phase (with start set-up) */
+  double seconds_high;  /* wall time of the FP64 phase and residual checks */
+  int iterations_low;
+  int iterations_high;
+  int restarts;
+  int converged;
+  int trace_len;
+} qkrylov_b200_mixed_result_t;
+
+int qkrylov_b200_lanczos_mixed(qkrylov_hamiltonian_h h, uint64_t seed, const void* start, int start_on_device,
+                               int maxiter, double tol, qkrylov_b200_mixed_result_t* result, void* psi_out,
+                               int trace_cap, int* trace_iteration, double* trace_energy, double* trace_seconds);
+
+/* The FP64 phase alone from the start (FP64 vector type) or a random FP64
+ * start: plain FP64 Lanczos with the same explicit-residual stopping rule,
+ * the baseline the mixed form is timed against. */
+int qkrylov_b200_lanczos_fp64(qkrylov_hamiltonian_h h, uint64_t seed, const void* start, int start_on_device,
+                              int maxiter, double tol, qkrylov_b200_mixed_result_t* result, void* psi_out,
+                              int trace_cap, int* trace_iteration, double* trace_energy, double* trace_seconds);
+
 #ifdef __cplusplus
 }
 #endif

@@ -462,6 +462,70 @@ def lanczos_ground_state(H: MatrixFreeHamiltonian, maxiter: int = 200, tol: floa
     return LanczosResult(float(res.energy), ev, res.iterations, bool(res.converged))
 
 
+class MixedLanczosResult:
+    """Result of lanczos_mixed / lanczos_fp64: energy, explicit FP64 residual
+    ||H psi - E psi|| / |E|, iterations per phase, wall seconds per phase and
+    the per-step trace (iteration, Ritz value, seconds since the start)."""
+
+    def __init__(self, r, trace, eigenvector):
+        self.energy, self.residual = r.energy, r.residual
+        self.iterations_low, self.iterations_high = r.iterations_low, r.iterations_high
+        self.seconds_low, self.seconds_high = r.seconds_low, r.seconds_high
+        self.seconds = r.seconds_low + r.seconds_high
+        self.restarts, self.converged = r.restarts, bool(r.converged)
+        self.trace, self.eigenvector = trace, eigenvector
+
+    def __repr__(self):
+        return (f"MixedLanczosResult(energy={self.energy:.15g}, residual={self.residual:.2e}, "
+                f"iterations={self.iterations_low}+{self.iterations_high}, seconds={self.seconds:.4f})")
+
+
+def _two_phase(fn, H, seed, start, start_device, maxiter, tol, want_vector, low):
+    L = lib()
+    dim = H.dimension
+    real = bool(L.qkrylov_hamiltonian_all_real(H._h))
+    sdt = (np.float32 if real else np.complex64) if low else (np.float64 if real else np.complex128)
+    odt = np.float64 if real else np.complex128
+    sp, on_dev = None, 0
+    if start_device is not None:
+        sp, on_dev = int(start_device), 1
+    elif start is not None:
+        st = np.ascontiguousarray(start, dtype=sdt)
+        if st.size != dim:
+            raise ValueError("start vector has the wrong length")
+        sp = st.ctypes.data
+    psi = np.empty(dim, dtype=odt) if want_vector else None
+    cap = 8 * max(maxiter, 1) + 8
+    ti, te, ts = np.zeros(cap, np.int32), np.zeros(cap), np.zeros(cap)
+    r = _MixedC()
+    _check(fn(H._h, ctypes.c_uint64(seed), sp, on_dev, maxiter, tol, ctypes.byref(r),
+              psi.ctypes.data if psi is not None else None, cap, ti.ctypes.data, te.ctypes.data, ts.ctypes.data),
+           "lanczos_mixed" if low else "lanczos_fp64")
+    n = r.trace_len
+    trace = list(zip(ti[:n].tolist(), te[:n].tolist(), ts[:n].tolist()))
+    return MixedLanczosResult(r, trace, psi)
+
+
+def lanczos_mixed(H: MatrixFreeHamiltonian, seed: int = 0, start: Optional[np.ndarray] = None,
+                  maxiter: int = 200, tol: float = 1e-10, start_device: Optional[int] = None,
+                  eigenvector: bool = False) -> MixedLanczosResult:
+    """FP32-vector Lanczos (FP64 scalars) followed by FP64 refinement until the
+    explicit residual ||H psi - E psi|| / |E| <= tol.  `start`: host FP32
+    vector (float32 for real operators, complex64 otherwise), or
+    `start_device`: a device pointer to one; neither: GPU random start."""
+    return _two_phase(lib().qkrylov_b200_lanczos_mixed, H, seed, start, start_device, maxiter, tol, eigenvector,
+                      True)
+
+
+def lanczos_fp64(H: MatrixFreeHamiltonian, seed: int = 0, start: Optional[np.ndarray] = None,
+                 maxiter: int = 200, tol: float = 1e-10, start_device: Optional[int] = None,
+                 eigenvector: bool = False) -> MixedLanczosResult:
+    """Plain FP64 Lanczos with lanczos_mixed's stopping rule (the baseline of
+    time-to-E0 comparisons); `start` is float64 / complex128."""
+    return _two_phase(lib().qkrylov_b200_lanczos_fp64, H, seed, start, start_device, maxiter, tol, eigenvector,
+                      False)
+
+
 class DavidsonResult:
     def __init__(self, eigenvalues, eigenvectors, iterations=0, converged=False):
         self.eigenvalues, self.eigenvectors = eigenvalues, eigenvectors
@@ -590,6 +654,13 @@ class _LanczosF64(ctypes.Structure):
 
 class _LanczosC(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_float), ("iterations", ctypes.c_int), ("converged", ctypes.c_int)]
+
+
+class _MixedC(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("residual", ctypes.c_double), ("seconds_low", ctypes.c_double),
+                ("seconds_high", ctypes.c_double), ("iterations_low", ctypes.c_int),
+                ("iterations_high", ctypes.c_int), ("restarts", ctypes.c_int), ("converged", ctypes.c_int),
+                ("trace_len", ctypes.c_int)]
 
 
 class _DavidsonInfo(ctypes.Structure):

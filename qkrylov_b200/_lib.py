@@ -96,6 +96,8 @@ PROTOTYPES = {
     "qkrylov_continued_fraction_coeffs_f64": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "qkrylov_evaluate_spectral_function_f64": (_d, [_vp, _vp, _sz, _d, _d, _d, _d]),
     "qkrylov_ftlm_sweep_f64": (_i, [_vp, _i, _vp, _i, _i, _vp, _vp, _vp]),
+    "qkrylov_b200_lanczos_mixed": (_i, [_vp, _u64, _vp, _i, _i, _d, _vp, _vp, _i, _vp, _vp, _vp]),
+    "qkrylov_b200_lanczos_fp64": (_i, [_vp, _u64, _vp, _i, _i, _d, _vp, _vp, _i, _vp, _vp, _vp]),
 }
 
 _lock = threading.Lock()

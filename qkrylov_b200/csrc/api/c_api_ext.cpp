@@ -2,6 +2,7 @@
 // pointers, multi-temperature FTLM, compiler inspection, diagnostics.
 #include <cstring>
 #include <exception>
+#include <memory>
 
 #include "api/handles.hpp"
 #include "engine/solvers.hpp"
@@ -245,6 +246,66 @@ int qkrylov_lanczos_ground_state_f64(qkrylov_hamiltonian_h h, int maxiter, doubl
     if (betas) std::copy(r.betas.begin(), r.betas.end(), betas);
     return QKRYLOV_SUCCESS;
   });
+}
+
+static int lanczos_two_phase(qkrylov_hamiltonian_h h, bool low_phase, uint64_t seed, const void* start,
+                             int start_on_device, int maxiter, double tol, qkrylov_b200_mixed_result_t* result,
+                             void* psi_out, int trace_cap, int* trace_iteration, double* trace_energy,
+                             double* trace_seconds) {
+  if (!h || !h->op || !result || maxiter < 1 || maxiter > 511 || !(tol > 0) || trace_cap < 0)
+    return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const qkb::Operator& H = *h->op;
+    const uint64_t dim = H.dim();
+    const bool real = H.all_real();
+    const qk_dtype st = low_phase ? (real ? QK_F32 : QK_C64) : (real ? QK_F64 : QK_C128);
+    const qk_dtype hi = real ? QK_F64 : QK_C128;
+    std::unique_ptr<qkb::DevVec> sdev, pdev;
+    const void* sptr = start;
+    if (start && !start_on_device) {
+      sdev = std::make_unique<qkb::DevVec>(dim, st, H.device(), false);
+      qkb::cuda_check(cudaMemcpyAsync(sdev->data(), start, dim * qk_dtype_size(st), cudaMemcpyHostToDevice,
+                                      H.ctx().stream), "H2D");
+      sptr = sdev->data();
+    }
+    if (psi_out) pdev = std::make_unique<qkb::DevVec>(dim, hi, H.device(), false);
+    auto r = qkb::lanczos_mixed(H, sptr, seed, maxiter, tol, pdev ? pdev->data() : nullptr, low_phase);
+    if (psi_out) {
+      qkb::cuda_check(cudaMemcpyAsync(psi_out, pdev->data(), dim * qk_dtype_size(hi), cudaMemcpyDeviceToHost,
+                                      H.ctx().stream), "D2H");
+      H.ctx().sync();
+    }
+    result->energy = r.energy;
+    result->residual = r.residual;
+    result->seconds_low = r.seconds_low;
+    result->seconds_high = r.seconds_high;
+    result->iterations_low = r.iters_low;
+    result->iterations_high = r.iters_high;
+    result->restarts = r.restarts;
+    result->converged = r.converged;
+    const int n = int(std::min<size_t>(size_t(trace_cap), r.trace.size()));
+    for (int i = 0; i < n; ++i) {
+      if (trace_iteration) trace_iteration[i] = r.trace[i].iteration;
+      if (trace_energy) trace_energy[i] = r.trace[i].energy;
+      if (trace_seconds) trace_seconds[i] = r.trace[i].seconds;
+    }
+    result->trace_len = n;
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_lanczos_mixed(qkrylov_hamiltonian_h h, uint64_t seed, const void* start, int start_on_device,
+                               int maxiter, double tol, qkrylov_b200_mixed_result_t* result, void* psi_out,
+                               int trace_cap, int* trace_iteration, double* trace_energy, double* trace_seconds) {
+  return lanczos_two_phase(h, true, seed, start, start_on_device, maxiter, tol, result, psi_out, trace_cap,
+                           trace_iteration, trace_energy, trace_seconds);
+}
+
+int qkrylov_b200_lanczos_fp64(qkrylov_hamiltonian_h h, uint64_t seed, const void* start, int start_on_device,
+                              int maxiter, double tol, qkrylov_b200_mixed_result_t* result, void* psi_out,
+                              int trace_cap, int* trace_iteration, double* trace_energy, double* trace_seconds) {
+  return lanczos_two_phase(h, false, seed, start, start_on_device, maxiter, tol, result, psi_out, trace_cap,
+                           trace_iteration, trace_energy, trace_seconds);
 }
 
 int qkrylov_davidson_lowest_f64(qkrylov_hamiltonian_h h, int n_eig, int max_subspace, double tol, double* evals,

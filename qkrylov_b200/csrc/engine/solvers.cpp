@@ -265,34 +265,41 @@ CoreOut lanczos_core(const Operator& H, qk_dtype T, const void* start, int maxit
   return res;
 }
 
-MixedOut lanczos_mixed(const Operator& H, const void* start_low, uint64_t seed, int maxiter, double tol_res,
-                       void* psi_out) {
+MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int maxiter, double tol_res,
+                       void* psi_out, bool low_phase) {
   MixedOut out;
   const uint64_t dim = H.dim();
   if (dim == 0) return out;
+  if (maxiter < 1 || maxiter > 511) throw std::invalid_argument("qkrylov_b200: maxiter must be in [1, 511]");
   const bool real = H.all_real();
   const qk_dtype lo = real ? QK_F32 : QK_C64, hi = real ? QK_F64 : QK_C128;
   const double t0 = now_s();
   Dev dl(H, lo), dh(H, hi);
-  DevVec s0 = dl.vec(false);
-  if (start_low) qkd_check(qkd_copy(lo, dim, start_low, s0.data(), dl.c.stream), "copy");
-  else qkd_check(qkd_random(lo, dim, seed, 0, s0.data(), dl.c.stream), "random");
   DevVec psi = dh.vec(false);
-  // Phase 1: FP32 vectors until the Ritz value is settled to FP32 accuracy.
-  auto p1 = lanczos_core(H, lo, s0.data(), maxiter, 1e-8, 1e-5, hi, psi.data(), t0);
-  out.iters_low = p1.iterations;
-  out.trace = p1.trace;
+  double e = 0.0;
+  if (low_phase) {
+    // Phase 1: FP32 vectors until the Ritz value is settled to FP32 accuracy.
+    DevVec s0 = dl.vec(false);
+    if (start) qkd_check(qkd_copy(lo, dim, start, s0.data(), dl.c.stream), "copy");
+    else qkd_check(qkd_random(lo, dim, seed, 0, s0.data(), dl.c.stream), "random");
+    auto p1 = lanczos_core(H, lo, s0.data(), maxiter, 1e-8, 1e-5, hi, psi.data(), t0);
+    out.iters_low = p1.iterations;
+    out.trace = p1.trace;
+    e = p1.energy;
+  } else {
+    if (start) qkd_check(qkd_copy(hi, dim, start, psi.data(), dh.c.stream), "copy");
+    else qkd_check(qkd_random(hi, dim, seed, 0, psi.data(), dh.c.stream), "random");
+  }
   out.seconds_low = now_s() - t0;
-  // Phase 2: FP64 restarts from the current Ritz vector, each checked by an
-  // explicit FP64 residual.
+  // FP64 Lanczos restarted from the current vector, each restart checked by
+  // an explicit FP64 residual ||H psi - E psi|| / |E|.
   DevVec r = dh.vec(false);
   PtrArray P(1, H.device());
   P.set(0, r.data(), dh.c.stream);
-  double e = p1.energy;
   for (int rs = 0; rs < 8; ++rs) {
     auto p2 = lanczos_core(H, hi, psi.data(), maxiter, 0.0, 0.1 * tol_res, hi, psi.data(), t0);
     out.iters_high += p2.iterations;
-    for (auto te : p2.trace) { te.iteration += out.iters_low; out.trace.push_back(te); }
+    for (auto te : p2.trace) { te.iteration += out.iters_low + out.iters_high - p2.iterations; out.trace.push_back(te); }
     e = p2.energy;
     H.apply(hi, psi.data(), r.data());
     const void* U[1] = {psi.data()};

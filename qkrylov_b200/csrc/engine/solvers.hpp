@@ -80,6 +80,9 @@ CoreOut lanczos_core(const Operator& H, qk_dtype t, const void* start, int maxit
 // Lanczos restarted from the FP32 Ritz vector until the explicit FP64
 // residual ||H psi - E psi|| / |E| <= tol_res.  Real operators use real
 // vectors (float32 / float64), complex ones complex64 / complex128.
+// low_phase = false skips phase 1 (plain FP64 with the same stopping rule);
+// start (device, FP32 type with phase 1, FP64 type without) or, when null,
+// a device random start from seed.  maxiter <= 511 per restart.
 struct MixedOut {
   double energy = 0, residual = 0;
   int iters_low = 0, iters_high = 0, restarts = 0;
@@ -87,8 +90,8 @@ struct MixedOut {
   double seconds_low = 0, seconds_high = 0;
   std::vector<TraceEntry> trace;  // both phases, seconds from the start
 };
-MixedOut lanczos_mixed(const Operator& H, const void* start_low, uint64_t seed, int maxiter, double tol_res,
-                       void* psi_out_high);
+MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int maxiter, double tol_res,
+                       void* psi_out_high, bool low_phase = true);
 
 // src/solvers/dynamics.cpp:12-59
 template <class Real>

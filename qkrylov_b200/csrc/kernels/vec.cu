@@ -101,75 +101,196 @@ __global__ void k_normalize_into(size_t n, const double* nrm2, const void* x, vo
 
 struct UPack { const void* u[4]; double ar[4], ai[4]; };
 
-// Tiled multi-dot.  Each warp owns tiles of 32*E consecutive elements: the x
-// tile stays in registers (after the optional update by U) while the warp
-// streams the matching tile of every V_j and adds the warp-reduced partial
-// of <V_j, x> to its own slot in shared memory.
-template <int DT, int E>
+// 16-byte packs: W consecutive elements per lane and load (one complex128,
+// two complex64 or float64, four float32).
+template <int DT> struct Pk;
+template <> struct Pk<QK_C128> {
+  using V = double2; static constexpr int W = 1;
+  __device__ static void un(const V& v, double* re, double* im) { re[0] = v.x; im[0] = v.y; }
+  __device__ static V pk(const double* re, const double* im) { return make_double2(re[0], im[0]); }
+};
+template <> struct Pk<QK_C64> {
+  using V = float4; static constexpr int W = 2;
+  __device__ static void un(const V& v, double* re, double* im) { re[0] = v.x; im[0] = v.y; re[1] = v.z; im[1] = v.w; }
+  __device__ static V pk(const double* re, const double* im) {
+    return make_float4(float(re[0]), float(im[0]), float(re[1]), float(im[1]));
+  }
+};
+template <> struct Pk<QK_F64> {
+  using V = double2; static constexpr int W = 2;
+  __device__ static void un(const V& v, double* re, double* im) { re[0] = v.x; re[1] = v.y; im[0] = 0.0; im[1] = 0.0; }
+  __device__ static V pk(const double* re, const double*) { return make_double2(re[0], re[1]); }
+};
+template <> struct Pk<QK_F32> {
+  using V = float4; static constexpr int W = 4;
+  __device__ static void un(const V& v, double* re, double* im) {
+    re[0] = v.x; re[1] = v.y; re[2] = v.z; re[3] = v.w; im[0] = im[1] = im[2] = im[3] = 0.0;
+  }
+  __device__ static V pk(const double* re, const double*) {
+    return make_float4(float(re[0]), float(re[1]), float(re[2]), float(re[3]));
+  }
+};
+
+__device__ __forceinline__ bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Multi-dot with optional update, out_j = <V_j, x> after x -= sum_m a_m U_m.
+// Each warp owns tiles of 32*E packs of 16 bytes: the x tile stays in
+// registers (after the update) while the warp streams the matching tiles
+// of J vectors V_j at a time, all their loads in flight together, and adds
+// the warp-reduced partials to its own slots in shared memory.  The inner
+// loop is branch-free: a missing vector (j >= k) reads V_{k-1} with weight
+// 0 and a partial tile clamps its pack index with weight 0.  Elements past
+// the last whole pack are done by one warp with scalar loads.  If any
+// pointer is not 16-byte aligned the same scheme runs on single elements.
+template <int DT> struct MdotShape { static constexpr int E = 4, J = 4; };
+
+template <int DT, int W, class LD, class ST>
+__device__ __forceinline__ void mdot_tiles(size_t nq, int M, const UPack& U, int k, const void* const* sV,
+                                          void* x, double* wacc, LD ld, ST st) {
+  constexpr int E = MdotShape<DT>::E, J = MdotShape<DT>::J;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t tile = size_t(32) * E;
+  const size_t nwarps = size_t(gridDim.x) * (kThreads / 32);
+  for (size_t qb = (size_t(blockIdx.x) * (kThreads / 32) + warp) * tile; qb < nq; qb += nwarps * tile) {
+    const bool full = qb + tile <= nq;
+    size_t iq[E];
+    bool in[E];
+    #pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const size_t q = qb + size_t(e) * 32 + lane;
+      in[e] = full || q < nq;
+      iq[e] = in[e] ? q : nq - 1;
+    }
+    double xr[E][W], xi[E][W];
+    #pragma unroll
+    for (int e = 0; e < E; ++e) ld(x, iq[e], xr[e], xi[e], false);
+    if (M > 0) {
+      #pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        if (m >= M) break;
+        const double ar = U.ar[m], ai = U.ai[m];
+        #pragma unroll
+        for (int e = 0; e < E; ++e) {
+          double ur[W], ui[W];
+          ld(U.u[m], iq[e], ur, ui, true);
+          #pragma unroll
+          for (int w = 0; w < W; ++w) {
+            xr[e][w] -= ar * ur[w] - ai * ui[w];
+            xi[e][w] -= ar * ui[w] + ai * ur[w];
+          }
+        }
+      }
+      #pragma unroll
+      for (int e = 0; e < E; ++e)
+        if (in[e]) st(x, iq[e], xr[e], xi[e]);  // rounds xr, xi to the stored values
+    }
+    #pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (!in[e]) {
+        #pragma unroll
+        for (int w = 0; w < W; ++w) { xr[e][w] = 0.0; xi[e][w] = 0.0; }
+      }
+    for (int j0 = 0; j0 < k; j0 += J) {
+      double pr[J], pi[J];
+      #pragma unroll
+      for (int jj = 0; jj < J; ++jj) {
+        const void* vj = sV[j0 + jj < k ? j0 + jj : k - 1];
+        pr[jj] = 0.0; pi[jj] = 0.0;
+        #pragma unroll
+        for (int e = 0; e < E; ++e) {
+          double vr[W], vi[W];
+          ld(vj, iq[e], vr, vi, true);
+          #pragma unroll
+          for (int w = 0; w < W; ++w) {
+            pr[jj] += vr[w] * xr[e][w] + vi[w] * xi[e][w];
+            if (VT<DT>::cplx) pi[jj] += vr[w] * xi[e][w] - vi[w] * xr[e][w];
+          }
+        }
+      }
+      #pragma unroll
+      for (int jj = 0; jj < J; ++jj) {
+        pr[jj] = warp_sum(pr[jj]);
+        if (VT<DT>::cplx) pi[jj] = warp_sum(pi[jj]);
+      }
+      if (lane == 0) {
+        #pragma unroll
+        for (int jj = 0; jj < J; ++jj)
+          if (j0 + jj < k) { wacc[2 * (j0 + jj)] += pr[jj]; wacc[2 * (j0 + jj) + 1] += pi[jj]; }
+      }
+    }
+  }
+}
+
+template <int DT>
 __global__ void __launch_bounds__(kThreads)
 k_update_mdot(size_t n, int M, UPack U, int k,
               const void* const* __restrict__ V, void* x, double* partials, unsigned* ticket,
               double* out) {
   using T = VT<DT>;
   using R = typename T::R;
-  extern __shared__ double sacc[];  // [8 warps][k][2]
+  using P = Pk<DT>;
+  constexpr int W = P::W;
+  extern __shared__ double sacc[];  // [8 warps][k][2], then k pointers
+  const void** sV = reinterpret_cast<const void**>(sacc + size_t(kThreads / 32) * k * 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* wacc = sacc + size_t(warp) * k * 2;
   for (int j = lane; j < k; j += 32) { wacc[2 * j] = 0.0; wacc[2 * j + 1] = 0.0; }
-  __syncwarp();
-  const size_t tile = size_t(32) * E;
-  const size_t nwarps = size_t(gridDim.x) * (kThreads / 32);
-  for (size_t base = (size_t(blockIdx.x) * (kThreads / 32) + warp) * tile; base < n; base += nwarps * tile) {
-    double xr[E], xi[E];
-    #pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const size_t i = base + size_t(e) * 32 + lane;
-      xr[e] = 0.0; xi[e] = 0.0;
-      if (i < n) {
-        R r, m; T::ld_plain(x, i, r, m); xr[e] = r; xi[e] = m;
+  bool ok = al16(x);
+  for (int m = 0; m < M; ++m) ok = ok && al16(U.u[m]);
+  for (int j = threadIdx.x; j < k; j += kThreads) {
+    sV[j] = V[j];
+    ok = ok && al16(sV[j]);
+  }
+  ok = __syncthreads_and(ok) != 0;
+  if (ok && W > 1) {
+    auto ld = [](const void* p, size_t q, double* re, double* im, bool ro) {
+      const typename P::V* v = reinterpret_cast<const typename P::V*>(p) + q;
+      P::un(ro ? __ldg(v) : *v, re, im);
+    };
+    auto st = [](void* p, size_t q, double* re, double* im) {
+      const typename P::V v = P::pk(re, im);
+      reinterpret_cast<typename P::V*>(p)[q] = v;
+      P::un(v, re, im);
+    };
+    const size_t nq = n / W;
+    mdot_tiles<DT, W>(nq, M, U, k, sV, x, wacc, ld, st);
+    // elements past the last whole pack: one warp, scalar
+    if (blockIdx.x == 0 && warp == 0 && nq * W < n) {
+      const size_t i = nq * W + lane;
+      const bool in = i < n;
+      double xr = 0.0, xi = 0.0;
+      if (in) {
+        R r, m; T::ld_plain(x, in ? i : 0, r, m); xr = r; xi = m;
+        for (int mm = 0; mm < M; ++mm) {
+          R ur, ui; T::ld(U.u[mm], i, ur, ui);
+          xr -= U.ar[mm] * double(ur) - U.ai[mm] * double(ui);
+          xi -= U.ar[mm] * double(ui) + U.ai[mm] * double(ur);
+        }
+        if (M > 0) { T::st(x, i, R(xr), R(xi)); xr = double(R(xr)); xi = double(R(xi)); }
+      }
+      for (int j = 0; j < k; ++j) {
+        double pr = 0.0, pi = 0.0;
+        if (in) {
+          R vr, vi; T::ld(sV[j], i, vr, vi);
+          pr = double(vr) * xr + double(vi) * xi;
+          pi = double(vr) * xi - double(vi) * xr;
+        }
+        pr = warp_sum(pr);
+        pi = warp_sum(pi);
+        if (lane == 0) { wacc[2 * j] += pr; wacc[2 * j + 1] += pi; }
       }
     }
-    if (M > 0) {
-      #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        if (m >= M) break;
-        const void* um = U.u[m];
-        const double ar = U.ar[m], ai = U.ai[m];
-        #pragma unroll
-        for (int e = 0; e < E; ++e) {
-          const size_t i = base + size_t(e) * 32 + lane;
-          if (i < n) {
-            R ur, ui; T::ld(um, i, ur, ui);
-            xr[e] -= ar * double(ur) - ai * double(ui);
-            xi[e] -= ar * double(ui) + ai * double(ur);
-          }
-        }
-      }
-      #pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const size_t i = base + size_t(e) * 32 + lane;
-        if (i < n) {
-          T::st(x, i, R(xr[e]), R(xi[e]));
-          xr[e] = double(R(xr[e])); xi[e] = double(R(xi[e]));  // dot the stored values
-        }
-      }
-    }
-    for (int j = 0; j < k; ++j) {
-      const void* vj = V[j];
-      double pr = 0.0, pi = 0.0;
-      #pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const size_t i = base + size_t(e) * 32 + lane;
-        if (i < n) {
-          R vr, vi; T::ld(vj, i, vr, vi);
-          pr += double(vr) * xr[e] + double(vi) * xi[e];
-          pi += double(vr) * xi[e] - double(vi) * xr[e];
-        }
-      }
-      pr = warp_sum(pr);
-      pi = warp_sum(pi);
-      if (lane == 0) { wacc[2 * j] += pr; wacc[2 * j + 1] += pi; }
-    }
+  } else {
+    auto ld = [](const void* p, size_t i, double* re, double* im, bool ro) {
+      R r, m;
+      if (ro) T::ld(p, i, r, m); else T::ld_plain(p, i, r, m);
+      re[0] = r; im[0] = m;
+    };
+    auto st = [](void* p, size_t i, double* re, double* im) {
+      T::st(p, i, R(re[0]), R(im[0]));
+      re[0] = double(R(re[0])); im[0] = double(R(im[0]));
+    };
+    mdot_tiles<DT, 1>(n, M, U, k, sV, x, wacc, ld, st);
   }
   __syncthreads();
   const int G = gridDim.x;
@@ -182,24 +303,64 @@ k_update_mdot(size_t n, int M, UPack U, int k,
   grid_finish(partials, ticket, k, out);
 }
 
-// x <- x - sum_j c_j V_j, optional ||x||^2.
+// x <- x - sum_j c_j V_j, optional ||x||^2.  Coefficients and V_j pointers
+// are staged in shared memory; with 16-byte aligned pointers each thread
+// handles 16-byte packs, and the j loop is unrolled so several vectors'
+// loads are in flight at once.
 template <int DT, bool NRM>
 __global__ void __launch_bounds__(kThreads)
 k_mupdate(size_t n, int k, const void* const* __restrict__ V, const double* __restrict__ c, void* x,
           double* partials, unsigned* ticket, double* nrm2) {
   using T = VT<DT>;
   using R = typename T::R;
-  extern __shared__ double sc[];  // 2k coefficients, then 2*8 reduction scratch
+  using P = Pk<DT>;
+  constexpr int W = P::W;
+  extern __shared__ double sc[];  // 2k coefficients, 2*8 reduction scratch, then k pointers
+  const void** sV = reinterpret_cast<const void**>(sc + 2 * k + 16);
+  bool ok = al16(x);
   for (int j = threadIdx.x; j < 2 * k; j += kThreads) sc[j] = c[j];
-  __syncthreads();
+  for (int j = threadIdx.x; j < k; j += kThreads) {
+    sV[j] = V[j];
+    ok = ok && al16(sV[j]);
+  }
+  ok = __syncthreads_and(ok) != 0;
   double acc = 0.0;
-  for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n; i += size_t(gridDim.x) * kThreads) {
+  size_t done = 0;  // elements handled by the pack loop
+  if (ok && W > 1) {
+    const size_t nq = n / W;
+    done = nq * W;
+    using PV = typename P::V;
+    for (size_t q = blockIdx.x * size_t(kThreads) + threadIdx.x; q < nq; q += size_t(gridDim.x) * kThreads) {
+      double xr[W], xi[W];
+      P::un(reinterpret_cast<const PV*>(x)[q], xr, xi);
+      #pragma unroll 4
+      for (int j = 0; j < k; ++j) {
+        double vr[W], vi[W];
+        P::un(__ldg(reinterpret_cast<const PV*>(sV[j]) + q), vr, vi);
+        const double cr = sc[2 * j], ci = sc[2 * j + 1];
+        #pragma unroll
+        for (int w = 0; w < W; ++w) {
+          xr[w] -= cr * vr[w] - ci * vi[w];
+          if (T::cplx) xi[w] -= cr * vi[w] + ci * vr[w];
+        }
+      }
+      const PV v = P::pk(xr, xi);
+      reinterpret_cast<PV*>(x)[q] = v;
+      if (NRM) {
+        P::un(v, xr, xi);
+        #pragma unroll
+        for (int w = 0; w < W; ++w) acc += xr[w] * xr[w] + xi[w] * xi[w];
+      }
+    }
+  }
+  for (size_t i = done + blockIdx.x * size_t(kThreads) + threadIdx.x; i < n; i += size_t(gridDim.x) * kThreads) {
     R r0, i0; T::ld_plain(x, i, r0, i0);
     double xr = r0, xi = i0;
+    #pragma unroll 8
     for (int j = 0; j < k; ++j) {
-      R vr, vi; T::ld(V[j], i, vr, vi);
+      R vr, vi; T::ld(sV[j], i, vr, vi);
       xr -= sc[2 * j] * double(vr) - sc[2 * j + 1] * double(vi);
-      xi -= sc[2 * j] * double(vi) + sc[2 * j + 1] * double(vr);
+      if (T::cplx) xi -= sc[2 * j] * double(vi) + sc[2 * j + 1] * double(vr);
     }
     const R sr = R(xr), si = R(xi);
     T::st(x, i, sr, si);
@@ -314,12 +475,12 @@ int qkd_update_mdot(qk_workspace* w, qk_dtype t, size_t n, int M, const void* co
   UPack up{};
   for (int m = 0; m < M; ++m) { up.u[m] = U[m]; up.ar[m] = a[2 * m]; up.ai[m] = a[2 * m + 1]; }
   const unsigned G = std::min<unsigned>(reduce_grid(n), kMaxG);
-  const size_t smem = size_t(kThreads / 32) * std::max(k, 1) * 2 * sizeof(double);
+  const size_t smem = size_t(kThreads / 32) * std::max(k, 1) * 2 * sizeof(double) + size_t(k) * sizeof(void*);
   if (smem > 48 * 1024) {
-    QKD_DISPATCH(t, cudaFuncSetAttribute(k_update_mdot<DT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    QKD_DISPATCH(t, cudaFuncSetAttribute(k_update_mdot<DT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   }
-  QKD_DISPATCH(t, k_update_mdot<DT, 8><<<G, kThreads, smem, s>>>(n, M, up, k, V, x, w->partials,
-                                                                 w->ticket, out));
+  QKD_DISPATCH(t, k_update_mdot<DT><<<G, kThreads, smem, s>>>(n, M, up, k, V, x, w->partials,
+                                                              w->ticket, out));
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
@@ -344,7 +505,7 @@ int qkd_mupdate(qk_workspace* w, qk_dtype t, size_t n, int k, const void* const*
                 const double* c, void* x, double* nrm2, cudaStream_t s) {
   if (!w || !x || k < 0 || k > kMaxK || (k > 0 && (!V || !c))) return QKD_EINVAL;
   const unsigned G = std::min<unsigned>(reduce_grid(n), kMaxG);
-  const size_t smem = (2 * size_t(k) + 16) * sizeof(double);
+  const size_t smem = (2 * size_t(k) + 16) * sizeof(double) + size_t(k) * sizeof(void*);
   if (nrm2) {
     QKD_DISPATCH(t, k_mupdate<DT, true><<<G, kThreads, smem, s>>>(n, k, V, c, x, w->partials, w->ticket, nrm2));
   } else {
