@@ -149,30 +149,33 @@ int qkrylov_ftlm_sweep_f64(qkrylov_hamiltonian_h h, int n_beta, const double* be
                            double* Z_out, double* U_out, double* Cv_out);
 
 /* ------------------------------------------------ mixed-precision Lanczos
- * No counterpart in the reference.  Lanczos with full reorthogonalisation
- * whose vectors and H.x are FP32 (float32 for a real operator, complex64
- * otherwise) while alpha, beta, the reorthogonalisation coefficients, the
- * norms and the tridiagonal eigensolve are FP64.  It stops when the Ritz
- * value settles (|dE| < 1e-8 |E|) or the residual estimate beta_k |z_k|
- * drops below 1e-5 |E|; FP64 Lanczos (float64 / complex128 vectors) then
- * restarts from that Ritz vector until the explicit FP64 residual
- * ||H psi - E psi|| / |E| <= tol, at most 8 restarts of up to maxiter
- * (<= 511) steps each.
+ * No counterpart in the reference.  The iterate psi, its energy E and the
+ * residual r = H psi - E psi are FP64 (float64 for a real operator,
+ * complex128 otherwise; one FP64 apply per outer step).  Each correction
+ * comes from a Lanczos pass on FP32 vectors (float32 / complex64 H.x and
+ * vectors; alpha, beta, reorthogonalisation coefficients, norms and the
+ * tridiagonal eigensolve in FP64) over the Krylov space of r kept
+ * orthogonal to psi, followed by the Rayleigh-Ritz step on span{psi, v_1..
+ * v_m}.  It stops when ||H psi - E psi|| / |E| <= tol; a pass stops when
+ * its Ritz residual estimate drops below max(0.3 tol, 1e-6 |r| / |E|) or
+ * after maxiter (<= 511) steps; a pass that fails to halve the residual
+ * switches the remaining passes to FP64.
  *   start: NULL for a random start generated on the GPU from `seed`
  *          (uniform in [-1, 1)), else dimension() elements of the FP32
  *          vector type, in host memory, or in device memory of the
  *          operator's GPU when start_on_device is non-zero.
  *   psi_out: NULL, or host memory for the normalised FP64 ground state.
- *   trace_*: NULL, or trace_cap entries receiving (iteration, Ritz value,
- *          seconds since the call started) for every step of both phases. */
+ *   trace_*: NULL, or trace_cap entries receiving (step, energy or Ritz
+ *          value, seconds since the call started) for every FP32 step and
+ *          every FP64 residual evaluation. */
 typedef struct {
   double energy;
   double residual;      /* explicit ||H psi - E psi|| / |E| of psi_out */
-  double seconds_low;   /* wall time of the FP32 phase (with start set-up) */
-  double seconds_high;  /* wall time of the FP64 phase and residual checks */
-  int iterations_low;
-  int iterations_high;
-  int restarts;
+  double seconds_low;   /* wall time in FP32 passes (and start set-up) */
+  double seconds_high;  /* wall time in FP64 applies, residuals and passes */
+  int iterations_low;   /* FP32 Lanczos steps */
+  int iterations_high;  /* FP64 Lanczos steps and residual applies */
+  int restarts;         /* refinement passes (plain FP64: Lanczos runs) */
   int converged;
   int trace_len;
 } qkrylov_b200_mixed_result_t;
@@ -181,9 +184,10 @@ int qkrylov_b200_lanczos_mixed(qkrylov_hamiltonian_h h, uint64_t seed, const voi
                                int maxiter, double tol, qkrylov_b200_mixed_result_t* result, void* psi_out,
                                int trace_cap, int* trace_iteration, double* trace_energy, double* trace_seconds);
 
-/* The FP64 phase alone from the start (FP64 vector type) or a random FP64
- * start: plain FP64 Lanczos with the same explicit-residual stopping rule,
- * the baseline the mixed form is timed against. */
+/* Plain FP64 Lanczos with full reorthogonalisation from the start (FP64
+ * vector type) or a random FP64 start, restarted from its Ritz vector (at
+ * most 8 runs of up to maxiter steps) until the explicit residual meets
+ * tol: the baseline the mixed form is timed against. */
 int qkrylov_b200_lanczos_fp64(qkrylov_hamiltonian_h h, uint64_t seed, const void* start, int start_on_device,
                               int maxiter, double tol, qkrylov_b200_mixed_result_t* result, void* psi_out,
                               int trace_cap, int* trace_iteration, double* trace_energy, double* trace_seconds);

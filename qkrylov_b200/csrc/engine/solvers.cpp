@@ -265,6 +265,70 @@ CoreOut lanczos_core(const Operator& H, qk_dtype T, const void* start, int maxit
   return res;
 }
 
+namespace {
+// One refinement pass: Lanczos in dtype ti on the Krylov space of r = H psi -
+// E psi, kept orthogonal to psi, then psi <- the Ritz vector of
+// span{psi, v_1..v_m}.  With v_1 = r / |r| the projection of H onto that
+// span is the tridiagonal [E, |r|; |r|, a_1, b_1; ...], so the Rayleigh-Ritz
+// step needs no further products.  The v_j can be FP32: they only carry the
+// correction, whose size is that of the residual, so their rounding enters
+// psi at (FP32 epsilon) x |r|.  Stops when the Ritz residual estimate
+// b_m |z_m| / |theta| <= target, at breakdown or after maxiter steps.
+int refine_pass(const Operator& H, qk_dtype ti, qk_dtype hi, DevVec& psi, const DevVec& r, double E, double nr,
+                int maxiter, double target, std::vector<DevVec>& V, DevVec& psi_t, DevVec& wt, DevVec& tmp,
+                PtrArray& P, DevVec& coef, std::vector<TraceEntry>& trace, int it0, double t0) {
+  Dev d(H, ti), dh(H, hi);
+  const uint64_t dim = H.dim();
+  double* cd = static_cast<double*>(coef.data());
+  if (ti == hi) qkd_check(qkd_copy(hi, dim, psi.data(), psi_t.data(), d.c.stream), "copy");
+  else qkd_check(qkd_convert(hi, psi.data(), ti, psi_t.data(), dim, d.c.stream), "convert");
+  while (V.size() < 1) V.push_back(d.vec(false));
+  qkd_check(qkd_convert(hi, r.data(), ti, V[0].data(), dim, d.c.stream), "convert");
+  d.scal(1.0 / nr, V[0].data());
+  P.set(0, psi_t.data(), d.c.stream);
+  P.set(1, V[0].data(), d.c.stream);
+  std::vector<double> a{E}, b{nr}, z;
+  int m = 0;
+  for (int j = 0; j < maxiter; ++j) {
+    m = j + 1;
+    H.apply_dot(ti, V[j].data(), wt.data(), d.c.dres(0));
+    const double alpha = d.c.fetch(d.c.dres(0), 1)[0];
+    a.push_back(alpha);
+    const void* U[2] = {V[j].data(), j > 0 ? V[j - 1].data() : nullptr};
+    const double co[4] = {alpha, 0.0, j > 0 ? b.back() : 0.0, 0.0};
+    const int np = j + 2;  // psi_t, v_1..v_{j+1}
+    P.set(np, wt.data(), d.c.stream);
+    d.update_mdot(j > 0 ? 2 : 1, U, co, P, np + 1, wt.data(), cd);
+    d.mupdate(P, np, cd, wt.data(), cd + 2 * (np + 1));
+    const double* hh = d.c.fetch(cd + 2 * np, 4);
+    double after = hh[2];
+    if (after < 0.25 * hh[0]) {
+      d.update_mdot(0, nullptr, nullptr, P, np, wt.data(), cd);
+      d.mupdate(P, np, cd, wt.data(), cd + 2 * (np + 1));
+      after = d.c.fetch(cd + 2 * (np + 1), 1)[0];
+    }
+    const double beta = std::sqrt(after);
+    const double theta = tridiag_ground<double>(a, b, int(a.size()), &z);
+    const double est = beta * std::abs(z.back()) / std::abs(theta);
+    trace.push_back({it0 + m, theta, now_s() - t0, est});
+    if (est <= target || beta < 1e-15 || j + 1 == maxiter) break;
+    b.push_back(beta);
+    if (int(V.size()) < j + 2) V.push_back(d.vec(false));
+    d.scale_into(1.0 / beta, wt.data(), V[j + 1].data());
+    P.set(j + 2, V[j + 1].data(), d.c.stream);
+  }
+  // psi <- z_0 psi + sum_i z_i v_i, assembled in FP64, normalised
+  std::vector<double> cz(2 * size_t(m), 0.0);
+  for (int i = 0; i < m; ++i) cz[2 * i] = z[i + 1];
+  cuda_check(cudaMemcpyAsync(cd, cz.data(), sizeof(double) * 2 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
+  qkd_check(qkd_combine(ti, dim, m, P.at(1), cd, hi, tmp.data(), d.c.stream), "combine");
+  qkd_check(qkd_axpby(hi, dim, 1.0, 0.0, tmp.data(), z[0], 0.0, psi.data(), d.c.stream), "axpby");
+  const double np2 = dh.dot(psi.data(), psi.data()).real();
+  dh.scal(1.0 / std::sqrt(np2), psi.data());
+  return m;
+}
+}  // namespace
+
 MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int maxiter, double tol_res,
                        void* psi_out, bool low_phase) {
   MixedOut out;
@@ -274,44 +338,88 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
   const bool real = H.all_real();
   const qk_dtype lo = real ? QK_F32 : QK_C64, hi = real ? QK_F64 : QK_C128;
   const double t0 = now_s();
-  Dev dl(H, lo), dh(H, hi);
-  DevVec psi = dh.vec(false);
-  double e = 0.0;
-  if (low_phase) {
-    // Phase 1: FP32 vectors until the Ritz value is settled to FP32 accuracy.
+  Dev dh(H, hi);
+  DevVec psi = dh.vec(false), w = dh.vec(false);
+  PtrArray Pw(1, H.device());
+  Pw.set(0, w.data(), dh.c.stream);
+  // E = <psi, H psi> and w <- H psi - E psi, |w|^2 (one FP64 apply)
+  auto residual = [&](double& E) {
+    H.apply_dot(hi, psi.data(), w.data(), dh.c.dres(0));
+    E = dh.c.fetch(dh.c.dres(0), 1)[0];
+    const void* U[1] = {psi.data()};
+    const double co[2] = {E, 0.0};
+    dh.update_mdot(1, U, co, Pw, 1, w.data(), dh.c.dres(0));
+    return std::sqrt(dh.c.fetch(dh.c.dres(0), 1)[0]);
+  };
+  if (!low_phase) {
+    // plain FP64: Lanczos from the start, restarted from the Ritz vector
+    // until the explicit residual meets tol_res
+    if (start) qkd_check(qkd_copy(hi, dim, start, psi.data(), dh.c.stream), "copy");
+    else qkd_check(qkd_random(hi, dim, seed, 0, psi.data(), dh.c.stream), "random");
+    double e = 0.0;
+    for (int rs = 0; rs < 8; ++rs) {
+      auto p2 = lanczos_core(H, hi, psi.data(), maxiter, 0.0, 0.1 * tol_res, hi, psi.data(), t0);
+      out.iters_high += p2.iterations;
+      for (auto te : p2.trace) { te.iteration += out.iters_high - p2.iterations; out.trace.push_back(te); }
+      const double nr = residual(e);
+      out.residual = nr / std::abs(e);
+      out.restarts = rs + 1;
+      if (out.residual <= tol_res) { out.converged = true; break; }
+    }
+    out.energy = e;
+    out.seconds_high = now_s() - t0;
+    if (psi_out) qkd_check(qkd_copy(hi, dim, psi.data(), psi_out, dh.c.stream), "copy");
+    dh.c.sync();
+    return out;
+  }
+  // Mixed: FP64 iterate psi and FP64 residuals; the Krylov passes that
+  // build each correction run on FP32 vectors (FP64 scalars).  A pass that
+  // fails to halve the residual switches the passes to FP64.
+  {
+    Dev dl(H, lo);
     DevVec s0 = dl.vec(false);
     if (start) qkd_check(qkd_copy(lo, dim, start, s0.data(), dl.c.stream), "copy");
     else qkd_check(qkd_random(lo, dim, seed, 0, s0.data(), dl.c.stream), "random");
-    auto p1 = lanczos_core(H, lo, s0.data(), maxiter, 1e-8, 1e-5, hi, psi.data(), t0);
-    out.iters_low = p1.iterations;
-    out.trace = p1.trace;
-    e = p1.energy;
-  } else {
-    if (start) qkd_check(qkd_copy(hi, dim, start, psi.data(), dh.c.stream), "copy");
-    else qkd_check(qkd_random(hi, dim, seed, 0, psi.data(), dh.c.stream), "random");
+    qkd_check(qkd_convert(lo, s0.data(), hi, psi.data(), dim, dl.c.stream), "convert");
+    const double n0 = std::sqrt(dh.dot(psi.data(), psi.data()).real());
+    if (n0 == 0.0) throw std::invalid_argument("qkrylov_b200: zero start vector");
+    dh.scal(1.0 / n0, psi.data());
   }
-  out.seconds_low = now_s() - t0;
-  // FP64 Lanczos restarted from the current vector, each restart checked by
-  // an explicit FP64 residual ||H psi - E psi|| / |E|.
-  DevVec r = dh.vec(false);
-  PtrArray P(1, H.device());
-  P.set(0, r.data(), dh.c.stream);
-  for (int rs = 0; rs < 8; ++rs) {
-    auto p2 = lanczos_core(H, hi, psi.data(), maxiter, 0.0, 0.1 * tol_res, hi, psi.data(), t0);
-    out.iters_high += p2.iterations;
-    for (auto te : p2.trace) { te.iteration += out.iters_low + out.iters_high - p2.iterations; out.trace.push_back(te); }
-    e = p2.energy;
-    H.apply(hi, psi.data(), r.data());
-    const void* U[1] = {psi.data()};
-    const double co[2] = {e, 0.0};
-    dh.update_mdot(1, U, co, P, 1, r.data(), dh.c.dres(0));
-    const double rn = std::sqrt(dh.c.fetch(dh.c.dres(0), 1)[0]);
-    out.residual = rn / std::abs(e);
-    out.restarts = rs + 1;
-    if (out.residual <= tol_res) { out.converged = true; break; }
+  std::vector<DevVec> V;
+  qk_dtype ti = lo;
+  DevVec psi_t(dim, ti, H.device(), false), wt(dim, ti, H.device(), false), tmp = dh.vec(false);
+  PtrArray P(size_t(maxiter) + 3, H.device());
+  DevVec coef(size_t(2) * (maxiter + 8), QK_F64, H.device());
+  double e = 0.0, eps_prev = 1e300, t_fp64 = 0.0;
+  int steps = 0;
+  for (int outer = 0; outer < 40; ++outer) {
+    const double tr0 = now_s();
+    const double nr = residual(e);
+    t_fp64 += now_s() - tr0;
+    const double eps = nr / std::abs(e);
+    out.iters_high += 1;
+    out.trace.push_back({steps + out.iters_high, e, now_s() - t0, eps});
+    out.residual = eps;
+    out.restarts = outer;
+    if (eps <= tol_res || nr == 0.0) { out.converged = true; break; }
+    if (ti == lo && outer > 0 && eps > 0.5 * eps_prev) {
+      ti = hi;  // FP32 passes stopped helping: finish in FP64
+      V.clear();
+      psi_t = DevVec(dim, ti, H.device(), false);
+      wt = DevVec(dim, ti, H.device(), false);
+    }
+    eps_prev = eps;
+    const double target = std::max(0.3 * tol_res, 1e-6 * eps);
+    const double tp0 = now_s();
+    const int m = refine_pass(H, ti, hi, psi, w, e, nr, maxiter, target, V, psi_t, wt, tmp, P, coef, out.trace,
+                              steps + out.iters_high, t0);
+    steps += m;
+    if (ti == lo) out.iters_low += m;
+    else { out.iters_high += m; t_fp64 += now_s() - tp0; }
   }
   out.energy = e;
-  out.seconds_high = now_s() - t0 - out.seconds_low;
+  out.seconds_high = t_fp64;
+  out.seconds_low = now_s() - t0 - t_fp64;
   if (psi_out) qkd_check(qkd_copy(hi, dim, psi.data(), psi_out, dh.c.stream), "copy");
   dh.c.sync();
   return out;

@@ -76,19 +76,27 @@ struct CoreOut {
 CoreOut lanczos_core(const Operator& H, qk_dtype t, const void* start, int maxiter, double tol_dE,
                      double tol_res, qk_dtype tout, void* ritz, double t0_seconds);
 
-// Mixed precision: phase 1 on FP32 vectors (FP64 scalars), then FP64
-// Lanczos restarted from the FP32 Ritz vector until the explicit FP64
-// residual ||H psi - E psi|| / |E| <= tol_res.  Real operators use real
-// vectors (float32 / float64), complex ones complex64 / complex128.
-// low_phase = false skips phase 1 (plain FP64 with the same stopping rule);
-// start (device, FP32 type with phase 1, FP64 type without) or, when null,
-// a device random start from seed.  maxiter <= 511 per restart.
+// Mixed precision.  The iterate psi, its Rayleigh quotient E and the
+// residual r = H psi - E psi are FP64 (one FP64 apply per outer step); each
+// correction comes from a Lanczos pass on FP32 vectors (FP64 alpha, beta,
+// reorthogonalisation coefficients and tridiagonal) over the Krylov space
+// of r kept orthogonal to psi, followed by the Rayleigh-Ritz step on
+// span{psi, v_1..v_m}.  A pass stops when its Ritz residual estimate falls
+// below max(0.3 tol, 1e-6 |r|/|E|); the loop ends when the explicit FP64
+// residual |r| / |E| <= tol_res.  A pass that fails to halve the residual
+// switches the passes to FP64.  Real operators use float32 / float64
+// vectors, complex ones complex64 / complex128.
+// low_phase = false: plain FP64 Lanczos from the start (restarted from the
+// Ritz vector, at most 8 times) with the same explicit-residual stopping
+// rule.  start: device vector of the FP32 type (mixed) or FP64 type
+// (plain); null: a device random start from seed.  maxiter <= 511 steps
+// per pass.
 struct MixedOut {
   double energy = 0, residual = 0;
-  int iters_low = 0, iters_high = 0, restarts = 0;
+  int iters_low = 0, iters_high = 0, restarts = 0;  // FP32 steps; FP64 steps and applies; outer steps
   bool converged = false;
-  double seconds_low = 0, seconds_high = 0;
-  std::vector<TraceEntry> trace;  // both phases, seconds from the start
+  double seconds_low = 0, seconds_high = 0;         // wall time in FP32 passes / FP64 work
+  std::vector<TraceEntry> trace;                    // every step, seconds from the start
 };
 MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int maxiter, double tol_res,
                        void* psi_out_high, bool low_phase = true);

@@ -32,9 +32,10 @@ def test_mixed_heisenberg16_matches_reference(golden):
     assert abs(np.linalg.norm(r.eigenvector) - 1.0) < 1e-12
     assert residual(H, r.energy, r.eigenvector) < 2 * TOL
     assert r.iterations_low > 0 and r.iterations_high > 0
-    # Ritz values of the FP32 phase decrease monotonically (Cauchy interlacing)
-    e_low = [e for (it, e, s) in r.trace[:r.iterations_low]]
-    assert all(b <= a + 1e-6 * abs(a) for a, b in zip(e_low, e_low[1:]))
+    # energies and Ritz values decrease (Cauchy interlacing within a pass;
+    # across passes up to FP32 rounding of the correction)
+    es = [e for (it, e, s) in r.trace]
+    assert all(b <= a + 1e-6 * abs(a) for a, b in zip(es, es[1:]))
     assert [it for (it, e, s) in r.trace] == list(range(1, len(r.trace) + 1))
 
 
@@ -52,7 +53,7 @@ def test_fp64_baseline_reaches_the_same_energy(golden):
     m = golden["models"]["heis16_sz0"]
     H = ham("spin", 16, m["sector"], O.heisenberg_chain(16))
     r = qk.lanczos_fp64(H, seed=5, tol=TOL, eigenvector=True)
-    assert r.converged and r.residual <= TOL and r.iterations_low == 0
+    assert r.converged and r.residual <= TOL and r.iterations_low == 0 and r.iterations_high > 0
     assert abs(r.energy - m["lanczos"]["energy"]) < 1e-10
     assert residual(H, r.energy, r.eigenvector) < 2 * TOL
 
