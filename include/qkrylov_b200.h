@@ -192,6 +192,42 @@ int qkrylov_b200_lanczos_fp64(qkrylov_hamiltonian_h h, uint64_t seed, const void
                               int maxiter, double tol, qkrylov_b200_mixed_result_t* result, void* psi_out,
                               int trace_cap, int* trace_iteration, double* trace_energy, double* trace_seconds);
 
+/* ---------------------------------------------------------- batched FTLM
+ * No counterpart in the reference (its ftlm, ftlm.hpp:21-27, runs one
+ * complex Gaussian vector at a time and one temperature per call).
+ * n_random (32, 64 or 128) seeded Rademacher (+-1) vectors advanced together
+ * as one block: each of the n_steps Lanczos steps (the reference's
+ * recurrence without reorthogonalisation, ftlm.cpp:24-53) is one block H.X
+ * with fused column dots, one column update with fused FP64 norms and one
+ * column scaling, with alpha and beta kept on the GPU; with use_graph the
+ * steps are captured once as a CUDA graph.  The block H.X tile shape (lanes
+ * per row) is autotuned on first use.  precision 32: float32 vectors
+ * (complex64 for a complex operator), FP64 dots, norms and tridiagonals;
+ * 64: float64 / complex128.  For each of the n_temps temperatures T (> 0):
+ * logZ = log Z, U = <H>, Cv = beta^2 (<H^2> - <H>^2), beta = 1/T, with
+ * Z = (1/R) sum_r sum_i |r|^2 z_0i^2 exp(-beta e_i) evaluated with the
+ * lowest Ritz value as energy shift (no overflow at low T). */
+typedef struct {
+  double seconds;         /* whole call */
+  double seconds_device;  /* the Lanczos steps (graph replay: CUDA events) */
+  double e_min;           /* lowest Ritz value over all vectors */
+  int lanes_per_row;      /* block H.X shape chosen by the autotuner */
+  int graph;
+  int vectors;
+  int steps;
+} qkrylov_b200_ftlm_info_t;
+
+int qkrylov_b200_ftlm_block(qkrylov_hamiltonian_h h, int precision, int n_random, int n_steps, uint64_t seed,
+                            int n_temps, const double* temps, double* logZ, double* U, double* Cv, int use_graph,
+                            qkrylov_b200_ftlm_info_t* info);
+
+/* The same random vectors (columns 0..n_vectors-1 of the n_random block)
+ * run one at a time through the single-vector kernels: the one-vector
+ * loop the batched form is measured against. */
+int qkrylov_b200_ftlm_loop(qkrylov_hamiltonian_h h, int precision, int n_random, int n_steps, uint64_t seed,
+                           int n_vectors, int n_temps, const double* temps, double* logZ, double* U, double* Cv,
+                           qkrylov_b200_ftlm_info_t* info);
+
 #ifdef __cplusplus
 }
 #endif

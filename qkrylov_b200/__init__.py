@@ -526,6 +526,49 @@ def lanczos_fp64(H: MatrixFreeHamiltonian, seed: int = 0, start: Optional[np.nda
                       False)
 
 
+class FTLMBlockResult:
+    """Thermodynamics at each temperature (log Z, U, Cv arrays) plus timing:
+    seconds (whole call), seconds_device (the Lanczos steps), the autotuned
+    block H.X shape (lanes_per_row) and whether a CUDA graph ran."""
+
+    def __init__(self, temps, logZ, U, Cv, info):
+        self.temperatures, self.logZ, self.U, self.Cv = temps, logZ, U, Cv
+        self.seconds, self.seconds_device = info.seconds, info.seconds_device
+        self.e_min, self.lanes_per_row, self.graph = info.e_min, info.lanes_per_row, bool(info.graph)
+        self.vectors, self.steps = info.vectors, info.steps
+
+    def __repr__(self):
+        return (f"FTLMBlockResult(vectors={self.vectors}, steps={self.steps}, seconds={self.seconds:.3f}, "
+                f"lanes_per_row={self.lanes_per_row}, graph={self.graph})")
+
+
+def _ftlm_call(fn, H, temps, extra):
+    T = np.ascontiguousarray(temps, dtype=np.float64)
+    lz, u, cv = np.zeros(T.size), np.zeros(T.size), np.zeros(T.size)
+    info = _FTLMInfo()
+    _check(fn(H._h, *extra[0], T.size, T.ctypes.data, lz.ctypes.data, u.ctypes.data, cv.ctypes.data, *extra[1],
+              ctypes.byref(info)), "ftlm")
+    return FTLMBlockResult(T, lz, u, cv, info)
+
+
+def ftlm_block(H: MatrixFreeHamiltonian, temperatures: Sequence[float], n_random: int = 64, n_steps: int = 100,
+               seed: int = 0, precision: int = 32, graph: bool = True) -> FTLMBlockResult:
+    """Batched FTLM: n_random (32/64/128) Rademacher vectors as one block,
+    n_steps Lanczos steps (one block H.X each, CUDA graph), Z/U/Cv at every
+    temperature.  precision 32: FP32 vectors with FP64 dots; 64: FP64."""
+    return _ftlm_call(lib().qkrylov_b200_ftlm_block, H, temperatures,
+                      ((precision, n_random, n_steps, ctypes.c_uint64(seed)), (int(graph),)))
+
+
+def ftlm_loop(H: MatrixFreeHamiltonian, temperatures: Sequence[float], n_random: int = 64, n_steps: int = 100,
+              seed: int = 0, precision: int = 64, n_vectors: Optional[int] = None) -> FTLMBlockResult:
+    """The same random vectors as ftlm_block run one at a time (the first
+    n_vectors of them; all by default)."""
+    nv = n_random if n_vectors is None else n_vectors
+    return _ftlm_call(lib().qkrylov_b200_ftlm_loop, H, temperatures,
+                      ((precision, n_random, n_steps, ctypes.c_uint64(seed), nv), ()))
+
+
 class DavidsonResult:
     def __init__(self, eigenvalues, eigenvectors, iterations=0, converged=False):
         self.eigenvalues, self.eigenvectors = eigenvalues, eigenvectors
@@ -654,6 +697,12 @@ class _LanczosF64(ctypes.Structure):
 
 class _LanczosC(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_float), ("iterations", ctypes.c_int), ("converged", ctypes.c_int)]
+
+
+class _FTLMInfo(ctypes.Structure):
+    _fields_ = [("seconds", ctypes.c_double), ("seconds_device", ctypes.c_double), ("e_min", ctypes.c_double),
+                ("lanes_per_row", ctypes.c_int), ("graph", ctypes.c_int), ("vectors", ctypes.c_int),
+                ("steps", ctypes.c_int)]
 
 
 class _MixedC(ctypes.Structure):

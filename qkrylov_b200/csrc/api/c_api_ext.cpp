@@ -308,6 +308,48 @@ int qkrylov_b200_lanczos_fp64(qkrylov_hamiltonian_h h, uint64_t seed, const void
                            trace_iteration, trace_energy, trace_seconds);
 }
 
+static int ftlm_common(qkrylov_hamiltonian_h h, bool block, int precision, int n_random, int n_steps, uint64_t seed,
+                       int n_vectors, int n_temps, const double* temps, double* logZ, double* U, double* Cv,
+                       int use_graph, qkrylov_b200_ftlm_info_t* info) {
+  if (!h || !h->op || (precision != 32 && precision != 64) || n_temps < 0 || (n_temps > 0 && !temps))
+    return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const qkb::Operator& H = *h->op;
+    const bool real = H.all_real();
+    const qk_dtype t = precision == 32 ? (real ? QK_F32 : QK_C64) : (real ? QK_F64 : QK_C128);
+    const std::vector<double> T(temps, temps + n_temps);
+    auto r = block ? qkb::ftlm_block(H, t, n_random, n_steps, seed, T, use_graph != 0)
+                   : qkb::ftlm_loop(H, t, n_random, n_steps, seed, T, n_vectors);
+    for (int q = 0; q < n_temps; ++q) {
+      if (logZ) logZ[q] = r.logZ[q];
+      if (U) U[q] = r.U[q];
+      if (Cv) Cv[q] = r.Cv[q];
+    }
+    if (info) {
+      info->seconds = r.seconds;
+      info->seconds_device = r.seconds_device;
+      info->e_min = r.e_min;
+      info->lanes_per_row = r.lanes_per_row;
+      info->graph = r.graph;
+      info->vectors = r.R;
+      info->steps = r.M;
+    }
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_ftlm_block(qkrylov_hamiltonian_h h, int precision, int n_random, int n_steps, uint64_t seed,
+                            int n_temps, const double* temps, double* logZ, double* U, double* Cv, int use_graph,
+                            qkrylov_b200_ftlm_info_t* info) {
+  return ftlm_common(h, true, precision, n_random, n_steps, seed, 0, n_temps, temps, logZ, U, Cv, use_graph, info);
+}
+
+int qkrylov_b200_ftlm_loop(qkrylov_hamiltonian_h h, int precision, int n_random, int n_steps, uint64_t seed,
+                           int n_vectors, int n_temps, const double* temps, double* logZ, double* U, double* Cv,
+                           qkrylov_b200_ftlm_info_t* info) {
+  return ftlm_common(h, false, precision, n_random, n_steps, seed, n_vectors, n_temps, temps, logZ, U, Cv, 0, info);
+}
+
 int qkrylov_davidson_lowest_f64(qkrylov_hamiltonian_h h, int n_eig, int max_subspace, double tol, double* evals,
                                 double* evecs, qkrylov_davidson_result_c_t* info) {
   if (!h || !h->op || !evals || n_eig <= 0) return QKRYLOV_ERROR_INVALID_ARG;

@@ -101,6 +101,23 @@ struct MixedOut {
 MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int maxiter, double tol_res,
                        void* psi_out_high, bool low_phase = true);
 
+// Batched FTLM on R (32, 64, 128) Rademacher vectors as one row-interleaved
+// block of dtype t, M Lanczos steps without reorthogonalisation (the
+// reference's recurrence), optionally captured as one CUDA graph; and the
+// same vectors run one at a time (ftlm_loop, the first nvec columns).
+struct FtlmBlockOut {
+  int R = 0, M = 0, lanes_per_row = 0;
+  bool graph = false;
+  double seconds = 0, seconds_device = 0, e_min = 0;
+  std::vector<double> alphas, betas, norm2;  // [r][M]; betas[r][k] = beta_k (len - 1 used)
+  std::vector<int> len;                      // tridiagonal length per vector (breakdown)
+  std::vector<double> logZ, U, Cv;           // per temperature
+};
+FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t seed, const std::vector<double>& temps,
+                        bool use_graph);
+FtlmBlockOut ftlm_loop(const Operator& H, qk_dtype t, int R, int M, uint64_t seed, const std::vector<double>& temps,
+                       int nvec);
+
 // src/solvers/dynamics.cpp:12-59
 template <class Real>
 CFOut<Real> continued_fraction(const Operator& H, const std::complex<Real>* phi0, int n_iter);

@@ -71,6 +71,18 @@ int qkd_apply_dot(const qk_plan* p, qk_workspace* w, qk_dtype t, const void* x, 
 /* Block form: X, Y hold nvec vectors, vector v at X + v*ldx elements. */
 int qkd_apply_block(const qk_plan* p, qk_dtype t, int nvec, const void* X, size_t ldx, void* Y,
                     size_t ldy, cudaStream_t s);
+/* Block apply on R vectors stored row-interleaved (element (i, r) at
+ * i*R + r; R = 32, 64 or 128): Y = H X and, if dots != NULL, dots[2r..2r+1]
+ * = <X_r, Y_r> (device memory).  lanes_per_row 8, 16 or 32 (R / lanes <= 8)
+ * sets the tile shape; 0 uses the autotuned shape (32 before tuning).
+ * X, Y 16-byte aligned. */
+int qkd_apply_rows(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lanes_per_row, const void* X,
+                   void* Y, double* dots, cudaStream_t s);
+/* Time every valid lanes-per-row shape on X, Y (three launches each) and
+ * keep the fastest for (t, R) in the plan; *chosen receives it.  Waits for
+ * the stream. */
+int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, cudaStream_t s,
+                  int* chosen);
 /* diag[i] = <i|H|i> as dtype t. */
 int qkd_diagonal(const qk_plan* p, qk_dtype t, void* diag, cudaStream_t s);
 /* Number of kernel launches issued by this library since load (for the
@@ -121,6 +133,19 @@ int qkd_random(qk_dtype t, size_t n, uint64_t seed, int kind, void* x, cudaStrea
 /* x (dtype tx) = sum_{j<k} c_j V_j (dtype tv), c: 2k device doubles. */
 int qkd_combine(qk_dtype tv, size_t n, int k, const void* const* V, const double* c, qk_dtype tx, void* x,
                 cudaStream_t s);
+/* ------------------------------------------------- row-interleaved blocks
+ * R vectors of n elements, element (i, r) at i*R + r; R divides 256.
+ * W_r <- W_r - a_r V_r - b_r Vp_r for every column r (a: 2R device doubles,
+ * complex; b: R device doubles, real; V / Vp with a / b may be NULL), then
+ * nrm2[2r] = |W_r|^2 (device, 2R doubles; odd entries 0). */
+int qkd_block_update(qk_workspace* w, qk_dtype t, size_t n, int R, const void* V, const double* a, const void* Vp,
+                     const double* b, void* W, double* nrm2, cudaStream_t s);
+/* beta_r = sqrt(nrm2[2r]); W_r *= 1 / beta_r, or W_r = 0 and
+ * len[r] = min(len[r], step + 1) when beta_r < 1e-15; beta_out[r] = beta_r. */
+int qkd_block_scale(qk_dtype t, size_t n, int R, const double* nrm2, void* W, double* beta_out, int* len, int step,
+                    cudaStream_t s);
+/* out (n elements) = column c of the block X. */
+int qkd_block_column(qk_dtype t, size_t n, int R, const void* X, int c, void* out, cudaStream_t s);
 /* Device scratch of the workspace: 2*kMaxK+16 doubles for small results. */
 double* qkd_workspace_results(qk_workspace* w);
 

@@ -39,6 +39,7 @@ struct qk_plan {
   uint32_t nterms, ngroups, ntiles;
   int has_diag, all_real;
   size_t bytes, smem;
+  int rows_lpr[4][3];  // autotuned lanes per row of the block apply, by dtype and R = 32, 64, 128
 };
 
 namespace qkd {
@@ -167,6 +168,118 @@ k_hx(DevPlan p, const void* __restrict__ x, void* __restrict__ y, double* partia
   }
 }
 
+// Block H.X on R vectors stored row-interleaved: element (i, r) at i*R + r.
+// LPR consecutive lanes share one row and each covers VPL = R / LPR
+// consecutive vectors with one vector load per gather, so the state, the
+// term table walk and the target ranking of a row are done once and reused
+// for all R vectors.  With dots != nullptr the column dots <X_r, Y_r> are
+// reduced deterministically (fixed thread order, then block order).
+template <class E, int VPL>
+struct alignas(sizeof(E) * VPL) RowPack { E v[VPL]; };
+
+template <int DT> __device__ __forceinline__ void unpack1(const typename VT<DT>::E& e, typename VT<DT>::R& re,
+                                                        typename VT<DT>::R& im);
+template <> __device__ __forceinline__ void unpack1<QK_C128>(const double2& e, double& re, double& im) { re = e.x; im = e.y; }
+template <> __device__ __forceinline__ void unpack1<QK_C64>(const float2& e, float& re, float& im) { re = e.x; im = e.y; }
+template <> __device__ __forceinline__ void unpack1<QK_F64>(const double& e, double& re, double& im) { re = e; im = 0; }
+template <> __device__ __forceinline__ void unpack1<QK_F32>(const float& e, float& re, float& im) { re = e; im = 0; }
+__device__ __forceinline__ double2 pack1(double re, double im, double2*) { return make_double2(re, im); }
+__device__ __forceinline__ float2 pack1(float re, float im, float2*) { return make_float2(re, im); }
+__device__ __forceinline__ double pack1(double re, double, double*) { return re; }
+__device__ __forceinline__ float pack1(float re, float, float*) { return re; }
+
+template <int DT, bool CC, int LPR, int VPL>
+__global__ void __launch_bounds__(kTile)
+k_hx_block(DevPlan p, const void* __restrict__ X, void* __restrict__ Y, double* partials, unsigned* ticket,
+           double* dots) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  using E = typename T::E;
+  using Pack = RowPack<E, VPL>;
+  constexpr int RV = LPR * VPL, RPW = 32 / LPR;
+  qk_term_t* st;
+  qk_group_t* sg;
+  stage_plan(p, st, sg);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane / LPR, l = lane % LPR;
+  const E* __restrict__ Xe = reinterpret_cast<const E*>(X);
+  E* __restrict__ Ye = reinterpret_cast<E*>(Y);
+  double dr[VPL], di[VPL];
+  #pragma unroll
+  for (int v = 0; v < VPL; ++v) { dr[v] = 0.0; di[v] = 0.0; }
+  for (uint32_t ti = blockIdx.x; ti < p.ntiles; ti += gridDim.x) {
+    const qk_tile_t tile = p.tiles[ti];
+    for (uint32_t rr = warp * RPW + sub; rr < tile.count; rr += (kTile / 32) * RPW) {
+      const uint64_t row = tile.row0 + rr;
+      const uint64_t s = (uint64_t(tile.h) << p.L) | __ldg(p.llist + tile.lstart + rr);
+      const Pack x0 = *reinterpret_cast<const Pack*>(Xe + row * RV + l * VPL);
+      R x0r[VPL], x0i[VPL], ar[VPL], ai[VPL];
+      #pragma unroll
+      for (int v = 0; v < VPL; ++v) { unpack1<DT>(x0.v[v], x0r[v], x0i[v]); ar[v] = R(0); ai[v] = R(0); }
+      uint32_t g0 = 0;
+      if (p.has_diag) {
+        R cr, ci;
+        if (group_coef<CC, R>(st, sg[0].first, sg[0].count, s, cr, ci)) {
+          #pragma unroll
+          for (int v = 0; v < VPL; ++v) {
+            ar[v] += cr * x0r[v];
+            if (T::cplx) {
+              ai[v] += cr * x0i[v];
+              if (CC) { ar[v] -= ci * x0i[v]; ai[v] += ci * x0r[v]; }
+            }
+          }
+        }
+        g0 = 1;
+      }
+      for (uint32_t g = g0; g < p.ngroups; ++g) {
+        const qk_group_t grp = sg[g];
+        R cr, ci;
+        if (!group_coef<CC, R>(st, grp.first, grp.count, s, cr, ci)) continue;
+        const uint64_t t = s ^ grp.flip;
+        const uint64_t a = __ldg(p.A + (t >> p.L));
+        const uint32_t b = __ldg(p.B + (t & p.lmask));
+        if (uint32_t(a >> 56) != (b >> 24)) continue;  // target outside the sector
+        const uint64_t col = (a & qkb::kOffsetMask) + (b & qkb::kRankMask);
+        const Pack xv = *reinterpret_cast<const Pack*>(Xe + col * RV + l * VPL);
+        #pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          R xr, xi;
+          unpack1<DT>(xv.v[v], xr, xi);
+          ar[v] += cr * xr;
+          if (T::cplx) {
+            ai[v] += cr * xi;
+            if (CC) { ar[v] -= ci * xi; ai[v] += ci * xr; }
+          }
+        }
+      }
+      Pack yv;
+      #pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        yv.v[v] = pack1(ar[v], ai[v], static_cast<E*>(nullptr));
+        dr[v] += double(x0r[v]) * double(ar[v]) + double(x0i[v]) * double(ai[v]);
+        di[v] += double(x0r[v]) * double(ai[v]) - double(x0i[v]) * double(ar[v]);
+      }
+      *reinterpret_cast<Pack*>(Ye + row * RV + l * VPL) = yv;
+    }
+  }
+  // column c = l * VPL + v: sum over the threads with the same l, fixed order
+  __shared__ double red[kTile * 2];
+  for (int v = 0; v < VPL; ++v) {
+    __syncthreads();
+    red[2 * threadIdx.x] = dr[v];
+    red[2 * threadIdx.x + 1] = di[v];
+    __syncthreads();
+    if (threadIdx.x < LPR) {
+      double sr = 0.0, si = 0.0;
+      for (int t = threadIdx.x; t < kTile; t += LPR) { sr += red[2 * t]; si += red[2 * t + 1]; }
+      const int c = threadIdx.x * VPL + v;
+      partials[(size_t(c) * gridDim.x + blockIdx.x) * 2] = sr;
+      partials[(size_t(c) * gridDim.x + blockIdx.x) * 2 + 1] = si;
+    }
+  }
+  grid_finish(partials, ticket, RV, dots);
+}
+
 template <int DT, bool CC>
 __global__ void __launch_bounds__(kTile) k_diag(DevPlan p, void* __restrict__ d) {
   using T = VT<DT>;
@@ -219,6 +332,29 @@ int launch_apply(const qk_plan* p, const void* x, void* y, cudaStream_t s, qk_wo
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
+
+template <int DT, bool CC, int LPR, int VPL>
+int launch_block(const qk_plan* p, qk_workspace* w, const void* X, void* Y, double* dots, cudaStream_t s) {
+  auto k = k_hx_block<DT, CC, LPR, VPL>;
+  if (set_smem(k, p->smem)) return QKD_EINVAL;
+  const unsigned g = std::min<unsigned>(hx_grid(p, k), kMaxG);
+  k<<<g, kTile, p->smem, s>>>(dev(p), X, Y, w->partials, w->ticket, dots ? dots : w->result);
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+template <int DT, bool CC>
+int launch_block_shape(const qk_plan* p, qk_workspace* w, int R, int lpr, const void* X, void* Y, double* dots,
+                       cudaStream_t s) {
+#define QKD_BLK(RR, L, V) if (R == RR && lpr == L) return launch_block<DT, CC, L, V>(p, w, X, Y, dots, s);
+  QKD_BLK(32, 32, 1) QKD_BLK(32, 16, 2) QKD_BLK(32, 8, 4)
+  QKD_BLK(64, 32, 2) QKD_BLK(64, 16, 4) QKD_BLK(64, 8, 8)
+  QKD_BLK(128, 32, 4) QKD_BLK(128, 16, 8)
+#undef QKD_BLK
+  return QKD_EINVAL;
+}
+
+int r_index(int R) { return R == 32 ? 0 : R == 64 ? 1 : R == 128 ? 2 : -1; }
 
 }  // namespace
 }  // namespace qkd
@@ -321,6 +457,44 @@ int qkd_apply_block(const qk_plan* p, qk_dtype t, int nvec, const void* X, size_
     const int rc = qkd_apply(p, t, static_cast<const char*>(X) + v * ldx * es, static_cast<char*>(Y) + v * ldy * es, s);
     if (rc) return rc;
   }
+  return QKD_OK;
+}
+
+int qkd_apply_rows(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lanes_per_row, const void* X,
+                   void* Y, double* dots, cudaStream_t s) {
+  if (!p || !w || !X || !Y || X == Y || r_index(R) < 0) return QKD_EINVAL;
+  if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
+  if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
+  const int lpr = lanes_per_row ? lanes_per_row : (p->rows_lpr[t][r_index(R)] ? p->rows_lpr[t][r_index(R)] : 32);
+  if (p->all_real) { QKD_DISPATCH(t, return launch_block_shape<DT, false>(p, w, R, lpr, X, Y, dots, s)); }
+  if (t == QK_C128) return launch_block_shape<QK_C128, true>(p, w, R, lpr, X, Y, dots, s);
+  if (t == QK_C64) return launch_block_shape<QK_C64, true>(p, w, R, lpr, X, Y, dots, s);
+  return QKD_EINVAL;
+}
+
+int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, cudaStream_t s,
+                  int* chosen) {
+  if (!p || !w || r_index(R) < 0 || t < QK_C128 || t > QK_F32) return QKD_EINVAL;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return QKD_ECUDA;
+  float best = 1e30f;
+  int pick = 0;
+  for (int lpr : {32, 16, 8}) {
+    if (R / lpr > 8) continue;
+    if (qkd_apply_rows(p, w, t, R, lpr, X, Y, nullptr, s) != QKD_OK) continue;  // warm-up
+    cudaEventRecord(e0, s);
+    for (int i = 0; i < 3; ++i) qkd_apply_rows(p, w, t, R, lpr, X, Y, nullptr, s);
+    cudaEventRecord(e1, s);
+    float ms = 0.f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) continue;
+    if (ms < best) { best = ms; pick = lpr; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  (void)cudaGetLastError();
+  if (!pick) return QKD_ECUDA;
+  p->rows_lpr[t][r_index(R)] = pick;
+  if (chosen) *chosen = pick;
   return QKD_OK;
 }
 
