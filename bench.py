@@ -14,6 +14,8 @@ tables, term tables and repeated gathers are not counted).
   variants  the same kernel on complex64 / float64 / float32 vectors
   time_to_e0  plain FP64 GPU Lanczos vs FP32-vector Lanczos + FP64
          refinement, both to the explicit residual 1e-10 (wall seconds)
+  batched_ftlm  t-J N=20 FTLM, 64 vectors x 100 steps x 200 temperatures:
+         one block (FP32 / FP64 vectors, CUDA graph) vs the one-vector loop
 
 --impl reference times the reference's own CPU implementation (its
 unchanged sources, oracle/_ref, OpenMP on all host cores) on a bounded
@@ -111,6 +113,27 @@ def profiled_traffic():
         return None
 
 
+def tj_opsum(qk, N, t, J):
+    """Periodic t-J chain: hops -t (annihilator listed first, both spins,
+    both directions) and J (S_i.S_j - n_i n_j / 4) as -J/2 (Nup_i Ndn_j +
+    Ndn_i Nup_j) plus the two spin-flip four-fermion terms, factors ordered
+    so that the operator qkrylov computes (T^dagger per term, factors applied
+    in list order) is the physical one."""
+    os_ = qk.OpSum(dtype=np.float64)
+    for i in range(N):
+        j = (i + 1) % N
+        for (a, b) in ((i, j), (j, i)):
+            os_.add_term(-t, "CUp", b, "CdagUp", a)
+            os_.add_term(-t, "CDn", b, "CdagDn", a)
+    for i in range(N):
+        j = (i + 1) % N
+        os_.add_term(-0.5 * J, "Nup", i, "Ndn", j)
+        os_.add_term(-0.5 * J, "Ndn", i, "Nup", j)
+        os_.add_term(0.5 * J, "CUp", j, "CdagDn", j, "CDn", i, "CdagUp", i)
+        os_.add_term(0.5 * J, "CUp", i, "CdagDn", i, "CDn", j, "CdagUp", j)
+    return os_
+
+
 def heisenberg_opsum(qk, N, dtype):
     os_ = qk.OpSum(dtype=dtype)
     for i in range(N):
@@ -166,6 +189,36 @@ def time_to_e0(qk, N, tol=1e-10, seed=1):
                      "restarts": r.restarts}
     out["dE_mixed_vs_plain"] = abs(out["mixed"]["energy"] - out["plain_fp64"]["energy"])
     out["speedup_mixed"] = out["plain_fp64"]["seconds"] / out["mixed"]["seconds"]
+    del H
+    return out
+
+
+def batched_ftlm(qk, N=20, R=64, M=100, loop_vectors=4, seed=5):
+    """Batched FTLM (R Rademacher vectors as one block, FP32 vectors, FP64
+    dots, CUDA graph) vs the one-vector FP64 loop on the same vectors, on
+    the periodic t-J chain (2 holes, Sz=0), 200 temperatures in [0.01, 10].
+    The loop is timed on its first `loop_vectors` vectors and scaled to R
+    (the vectors are independent and equal in cost)."""
+    ne = N - 2
+    B = qk.TJBasis(N, conserve_nup=True, nup=ne // 2, conserve_ndn=True, ndn=ne - ne // 2)
+    H = qk.MatrixFreeHamiltonian(B, qk.TJSite(), tj_opsum(qk, N, 1.0, 0.4), dtype=np.float64)
+    T = 0.01 * 1000.0 ** (np.arange(200) / 199.0)
+    out = {"workload": f"tj_chain_N{N}_2holes_Sz0", "dim": H.dimension, "R": R, "M": M, "temperatures": 200}
+    for prec in (32, 64):
+        r = qk.ftlm_block(H, T, n_random=R, n_steps=M, seed=seed, precision=prec)   # tunes the tile shape
+        r = qk.ftlm_block(H, T, n_random=R, n_steps=M, seed=seed, precision=prec)
+        out[f"block_fp{prec}"] = {"seconds": r.seconds, "seconds_device": r.seconds_device,
+                                  "lanes_per_row": r.lanes_per_row, "graph": r.graph}
+        if prec == 32:
+            r32 = r
+        else:
+            r64 = r
+    l = qk.ftlm_loop(H, T, n_random=R, n_steps=M, seed=seed, precision=64, n_vectors=loop_vectors)
+    loop_s = l.seconds_device * R / loop_vectors
+    out["loop_fp64"] = {"seconds": loop_s, "measured_vectors": loop_vectors}
+    out["speedup_block_fp32"] = loop_s / out["block_fp32"]["seconds"]
+    out["speedup_block_fp64"] = loop_s / out["block_fp64"]["seconds"]
+    out["max_rel_dU_fp32_vs_fp64"] = float(np.max(np.abs(r32.U - r64.U) / np.abs(r64.U)))
     del H
     return out
 
@@ -301,6 +354,11 @@ def run_b200(args):
             line["time_to_e0"] = time_to_e0(qk, N)
         except Exception as e:  # reported, never silently replaced
             line["time_to_e0"] = {"error": str(e)}
+        try:
+            torch.cuda.empty_cache()
+            line["batched_ftlm"] = batched_ftlm(qk)
+        except Exception as e:
+            line["batched_ftlm"] = {"error": str(e)}
     if rank == 0 and not args.no_cpu_baseline:
         try:
             cb = cpu_reference_gbs(N=24, steps=2)

@@ -1,10 +1,11 @@
 // Batched finite-temperature Lanczos: R random vectors advanced together as
-// one row-interleaved block (element (i, r) at i*R + r).  Every step is
-// one block H.X (the row's term walk and target ranks shared by all R
-// vectors) with fused column dots, one column update with fused FP64
-// column norms and one column scaling; alpha, beta and the breakdown
-// lengths stay on the device, so the M steps are captured once as a CUDA
-// graph and replayed.  The R tridiagonals then give Z, U and Cv at every
+// one row-interleaved block (element (i, r) at i*R + r).  The vectors are
+// kept unnormalised (v_k = s_k U_k), so every step is two kernels: one
+// block H.X (the row's term walk and target ranks shared by all R vectors,
+// the diagonal read from a precomputed vector) with fused column dots, and
+// one column recurrence with fused FP64 column norms that also produces
+// alpha, beta and the next scales.  Nothing returns to the host between
+// steps, so the M steps are captured once as a CUDA graph and replayed.  The R tridiagonals then give Z, U and Cv at every
 // temperature on the host.  ftlm_loop runs the same random vectors one at
 // a time through the single-vector kernels (the baseline).
 //
@@ -72,32 +73,46 @@ FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t se
   const int dev = H.device();
   DevVec B0(n * R, t, dev, false), B1(n * R, t, dev, false), B2(n * R, t, dev, false);
   DevVec* B[3] = {&B0, &B1, &B2};
-  DevVec alpha(size_t(M) * 2 * R, QK_F64, dev), beta(size_t(M) * R, QK_F64, dev), nrm(2 * size_t(R), QK_F64, dev),
-      bsc(size_t(R), QK_F64, dev);
+  DevVec dots(size_t(M) * 2 * R, QK_F64, dev), alpha(size_t(M) * R, QK_F64, dev), beta(size_t(M) * R, QK_F64, dev),
+      scale(size_t(M + 1) * R, QK_F64, dev), nrm(2 * size_t(R), QK_F64, dev), diag(n, t, dev, false);
   DevVec len(size_t(R), QK_F32, dev, false);  // R ints
   std::vector<int> hl(R, M);
   cuda_check(cudaMemcpyAsync(len.data(), hl.data(), sizeof(int) * R, cudaMemcpyHostToDevice, c.stream), "H2D");
-  double* ad = static_cast<double*>(alpha.data());
+  double* dd = static_cast<double*>(dots.data());
+  double* al = static_cast<double*>(alpha.data());
   double* bd = static_cast<double*>(beta.data());
+  double* sd = static_cast<double*>(scale.data());
   double* nd = static_cast<double*>(nrm.data());
   int* ld = static_cast<int*>(len.data());
-  // Rademacher start block, column norms, normalisation
+  // H's diagonal once (the block apply reads it instead of walking the
+  // diagonal terms); Rademacher start block and its column norms.  The
+  // vectors stay unnormalised: v_k = s_k U_k.
+  H.diagonal(t, diag.data());
   qkd_check(qkd_random(t, n * R, seed, 1, B0.data(), c.stream), "random");
   qkd_check(qkd_block_update(c.ws, t, n, R, nullptr, nullptr, nullptr, nullptr, B0.data(), nd, c.stream), "norms");
   const double* n2 = c.fetch(nd, 2 * R);
   out.norm2.resize(R);
-  for (int r = 0; r < R; ++r) out.norm2[r] = n2[2 * r];
-  qkd_check(qkd_block_scale(t, n, R, nd, B0.data(), static_cast<double*>(bsc.data()), ld, -1, c.stream), "scale");
+  std::vector<double> s0(R);
+  for (int r = 0; r < R; ++r) {
+    out.norm2[r] = n2[2 * r];
+    s0[r] = n2[2 * r] > 0 ? 1.0 / std::sqrt(n2[2 * r]) : 0.0;
+  }
+  cuda_check(cudaMemcpyAsync(sd, s0.data(), sizeof(double) * R, cudaMemcpyHostToDevice, c.stream), "H2D");
   qk_plan* plan = const_cast<qk_plan*>(H.plan());
-  qkd_check(qkd_tune_rows(plan, c.ws, t, R, B0.data(), B1.data(), c.stream, &out.lanes_per_row), "tune");
+  out.lanes_per_row = qkd_rows_shape(plan, t, R);  // tuned once per operator, dtype and block size
+  if (!out.lanes_per_row)
+    qkd_check(qkd_tune_rows(plan, c.ws, t, R, B0.data(), B1.data(), diag.data(), c.stream, &out.lanes_per_row),
+              "tune");
   auto step = [&](int k) {
-    void* V = B[k % 3]->data();
-    void* W = B[(k + 1) % 3]->data();
-    void* Vp = B[(k + 2) % 3]->data();
-    qkd_check(qkd_apply_rows(plan, c.ws, t, R, 0, V, W, ad + size_t(2) * R * k, c.stream), "block apply");
-    qkd_check(qkd_block_update(c.ws, t, n, R, V, ad + size_t(2) * R * k, k > 0 ? Vp : nullptr,
-                               k > 0 ? bd + size_t(R) * (k - 1) : nullptr, W, nd, c.stream), "block update");
-    qkd_check(qkd_block_scale(t, n, R, nd, W, bd + size_t(R) * k, ld, k, c.stream), "block scale");
+    void* U = B[k % 3]->data();
+    void* Y = B[(k + 1) % 3]->data();
+    void* Up = B[(k + 2) % 3]->data();
+    qkd_check(qkd_apply_rows(plan, c.ws, t, R, 0, U, Y, diag.data(), dd + size_t(2) * R * k, c.stream),
+              "block apply");
+    qkd_check(qkd_block_lanczos(c.ws, t, n, R, U, k > 0 ? Up : nullptr, dd + size_t(2) * R * k,
+                                k > 0 ? bd + size_t(R) * (k - 1) : nullptr, k > 0 ? sd + size_t(R) * (k - 1) : nullptr,
+                                sd + size_t(R) * k, sd + size_t(R) * (k + 1), Y, al + size_t(R) * k,
+                                bd + size_t(R) * k, ld, k, c.stream), "block step");
   };
   cudaEvent_t e0, e1;
   cuda_check(cudaEventCreate(&e0), "event");
@@ -130,8 +145,8 @@ FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t se
   if (exec) cudaGraphExecDestroy(exec);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  std::vector<double> ha(size_t(M) * 2 * R), hb(size_t(M) * R);
-  cuda_check(cudaMemcpy(ha.data(), ad, ha.size() * 8, cudaMemcpyDeviceToHost), "D2H");
+  std::vector<double> ha(size_t(M) * R), hb(size_t(M) * R);
+  cuda_check(cudaMemcpy(ha.data(), al, ha.size() * 8, cudaMemcpyDeviceToHost), "D2H");
   cuda_check(cudaMemcpy(hb.data(), bd, hb.size() * 8, cudaMemcpyDeviceToHost), "D2H");
   cuda_check(cudaMemcpy(hl.data(), ld, sizeof(int) * R, cudaMemcpyDeviceToHost), "D2H");
   out.len = hl;
@@ -139,7 +154,7 @@ FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t se
   out.betas.assign(size_t(R) * M, 0.0);
   for (int r = 0; r < R; ++r)
     for (int k = 0; k < M; ++k) {
-      out.alphas[size_t(r) * M + k] = ha[(size_t(k) * R + r) * 2];
+      out.alphas[size_t(r) * M + k] = ha[size_t(k) * R + r];
       out.betas[size_t(r) * M + k] = hb[size_t(k) * R + r];
     }
   thermo(out, temps);

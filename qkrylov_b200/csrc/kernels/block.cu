@@ -91,6 +91,110 @@ __global__ void k_block_scale(size_t n, int R, const double* __restrict__ nrm2, 
   }
 }
 
+// 16-byte packs of consecutive columns of one row.
+template <int DT> struct BPk;
+template <> struct BPk<QK_C128> {
+  using V = double2; static constexpr int W = 1;
+  __device__ static void un(const V& v, double* re, double* im) { re[0] = v.x; im[0] = v.y; }
+  __device__ static V pk(const double* re, const double* im) { return make_double2(re[0], im[0]); }
+};
+template <> struct BPk<QK_C64> {
+  using V = float4; static constexpr int W = 2;
+  __device__ static void un(const V& v, double* re, double* im) { re[0] = v.x; im[0] = v.y; re[1] = v.z; im[1] = v.w; }
+  __device__ static V pk(const double* re, const double* im) {
+    return make_float4(float(re[0]), float(im[0]), float(re[1]), float(im[1]));
+  }
+};
+template <> struct BPk<QK_F64> {
+  using V = double2; static constexpr int W = 2;
+  __device__ static void un(const V& v, double* re, double* im) { re[0] = v.x; re[1] = v.y; im[0] = im[1] = 0.0; }
+  __device__ static V pk(const double* re, const double*) { return make_double2(re[0], re[1]); }
+};
+template <> struct BPk<QK_F32> {
+  using V = float4; static constexpr int W = 4;
+  __device__ static void un(const V& v, double* re, double* im) {
+    re[0] = v.x; re[1] = v.y; re[2] = v.z; re[3] = v.w; im[0] = im[1] = im[2] = im[3] = 0.0;
+  }
+  __device__ static V pk(const double* re, const double*) {
+    return make_float4(float(re[0]), float(re[1]), float(re[2]), float(re[3]));
+  }
+};
+
+// One Lanczos step of R recurrences on unnormalised vectors (v_k = s_k U_k),
+// 16-byte packs; the grid stride in elements is a multiple of R, so each
+// thread keeps the same W columns and reads their coefficients once.  The
+// last block to finish turns the column norms into beta, s_{k+1} and the
+// breakdown lengths.
+template <int DT>
+__global__ void __launch_bounds__(kBT)
+k_block_lanczos(size_t n, int R, const void* __restrict__ Uk, const void* __restrict__ Ukm1,
+                const double* __restrict__ dots, const double* __restrict__ beta_prev,
+                const double* __restrict__ s_prev, const double* __restrict__ s_k, double* s_next, void* Y,
+                double* alpha_out, double* beta_out, int* len, int step, double* partials, unsigned* ticket) {
+  using P = BPk<DT>;
+  using PV = typename P::V;
+  constexpr int W = P::W;
+  const size_t nq = n * size_t(R) / W;
+  const size_t g = size_t(blockIdx.x) * kBT + threadIdx.x;
+  const int c0 = int((g * W) % size_t(R));
+  double cy[W], cu[W], cp[W];
+  #pragma unroll
+  for (int w = 0; w < W; ++w) {
+    const int c = c0 + w;
+    const double sk = s_k[c];
+    cy[w] = sk;
+    cu[w] = sk * sk * dots[2 * c] * sk;
+    cp[w] = Ukm1 ? beta_prev[c] * s_prev[c] : 0.0;
+  }
+  double acc[W];
+  #pragma unroll
+  for (int w = 0; w < W; ++w) acc[w] = 0.0;
+  for (size_t q = g; q < nq; q += size_t(gridDim.x) * kBT) {
+    double yr[W], yi[W], ur[W], ui[W];
+    P::un(reinterpret_cast<const PV*>(Y)[q], yr, yi);
+    P::un(__ldg(reinterpret_cast<const PV*>(Uk) + q), ur, ui);
+    #pragma unroll
+    for (int w = 0; w < W; ++w) { yr[w] = cy[w] * yr[w] - cu[w] * ur[w]; yi[w] = cy[w] * yi[w] - cu[w] * ui[w]; }
+    if (Ukm1) {
+      P::un(__ldg(reinterpret_cast<const PV*>(Ukm1) + q), ur, ui);
+      #pragma unroll
+      for (int w = 0; w < W; ++w) { yr[w] -= cp[w] * ur[w]; yi[w] -= cp[w] * ui[w]; }
+    }
+    const PV o = P::pk(yr, yi);
+    reinterpret_cast<PV*>(Y)[q] = o;
+    P::un(o, yr, yi);
+    #pragma unroll
+    for (int w = 0; w < W; ++w) acc[w] += yr[w] * yr[w] + yi[w] * yi[w];
+  }
+  // per-column block sums: slot t*W + w holds column (t*W + w) % R
+  __shared__ double red[kBT * W];
+  #pragma unroll
+  for (int w = 0; w < W; ++w) red[threadIdx.x * W + w] = acc[w];
+  __syncthreads();
+  for (int j = threadIdx.x; j < R; j += kBT) {
+    double sum = 0.0;
+    for (int i = j; i < kBT * W; i += R) sum += red[i];
+    partials[size_t(j) * gridDim.x + blockIdx.x] = sum;
+  }
+  __shared__ unsigned s_ticket;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_ticket = atomicAdd(ticket, 1u);
+  __syncthreads();
+  if (s_ticket != gridDim.x - 1) return;
+  __threadfence();
+  for (int j = threadIdx.x; j < R; j += kBT) {
+    double nrm = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) nrm += __ldcg(partials + size_t(j) * gridDim.x + b);
+    const double beta = sqrt(nrm), sk = s_k[j];
+    alpha_out[j] = sk * sk * dots[2 * j];
+    beta_out[j] = beta;
+    s_next[j] = beta < 1e-15 ? 0.0 : 1.0 / beta;
+    if (beta < 1e-15 && len[j] > step + 1) len[j] = step + 1;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
 template <int DT>
 __global__ void k_block_column(size_t n, int R, const void* __restrict__ X, int c, void* out) {
   using T = VT<DT>;
@@ -124,6 +228,24 @@ int qkd_block_scale(qk_dtype t, size_t n, int R, const double* nrm2, void* W, do
   if (!nrm2 || !W || !beta_out || !len || R <= 0) return QKD_EINVAL;
   if (n == 0) return QKD_OK;
   QKD_DISPATCH(t, k_block_scale<DT><<<block_grid(n * size_t(R)), kBT, 0, s>>>(n, R, nrm2, W, beta_out, len, step));
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+int qkd_block_lanczos(qk_workspace* w, qk_dtype t, size_t n, int R, const void* Uk, const void* Ukm1,
+                      const double* dots, const double* beta_prev, const double* s_prev, const double* s_k,
+                      double* s_next, void* Y, double* alpha_out, double* beta_out, int* len, int step,
+                      cudaStream_t s) {
+  if (!w || !Uk || !Y || !dots || !s_k || !s_next || !alpha_out || !beta_out || !len || R < 32 || R > kMaxK ||
+      kBT % R != 0 || (Ukm1 && (!beta_prev || !s_prev)))
+    return QKD_EINVAL;
+  const uintptr_t al = reinterpret_cast<uintptr_t>(Uk) | reinterpret_cast<uintptr_t>(Y) |
+                       reinterpret_cast<uintptr_t>(Ukm1);
+  if (al & 15) return QKD_EINVAL;  // 16-byte packs
+  if (n == 0) return QKD_OK;
+  const unsigned G = block_grid(n * size_t(R) / 4);
+  QKD_DISPATCH(t, k_block_lanczos<DT><<<G, kBT, 0, s>>>(n, R, Uk, Ukm1, dots, beta_prev, s_prev, s_k, s_next, Y,
+                                                        alpha_out, beta_out, len, step, w->partials, w->ticket));
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }

@@ -75,14 +75,17 @@ int qkd_apply_block(const qk_plan* p, qk_dtype t, int nvec, const void* X, size_
  * i*R + r; R = 32, 64 or 128): Y = H X and, if dots != NULL, dots[2r..2r+1]
  * = <X_r, Y_r> (device memory).  lanes_per_row 8, 16 or 32 (R / lanes <= 8)
  * sets the tile shape; 0 uses the autotuned shape (32 before tuning).
- * X, Y 16-byte aligned. */
+ * diag: NULL, or H's diagonal (dtype t, from qkd_diagonal) used instead of
+ * walking the diagonal terms.  X, Y 16-byte aligned. */
 int qkd_apply_rows(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lanes_per_row, const void* X,
-                   void* Y, double* dots, cudaStream_t s);
+                   void* Y, const void* diag, double* dots, cudaStream_t s);
 /* Time every valid lanes-per-row shape on X, Y (three launches each) and
  * keep the fastest for (t, R) in the plan; *chosen receives it.  Waits for
  * the stream. */
-int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, cudaStream_t s,
-                  int* chosen);
+int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, const void* diag,
+                  cudaStream_t s, int* chosen);
+/* The tuned lanes per row for (t, R), 0 before tuning. */
+int qkd_rows_shape(const qk_plan* p, qk_dtype t, int R);
 /* diag[i] = <i|H|i> as dtype t. */
 int qkd_diagonal(const qk_plan* p, qk_dtype t, void* diag, cudaStream_t s);
 /* Number of kernel launches issued by this library since load (for the
@@ -140,6 +143,17 @@ int qkd_combine(qk_dtype tv, size_t n, int k, const void* const* V, const double
  * nrm2[2r] = |W_r|^2 (device, 2R doubles; odd entries 0). */
 int qkd_block_update(qk_workspace* w, qk_dtype t, size_t n, int R, const void* V, const double* a, const void* Vp,
                      const double* b, void* W, double* nrm2, cudaStream_t s);
+/* One step of R Lanczos recurrences on unnormalised vectors U (v_k = s_k U_k):
+ * with raw dots d_r = <U_k,r, Y_r> of Y = H U_k, alpha_r = s_k^2 Re d_r and
+ *   W_r = s_k Y_r - alpha_r s_k U_k,r - beta_{k-1},r s_{k-1},r U_{k-1},r
+ * written over Y (Ukm1 / beta_prev / s_prev NULL at the first step); then
+ * beta_k,r = |W_r|, s_{k+1},r = 1 / beta_k,r (0 and len[r] = min(len[r],
+ * step + 1) when beta < 1e-15).  s: scales by step (s[k*R + r]); alpha_out,
+ * beta_out: R doubles each of this step (device). */
+int qkd_block_lanczos(qk_workspace* w, qk_dtype t, size_t n, int R, const void* Uk, const void* Ukm1,
+                      const double* dots, const double* beta_prev, const double* s_prev, const double* s_k,
+                      double* s_next, void* Y, double* alpha_out, double* beta_out, int* len, int step,
+                      cudaStream_t s);
 /* beta_r = sqrt(nrm2[2r]); W_r *= 1 / beta_r, or W_r = 0 and
  * len[r] = min(len[r], step + 1) when beta_r < 1e-15; beta_out[r] = beta_r. */
 int qkd_block_scale(qk_dtype t, size_t n, int R, const double* nrm2, void* W, double* beta_out, int* len, int step,

@@ -190,8 +190,8 @@ __device__ __forceinline__ float pack1(float re, float, float*) { return re; }
 
 template <int DT, bool CC, int LPR, int VPL>
 __global__ void __launch_bounds__(kTile)
-k_hx_block(DevPlan p, const void* __restrict__ X, void* __restrict__ Y, double* partials, unsigned* ticket,
-           double* dots) {
+k_hx_block(DevPlan p, const void* __restrict__ X, void* __restrict__ Y, const void* __restrict__ diag,
+           double* partials, unsigned* ticket, double* dots) {
   using T = VT<DT>;
   using R = typename T::R;
   using E = typename T::E;
@@ -218,8 +218,13 @@ k_hx_block(DevPlan p, const void* __restrict__ X, void* __restrict__ Y, double* 
       for (int v = 0; v < VPL; ++v) { unpack1<DT>(x0.v[v], x0r[v], x0i[v]); ar[v] = R(0); ai[v] = R(0); }
       uint32_t g0 = 0;
       if (p.has_diag) {
+        // the diagonal from the precomputed vector when given, else from the
+        // diagonal term group
         R cr, ci;
-        if (group_coef<CC, R>(st, sg[0].first, sg[0].count, s, cr, ci)) {
+        bool any = true;
+        if (diag) T::ld(diag, row, cr, ci);
+        else any = group_coef<CC, R>(st, sg[0].first, sg[0].count, s, cr, ci);
+        if (any) {
           #pragma unroll
           for (int v = 0; v < VPL; ++v) {
             ar[v] += cr * x0r[v];
@@ -334,19 +339,20 @@ int launch_apply(const qk_plan* p, const void* x, void* y, cudaStream_t s, qk_wo
 }
 
 template <int DT, bool CC, int LPR, int VPL>
-int launch_block(const qk_plan* p, qk_workspace* w, const void* X, void* Y, double* dots, cudaStream_t s) {
+int launch_block(const qk_plan* p, qk_workspace* w, const void* X, void* Y, const void* diag, double* dots,
+                 cudaStream_t s) {
   auto k = k_hx_block<DT, CC, LPR, VPL>;
   if (set_smem(k, p->smem)) return QKD_EINVAL;
   const unsigned g = std::min<unsigned>(hx_grid(p, k), kMaxG);
-  k<<<g, kTile, p->smem, s>>>(dev(p), X, Y, w->partials, w->ticket, dots ? dots : w->result);
+  k<<<g, kTile, p->smem, s>>>(dev(p), X, Y, diag, w->partials, w->ticket, dots ? dots : w->result);
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
 
 template <int DT, bool CC>
-int launch_block_shape(const qk_plan* p, qk_workspace* w, int R, int lpr, const void* X, void* Y, double* dots,
-                       cudaStream_t s) {
-#define QKD_BLK(RR, L, V) if (R == RR && lpr == L) return launch_block<DT, CC, L, V>(p, w, X, Y, dots, s);
+int launch_block_shape(const qk_plan* p, qk_workspace* w, int R, int lpr, const void* X, void* Y, const void* diag,
+                       double* dots, cudaStream_t s) {
+#define QKD_BLK(RR, L, V) if (R == RR && lpr == L) return launch_block<DT, CC, L, V>(p, w, X, Y, diag, dots, s);
   QKD_BLK(32, 32, 1) QKD_BLK(32, 16, 2) QKD_BLK(32, 8, 4)
   QKD_BLK(64, 32, 2) QKD_BLK(64, 16, 4) QKD_BLK(64, 8, 8)
   QKD_BLK(128, 32, 4) QKD_BLK(128, 16, 8)
@@ -461,19 +467,24 @@ int qkd_apply_block(const qk_plan* p, qk_dtype t, int nvec, const void* X, size_
 }
 
 int qkd_apply_rows(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lanes_per_row, const void* X,
-                   void* Y, double* dots, cudaStream_t s) {
+                   void* Y, const void* diag, double* dots, cudaStream_t s) {
   if (!p || !w || !X || !Y || X == Y || r_index(R) < 0) return QKD_EINVAL;
   if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
   if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
   const int lpr = lanes_per_row ? lanes_per_row : (p->rows_lpr[t][r_index(R)] ? p->rows_lpr[t][r_index(R)] : 32);
-  if (p->all_real) { QKD_DISPATCH(t, return launch_block_shape<DT, false>(p, w, R, lpr, X, Y, dots, s)); }
-  if (t == QK_C128) return launch_block_shape<QK_C128, true>(p, w, R, lpr, X, Y, dots, s);
-  if (t == QK_C64) return launch_block_shape<QK_C64, true>(p, w, R, lpr, X, Y, dots, s);
+  if (p->all_real) { QKD_DISPATCH(t, return launch_block_shape<DT, false>(p, w, R, lpr, X, Y, diag, dots, s)); }
+  if (t == QK_C128) return launch_block_shape<QK_C128, true>(p, w, R, lpr, X, Y, diag, dots, s);
+  if (t == QK_C64) return launch_block_shape<QK_C64, true>(p, w, R, lpr, X, Y, diag, dots, s);
   return QKD_EINVAL;
 }
 
-int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, cudaStream_t s,
-                  int* chosen) {
+int qkd_rows_shape(const qk_plan* p, qk_dtype t, int R) {
+  if (!p || r_index(R) < 0 || t < QK_C128 || t > QK_F32) return 0;
+  return p->rows_lpr[t][r_index(R)];
+}
+
+int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, const void* diag,
+                  cudaStream_t s, int* chosen) {
   if (!p || !w || r_index(R) < 0 || t < QK_C128 || t > QK_F32) return QKD_EINVAL;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return QKD_ECUDA;
@@ -481,9 +492,9 @@ int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X,
   int pick = 0;
   for (int lpr : {32, 16, 8}) {
     if (R / lpr > 8) continue;
-    if (qkd_apply_rows(p, w, t, R, lpr, X, Y, nullptr, s) != QKD_OK) continue;  // warm-up
+    if (qkd_apply_rows(p, w, t, R, lpr, X, Y, diag, nullptr, s) != QKD_OK) continue;  // warm-up
     cudaEventRecord(e0, s);
-    for (int i = 0; i < 3; ++i) qkd_apply_rows(p, w, t, R, lpr, X, Y, nullptr, s);
+    for (int i = 0; i < 3; ++i) qkd_apply_rows(p, w, t, R, lpr, X, Y, diag, nullptr, s);
     cudaEventRecord(e1, s);
     float ms = 0.f;
     if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) continue;
