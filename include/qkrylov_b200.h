@@ -228,6 +228,47 @@ int qkrylov_b200_ftlm_loop(qkrylov_hamiltonian_h h, int precision, int n_random,
                            int n_vectors, int n_temps, const double* temps, double* logZ, double* U, double* Cv,
                            qkrylov_b200_ftlm_info_t* info);
 
+/* ------------------------------------------------------ learned warm start
+ * No counterpart in the reference.  An MLP over the spin configurations of
+ * a spin-1/2 basis and a coupling J2: inputs the nsites spins as +-1 (bit
+ * set = +1) and J2, two hidden layers of 128 with GELU, outputs the
+ * log-amplitude o0 and a sign logit o1; BF16 weights, FP32 accumulation.
+ * Its start vector is phi(s) = M(s) exp(o0) tanh(o1) with M(s) =
+ * (-1)^(number of up spins on odd sites), Marshall's sign rule.  Training
+ * (forward, loss, backward, Adam; all on the GPU) fits o0 to log|psi| -
+ * log max|psi| and o1 to the sign of psi relative to M on samples drawn by
+ * |psi|^2 from each added ground state; per sample
+ *   loss = (o0 - a)^2 + c_sign * softplus(-y o1).
+ * Parameters (FP32): W1 [128][nsites+1], W2 [128][128], W3 [2][128], b1,
+ * b2, b3 (20,098 values for 24 sites). */
+typedef struct qkrylov_b200_mlp_t* qkrylov_b200_mlp_h;
+
+qkrylov_b200_mlp_h qkrylov_b200_mlp_create(qkrylov_basis_h basis, int device, uint64_t seed);
+void qkrylov_b200_mlp_destroy(qkrylov_b200_mlp_h net);
+size_t qkrylov_b200_mlp_num_params(qkrylov_b200_mlp_h net);
+int qkrylov_b200_mlp_get_params(qkrylov_b200_mlp_h net, float* out);
+int qkrylov_b200_mlp_set_params(qkrylov_b200_mlp_h net, const float* in);
+/* A real ground state psi (dimension() doubles, host) at coupling j2. */
+int qkrylov_b200_mlp_add_target(qkrylov_b200_mlp_h net, double j2, const double* psi);
+/* `steps` Adam steps (learning rate lr with cosine decay to lr/20) on
+ * minibatches of `batch` samples split evenly over the targets; loss_out:
+ * NULL or `steps` doubles. */
+int qkrylov_b200_mlp_train(qkrylov_b200_mlp_h net, int steps, int batch, double lr, uint64_t seed, double c_sign,
+                           double* loss_out);
+/* phi at coupling j2 over the whole basis (not normalised), FP32, into host
+ * memory or (out_on_device) device memory of the network's GPU. */
+int qkrylov_b200_mlp_start_vector(qkrylov_b200_mlp_h net, double j2, float* out, int out_on_device);
+/* Mean loss and its gradient (layout of the parameters) over n explicit
+ * samples: states (host), j2 per sample, targets (a, y, weight) per sample. */
+int qkrylov_b200_mlp_loss_grad(qkrylov_b200_mlp_h net, int n, const uint64_t* states, const double* j2,
+                               const float* targets, double c_sign, float* grad_out, double* loss_out);
+/* qkrylov_b200_lanczos_mixed started from the network's start vector at
+ * j2 (built on the GPU, its time included in seconds_low and returned in
+ * seconds_inference).  The operator must be real and act on the network's
+ * basis. */
+int qkrylov_b200_lanczos_warm(qkrylov_hamiltonian_h h, qkrylov_b200_mlp_h net, double j2, int maxiter, double tol,
+                              qkrylov_b200_mixed_result_t* result, double* seconds_inference);
+
 #ifdef __cplusplus
 }
 #endif

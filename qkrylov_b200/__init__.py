@@ -248,7 +248,10 @@ class Basis:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().qkrylov_basis_destroy(h)
+            try:
+                lib().qkrylov_basis_destroy(h)
+            except Exception:  # interpreter shutdown: the library is already gone
+                pass
             self._h = None
 
     @property
@@ -375,7 +378,10 @@ class MatrixFreeHamiltonian:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().qkrylov_hamiltonian_destroy(h)
+            try:
+                lib().qkrylov_hamiltonian_destroy(h)
+            except Exception:  # interpreter shutdown: the library is already gone
+                pass
             self._h = None
 
     @property
@@ -567,6 +573,91 @@ def ftlm_loop(H: MatrixFreeHamiltonian, temperatures: Sequence[float], n_random:
     nv = n_random if n_vectors is None else n_vectors
     return _ftlm_call(lib().qkrylov_b200_ftlm_loop, H, temperatures,
                       ((precision, n_random, n_steps, ctypes.c_uint64(seed), nv), ()))
+
+
+class WarmStartMLP:
+    """Learned warm start for spin-1/2 ground states: an MLP (spins as +-1
+    and the coupling J2 -> 128 -> 128 -> log-amplitude, sign logit; GELU;
+    BF16 weights, FP32 accumulation) trained on the GPU by the library's own
+    kernels on ground states added with add_target, whose start vector
+    M(s) exp(o0) tanh(o1) (M: Marshall's sign rule) seeds Lanczos at new
+    couplings (lanczos_warm)."""
+
+    def __init__(self, basis: "SpinHalfBasis", seed: int = 0, device: int = 0):
+        self._basis = basis
+        self._h = lib().qkrylov_b200_mlp_create(basis._h, device, ctypes.c_uint64(seed))
+        if not self._h:
+            raise RuntimeError(lib().qkrylov_b200_last_error().decode())
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().qkrylov_b200_mlp_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def n_params(self) -> int:
+        return int(lib().qkrylov_b200_mlp_num_params(self._h))
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, np.float32)
+        _check(lib().qkrylov_b200_mlp_get_params(self._h, p.ctypes.data), "mlp params")
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.n_params:
+            raise ValueError("parameter vector has the wrong size")
+        _check(lib().qkrylov_b200_mlp_set_params(self._h, p.ctypes.data), "mlp params")
+
+    def add_target(self, j2: float, psi: np.ndarray):
+        psi = np.ascontiguousarray(np.real(psi), dtype=np.float64)
+        if psi.size != self._basis.size:
+            raise ValueError("target state has the wrong length")
+        _check(lib().qkrylov_b200_mlp_add_target(self._h, float(j2), psi.ctypes.data), "mlp target")
+
+    def train(self, steps: int = 1000, batch: int = 8192, lr: float = 1e-3, seed: int = 0,
+              c_sign: float = 1.0) -> np.ndarray:
+        loss = np.zeros(max(steps, 1))
+        _check(lib().qkrylov_b200_mlp_train(self._h, steps, batch, lr, ctypes.c_uint64(seed), c_sign,
+                                            loss.ctypes.data), "mlp train")
+        return loss[:steps]
+
+    def start_vector(self, j2: float) -> np.ndarray:
+        out = np.zeros(self._basis.size, np.float32)
+        _check(lib().qkrylov_b200_mlp_start_vector(self._h, float(j2), out.ctypes.data, 0), "mlp start vector")
+        return out
+
+    def loss_grad(self, states, j2, targets, c_sign: float = 1.0):
+        st = np.ascontiguousarray(states, dtype=np.uint64)
+        j = np.ascontiguousarray(np.broadcast_to(np.asarray(j2, np.float64), st.shape), dtype=np.float64)
+        tg = np.ascontiguousarray(targets, dtype=np.float32)
+        if tg.shape != (st.size, 3):
+            raise ValueError("targets must be (n, 3): log-amplitude, sign, weight")
+        g = np.zeros(self.n_params, np.float32)
+        loss = ctypes.c_double()
+        _check(lib().qkrylov_b200_mlp_loss_grad(self._h, st.size, st.ctypes.data, j.ctypes.data, tg.ctypes.data,
+                                                c_sign, g.ctypes.data, ctypes.byref(loss)), "mlp loss")
+        return loss.value, g
+
+
+def lanczos_warm(H: MatrixFreeHamiltonian, net: WarmStartMLP, j2: float, maxiter: int = 200,
+                 tol: float = 1e-10) -> MixedLanczosResult:
+    """lanczos_mixed started from the network's start vector at j2 (built on
+    the GPU; its time is part of the result's seconds and is also given as
+    seconds_inference)."""
+    r = _MixedC()
+    tinf = ctypes.c_double()
+    _check(lib().qkrylov_b200_lanczos_warm(H._h, net._h, float(j2), maxiter, tol, ctypes.byref(r),
+                                           ctypes.byref(tinf)), "lanczos_warm")
+    out = MixedLanczosResult(r, [], None)
+    out.seconds_inference = tinf.value
+    return out
 
 
 class DavidsonResult:

@@ -100,6 +100,16 @@ PROTOTYPES = {
     "qkrylov_b200_lanczos_fp64": (_i, [_vp, _u64, _vp, _i, _i, _d, _vp, _vp, _i, _vp, _vp, _vp]),
     "qkrylov_b200_ftlm_block": (_i, [_vp, _i, _i, _i, _u64, _i, _vp, _vp, _vp, _vp, _i, _vp]),
     "qkrylov_b200_ftlm_loop": (_i, [_vp, _i, _i, _i, _u64, _i, _i, _vp, _vp, _vp, _vp, _vp]),
+    "qkrylov_b200_mlp_create": (_vp, [_vp, _i, _u64]),
+    "qkrylov_b200_mlp_destroy": (None, [_vp]),
+    "qkrylov_b200_mlp_num_params": (_sz, [_vp]),
+    "qkrylov_b200_mlp_get_params": (_i, [_vp, _vp]),
+    "qkrylov_b200_mlp_set_params": (_i, [_vp, _vp]),
+    "qkrylov_b200_mlp_add_target": (_i, [_vp, _d, _vp]),
+    "qkrylov_b200_mlp_train": (_i, [_vp, _i, _i, _d, _u64, _d, _vp]),
+    "qkrylov_b200_mlp_start_vector": (_i, [_vp, _d, _vp, _i]),
+    "qkrylov_b200_mlp_loss_grad": (_i, [_vp, _i, _vp, _vp, _vp, _d, _vp, _vp]),
+    "qkrylov_b200_lanczos_warm": (_i, [_vp, _vp, _d, _i, _d, _vp, _vp]),
 }
 
 _lock = threading.Lock()

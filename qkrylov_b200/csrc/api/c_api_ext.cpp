@@ -1,11 +1,13 @@
 // Extended C ABI (include/qkrylov_b200.h): double precision, device
 // pointers, multi-temperature FTLM, compiler inspection, diagnostics.
+#include <chrono>
 #include <cstring>
 #include <exception>
 #include <memory>
 
 #include "api/handles.hpp"
 #include "engine/solvers.hpp"
+#include "engine/warmstart.hpp"
 #include "qkrylov_b200.h"
 
 namespace qkapi {
@@ -348,6 +350,121 @@ int qkrylov_b200_ftlm_loop(qkrylov_hamiltonian_h h, int precision, int n_random,
                            int n_vectors, int n_temps, const double* temps, double* logZ, double* U, double* Cv,
                            qkrylov_b200_ftlm_info_t* info) {
   return ftlm_common(h, false, precision, n_random, n_steps, seed, n_vectors, n_temps, temps, logZ, U, Cv, 0, info);
+}
+
+struct qkrylov_b200_mlp_t {
+  std::unique_ptr<qkb::WarmStartNet> net;
+};
+
+qkrylov_b200_mlp_h qkrylov_b200_mlp_create(qkrylov_basis_h basis, int device, uint64_t seed) {
+  if (!basis || !basis->table) return nullptr;
+  try {
+    auto* h = new qkrylov_b200_mlp_t;
+    h->net = std::make_unique<qkb::WarmStartNet>(basis->table, device, seed);
+    return h;
+  } catch (const std::exception& e) {
+    qkapi::set_error(e.what());
+    return nullptr;
+  }
+}
+
+void qkrylov_b200_mlp_destroy(qkrylov_b200_mlp_h h) { delete h; }
+
+size_t qkrylov_b200_mlp_num_params(qkrylov_b200_mlp_h h) { return h ? h->net->num_params() : 0; }
+
+int qkrylov_b200_mlp_get_params(qkrylov_b200_mlp_h h, float* out) {
+  if (!h || !out) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const auto p = h->net->params();
+    std::copy(p.begin(), p.end(), out);
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_mlp_set_params(qkrylov_b200_mlp_h h, const float* in) {
+  if (!h || !in) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    h->net->set_params(std::vector<float>(in, in + h->net->num_params()));
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_mlp_add_target(qkrylov_b200_mlp_h h, double j2, const double* psi) {
+  if (!h || !psi) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    h->net->add_target(j2, psi);
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_mlp_train(qkrylov_b200_mlp_h h, int steps, int batch, double lr, uint64_t seed, double c_sign,
+                           double* loss_out) {
+  if (!h || steps < 0 || batch < 1 || !(lr > 0)) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const auto l = h->net->train(steps, batch, lr, seed, c_sign);
+    if (loss_out) std::copy(l.begin(), l.end(), loss_out);
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_mlp_start_vector(qkrylov_b200_mlp_h h, double j2, float* out, int out_on_device) {
+  if (!h || !out) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const uint64_t dim = h->net->dim();
+    if (out_on_device) {
+      h->net->start_vector(j2, out);
+      return QKRYLOV_SUCCESS;
+    }
+    float* d = nullptr;
+    qkb::cuda_check(cudaMalloc(&d, dim * 4), "device allocation");
+    try {
+      h->net->start_vector(j2, d);
+      qkb::cuda_check(cudaMemcpy(out, d, dim * 4, cudaMemcpyDeviceToHost), "D2H");
+    } catch (...) {
+      cudaFree(d);
+      throw;
+    }
+    cudaFree(d);
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_mlp_loss_grad(qkrylov_b200_mlp_h h, int n, const uint64_t* states, const double* j2,
+                               const float* targets, double c_sign, float* grad_out, double* loss_out) {
+  if (!h || n < 1 || !states || !j2 || !targets) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    std::vector<float> g;
+    const double l = h->net->loss_grad(n, states, j2, targets, c_sign, grad_out ? &g : nullptr);
+    if (grad_out) std::copy(g.begin(), g.end(), grad_out);
+    if (loss_out) *loss_out = l;
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_lanczos_warm(qkrylov_hamiltonian_h h, qkrylov_b200_mlp_h net, double j2, int maxiter, double tol,
+                              qkrylov_b200_mixed_result_t* result, double* seconds_inference) {
+  if (!h || !h->op || !net || !result || maxiter < 1 || maxiter > 511 || !(tol > 0)) return QKRYLOV_ERROR_INVALID_ARG;
+  if (!h->op->all_real() || h->op->dim() != net->net->dim()) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const qkb::Operator& H = *h->op;
+    const auto t0 = std::chrono::steady_clock::now();
+    qkb::DevVec start(H.dim(), QK_F32, H.device(), false);
+    net->net->start_vector(j2, static_cast<float*>(start.data()));
+    H.ctx().sync();
+    const double tinf = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    auto r = qkb::lanczos_mixed(H, start.data(), 0, maxiter, tol, nullptr, true);
+    result->energy = r.energy;
+    result->residual = r.residual;
+    result->seconds_low = r.seconds_low + tinf;
+    result->seconds_high = r.seconds_high;
+    result->iterations_low = r.iters_low;
+    result->iterations_high = r.iters_high;
+    result->restarts = r.restarts;
+    result->converged = r.converged;
+    result->trace_len = 0;
+    if (seconds_inference) *seconds_inference = tinf;
+    return QKRYLOV_SUCCESS;
+  });
 }
 
 int qkrylov_davidson_lowest_f64(qkrylov_hamiltonian_h h, int n_eig, int max_subspace, double tol, double* evals,
