@@ -16,6 +16,8 @@ tables, term tables and repeated gathers are not counted).
          refinement, both to the explicit residual 1e-10 (wall seconds)
   batched_ftlm  t-J N=20 FTLM, 64 vectors x 100 steps x 200 temperatures:
          one block (FP32 / FP64 vectors, CUDA graph) vs the one-vector loop
+  warm_start  J1-J2 N=24: network trained on 32 couplings, time-to-E0 at
+         untrained couplings for plain FP64 / mixed / mixed + warm start
 
 --impl reference times the reference's own CPU implementation (its
 unchanged sources, oracle/_ref, OpenMP on all host cores) on a bounded
@@ -223,6 +225,77 @@ def batched_ftlm(qk, N=20, R=64, M=100, loop_vectors=4, seed=5):
     return out
 
 
+def j1j2_opsum(qk, N, J1, J2):
+    """Periodic J1-J2 chain: per bond (nearest, then next-nearest)
+    J Sz Sz + J/2 (Sp Sm + Sm Sp)."""
+    os_ = qk.OpSum(dtype=np.float64)
+    for d, J in ((1, J1), (2, J2)):
+        for i in range(N):
+            j = (i + d) % N
+            os_.add_term(J, "Sz", i, "Sz", j)
+            os_.add_term(0.5 * J, "Sp", i, "Sm", j)
+            os_.add_term(0.5 * J, "Sm", i, "Sp", j)
+    return os_
+
+
+def warm_start(qk, N=24, eval_every=16, eval_offset=4, steps=1500, batch=8192, tol=1e-10):
+    """J1-J2 chain, Sz=0: plain FP64 Lanczos ground states at J2_k = k/255
+    for k = 0, 8, ..., 248 train the warm-start network on the GPU; at the
+    untrained couplings k = eval_offset, eval_offset + eval_every, ... the
+    plain FP64 GPU Lanczos (random start), the mixed-precision form (random
+    start) and the mixed form from the network's start vector (inference
+    included) are each timed to the explicit residual tol."""
+    B = qk.SpinHalfBasis(N, sz=0)
+    t0 = time.perf_counter()
+    net = qk.WarmStartMLP(B, seed=0)
+    train_k = list(range(0, 256, 8))
+    gs_s = 0.0
+    for k in train_k:
+        H = qk.MatrixFreeHamiltonian(B, qk.SpinHalfSite(), j1j2_opsum(qk, N, 1.0, k / 255.0), dtype=np.float64)
+        t1 = time.perf_counter()
+        r = qk.lanczos_fp64(H, seed=1, tol=tol, eigenvector=True)
+        gs_s += time.perf_counter() - t1
+        net.add_target(k / 255.0, r.eigenvector)
+        del H
+    t1 = time.perf_counter()
+    loss = net.train(steps=steps, batch=batch, lr=2e-3, seed=3)
+    train_s = time.perf_counter() - t1
+    rows = []
+    for k in range(eval_offset, 256, eval_every):
+        if k % 8 == 0:
+            continue
+        j2 = k / 255.0
+        H = qk.MatrixFreeHamiltonian(B, qk.SpinHalfSite(), j1j2_opsum(qk, N, 1.0, j2), dtype=np.float64)
+        qk.lanczos_mixed(H, seed=2, tol=tol)  # warm-up of this operator's kernels
+        res = {}
+        for name, fn in (("plain_fp64", lambda: qk.lanczos_fp64(H, seed=2, tol=tol)),
+                         ("mixed", lambda: qk.lanczos_mixed(H, seed=2, tol=tol)),
+                         ("mixed_warm", lambda: qk.lanczos_warm(H, net, j2, tol=tol))):
+            t1 = time.perf_counter()
+            r = fn()
+            res[name] = (time.perf_counter() - t1, r)
+        e_ref = res["plain_fp64"][1].energy
+        rows.append({"J2": j2,
+                     "seconds": {n: v[0] for n, v in res.items()},
+                     "iterations": {n: v[1].iterations_low + v[1].iterations_high for n, v in res.items()},
+                     "inference_s": res["mixed_warm"][1].seconds_inference,
+                     "dE": {n: abs(v[1].energy - e_ref) for n, v in res.items()},
+                     "converged": all(v[1].converged for v in res.values())})
+        del H
+    tot = {n: sum(r["seconds"][n] for r in rows) for n in ("plain_fp64", "mixed", "mixed_warm")}
+    return {"workload": f"j1j2_chain_N{N}_Sz0", "dim": B.size, "train_J2": len(train_k),
+            "eval_J2": [r["J2"] for r in rows], "train_steps": steps, "batch": batch,
+            "train_seconds": train_s, "ground_state_seconds": gs_s, "loss_first": float(loss[:20].mean()),
+            "loss_last": float(loss[-20:].mean()), "params": net.n_params,
+            "total_seconds": tot, "speedup_mixed": tot["plain_fp64"] / tot["mixed"],
+            "speedup_mixed_warm": tot["plain_fp64"] / tot["mixed_warm"],
+            "max_dE": max(max(r["dE"].values()) for r in rows), "all_converged": all(r["converged"] for r in rows),
+            "mean_iterations": {n: float(np.mean([r["iterations"][n] for r in rows]))
+                                for n in ("plain_fp64", "mixed", "mixed_warm")},
+            "mean_inference_s": float(np.mean([r["inference_s"] for r in rows])),
+            "wall_seconds": time.perf_counter() - t0}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -359,6 +432,11 @@ def run_b200(args):
             line["batched_ftlm"] = batched_ftlm(qk)
         except Exception as e:
             line["batched_ftlm"] = {"error": str(e)}
+        try:
+            torch.cuda.empty_cache()
+            line["warm_start"] = warm_start(qk)
+        except Exception as e:
+            line["warm_start"] = {"error": str(e)}
     if rank == 0 and not args.no_cpu_baseline:
         try:
             cb = cpu_reference_gbs(N=24, steps=2)

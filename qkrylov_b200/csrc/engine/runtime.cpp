@@ -29,6 +29,33 @@ Context::Context(int dev) : device(dev) {
   cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
   qkd_check(qkd_workspace_create(dev, &ws), "workspace");
   cuda_check(cudaMallocHost(&host, sizeof(double) * kHost), "cudaMallocHost");
+  // Solver vectors come from the device's stream-ordered pool, which keeps
+  // freed memory for the next solve instead of returning it at every
+  // synchronisation (a Lanczos run allocates and frees one vector per step).
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = ~0ull;
+    (void)cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  (void)cudaGetLastError();
+}
+
+void* Context::alloc(size_t bytes) {
+  void* p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+  if (e != cudaSuccess) {  // give the pool's cached memory back and retry once
+    (void)cudaGetLastError();
+    cudaStreamSynchronize(stream);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+    e = cudaMallocAsync(&p, bytes, stream);
+  }
+  cuda_check(e, "device allocation");
+  return p;
+}
+
+void Context::release(void* p) {
+  if (p) cudaFreeAsync(p, stream);
 }
 
 Context& Context::get(int dev) {
@@ -55,17 +82,17 @@ void Context::sync() { cuda_check(cudaStreamSynchronize(stream), "stream sync");
 DevVec::DevVec(size_t n, qk_dtype t, int device, bool zero) : n_(n), t_(t), dev_(device) {
   if (n == 0) return;
   Context& c = Context::get(device);
-  cuda_check(cudaMalloc(&p_, bytes()), "device allocation");
+  p_ = c.alloc(bytes());
   if (zero) cuda_check(cudaMemsetAsync(p_, 0, bytes(), c.stream), "memset");
 }
 
 DevVec::~DevVec() {
-  if (p_) { cudaSetDevice(dev_); cudaFree(p_); }
+  if (p_) Context::get(dev_).release(p_);
 }
 
 DevVec& DevVec::operator=(DevVec&& o) noexcept {
   if (this != &o) {
-    if (p_) { cudaSetDevice(dev_); cudaFree(p_); }
+    if (p_) Context::get(dev_).release(p_);
     p_ = o.p_; n_ = o.n_; t_ = o.t_; dev_ = o.dev_;
     o.p_ = nullptr; o.n_ = 0;
   }

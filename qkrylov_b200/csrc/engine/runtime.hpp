@@ -37,12 +37,18 @@ class Context {
   const double* fetch(const double* dev, int n);
   void sync();
   void activate() const;
+  // Stream-ordered device memory on this context's stream (the device's
+  // default pool, which keeps freed blocks); release() is ordered after all
+  // work already issued on the stream.
+  void* alloc(size_t bytes);
+  void release(void* p);
 
  private:
   explicit Context(int device);
 };
 
-// A device allocation of n elements of one dtype (zero-filled when asked).
+// A device allocation of n elements of one dtype (zero-filled when asked),
+// from the context's stream-ordered pool; only the context stream may use it.
 class DevVec {
  public:
   DevVec() = default;

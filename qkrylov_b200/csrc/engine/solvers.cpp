@@ -411,8 +411,12 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
     eps_prev = eps;
     const double target = std::max(0.3 * tol_res, 1e-6 * eps);
     const double tp0 = now_s();
-    const int m = refine_pass(H, ti, hi, psi, w, e, nr, maxiter, target, V, psi_t, wt, tmp, P, coef, out.trace,
-                              steps + out.iters_high, t0);
+    // passes of at most kPass steps: the reorthogonalisation cost of a pass
+    // grows with the square of its length, a restart from the Ritz vector
+    // resets it
+    constexpr int kPass = 64;
+    const int m = refine_pass(H, ti, hi, psi, w, e, nr, std::min(maxiter, kPass), target, V, psi_t, wt, tmp, P,
+                              coef, out.trace, steps + out.iters_high, t0);
     steps += m;
     if (ti == lo) out.iters_low += m;
     else { out.iters_high += m; t_fp64 += now_s() - tp0; }
