@@ -115,6 +115,18 @@ def profiled_traffic():
         return None
 
 
+def replica_throughput(ms, bytes_step, world, dist=None, device="cpu"):
+    """Replicas: every rank applies H to its own vector; the step time is
+    the maximum over ranks and the throughput is world * bytes / that time.
+    Returns (max ms, GB/s)."""
+    if dist is not None and world > 1:
+        import torch
+        t = torch.tensor([ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, world * bytes_step / (ms * 1e-3) / 1e9
+
+
 def tj_opsum(qk, N, t, J):
     """Periodic t-J chain: hops -t (annihilator listed first, both spins,
     both directions) and J (S_i.S_j - n_i n_j / 4) as -J/2 (Nup_i Ndn_j +
@@ -372,12 +384,8 @@ def run_b200(args):
         return
     with ClockSampler(local) as clk:
         ms, launches = time_apply(qk.DTYPE_C128, torch.complex128, 32, args.steps, args.warmup)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     bytes_step = D * 32
-    value = world * bytes_step / (ms * 1e-3) / 1e9
+    ms, value = replica_throughput(ms, bytes_step, world, dist, "cuda")
 
     variants = {}
     for name, code, tdt, b in [("c64", qk.DTYPE_C64, torch.complex64, 16), ("f64", qk.DTYPE_F64, torch.float64, 16),
