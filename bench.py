@@ -102,7 +102,7 @@ class ClockSampler:
 
 # ncu summary of the default kernel on this workload (complex128, N=28);
 # its dram_bytes_per_launch line is the roofline's measured traffic.
-PROFILE = os.path.join(ROOT, "profiles", "hx_spin_owner_heisenberg_n28_c128.md")
+PROFILE = os.path.join(ROOT, "profiles", "hx_spin_rows_heisenberg_n28.md")
 
 
 def profiled_traffic():
