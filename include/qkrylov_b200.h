@@ -192,6 +192,31 @@ int qkrylov_b200_lanczos_fp64(qkrylov_hamiltonian_h h, uint64_t seed, const void
                               int maxiter, double tol, qkrylov_b200_mixed_result_t* result, void* psi_out,
                               int trace_cap, int* trace_iteration, double* trace_energy, double* trace_seconds);
 
+/* ---------------------------------------------------------- block Davidson
+ * No counterpart in the reference (its davidson_lowest, davidson.hpp:21-27,
+ * has no block size and keeps complex V and HV, 340 GB for Hubbard 4x4).
+ * For real operators on float32 (precision 32) or float64 (64) vectors: a
+ * seeded random start block of `block` vectors, corrections r / (diag -
+ * theta) with the reference's clamp (davidson.cpp:171-175) for the
+ * unconverged among the lowest `block` Ritz pairs, orthogonalised twice
+ * against the basis; restart from the lowest 2*block Ritz vectors when the
+ * basis would exceed max_subspace (3*block <= max_subspace <= 510).  Only
+ * the basis is stored (H is applied again to the Ritz vectors for the
+ * residuals).  Converged when the n_eig lowest residual norms
+ * ||H u - theta u|| are below tol.  evecs: NULL or n_eig * dimension()
+ * doubles (host, vector a at a * dimension()). */
+typedef struct {
+  int iterations;
+  int applies;   /* H.x products */
+  int restarts;
+  int converged;
+  double seconds;
+} qkrylov_b200_davidson_info_t;
+
+int qkrylov_b200_davidson_block(qkrylov_hamiltonian_h h, int precision, int n_eig, int block, int max_subspace,
+                                double tol, uint64_t seed, int maxiter, double* evals, double* residuals,
+                                double* evecs, qkrylov_b200_davidson_info_t* info);
+
 /* ---------------------------------------------------------- batched FTLM
  * No counterpart in the reference (its ftlm, ftlm.hpp:21-27, runs one
  * complex Gaussian vector at a time and one temperature per call).

@@ -660,6 +660,34 @@ def lanczos_warm(H: MatrixFreeHamiltonian, net: WarmStartMLP, j2: float, maxiter
     return out
 
 
+class DavidsonBlockResult:
+    def __init__(self, evals, resid, evecs, info):
+        self.eigenvalues, self.residuals, self.eigenvectors = evals, resid, evecs
+        self.iterations, self.applies, self.restarts = info.iterations, info.applies, info.restarts
+        self.converged, self.seconds = bool(info.converged), info.seconds
+
+    def __repr__(self):
+        return (f"DavidsonBlockResult(eigenvalues={self.eigenvalues}, iterations={self.iterations}, "
+                f"applies={self.applies}, seconds={self.seconds:.3f})")
+
+
+def davidson_block(H: MatrixFreeHamiltonian, n_eig: int = 4, block: int = 8, max_subspace: int = 64,
+                   tol: float = 1e-8, seed: int = 0, maxiter: int = 200, precision: int = 64,
+                   eigenvectors: bool = False) -> DavidsonBlockResult:
+    """Block Davidson on real vectors for real operators: n_eig lowest
+    eigenpairs with `block` corrections per iteration, diagonal
+    preconditioner, basis of at most max_subspace vectors, seeded random
+    start block; converged at residual norms < tol."""
+    ev, rs = np.zeros(n_eig), np.zeros(n_eig)
+    vec = np.zeros((n_eig, H.dimension)) if eigenvectors else None
+    info = _DavidsonBlockInfo()
+    _check(lib().qkrylov_b200_davidson_block(H._h, precision, n_eig, block, max_subspace, tol, ctypes.c_uint64(seed),
+                                             maxiter, ev.ctypes.data, rs.ctypes.data,
+                                             vec.ctypes.data if vec is not None else None, ctypes.byref(info)),
+           "davidson_block")
+    return DavidsonBlockResult(ev, rs, vec, info)
+
+
 class DavidsonResult:
     def __init__(self, eigenvalues, eigenvectors, iterations=0, converged=False):
         self.eigenvalues, self.eigenvectors = eigenvalues, eigenvectors
@@ -788,6 +816,11 @@ class _LanczosF64(ctypes.Structure):
 
 class _LanczosC(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_float), ("iterations", ctypes.c_int), ("converged", ctypes.c_int)]
+
+
+class _DavidsonBlockInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("applies", ctypes.c_int), ("restarts", ctypes.c_int),
+                ("converged", ctypes.c_int), ("seconds", ctypes.c_double)]
 
 
 class _FTLMInfo(ctypes.Structure):

@@ -467,6 +467,27 @@ int qkrylov_b200_lanczos_warm(qkrylov_hamiltonian_h h, qkrylov_b200_mlp_h net, d
   });
 }
 
+int qkrylov_b200_davidson_block(qkrylov_hamiltonian_h h, int precision, int n_eig, int block, int max_subspace,
+                                double tol, uint64_t seed, int maxiter, double* evals, double* residuals,
+                                double* evecs, qkrylov_b200_davidson_info_t* info) {
+  if (!h || !h->op || !evals || (precision != 32 && precision != 64) || !(tol > 0)) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    auto r = qkb::davidson_block(*h->op, precision == 32 ? QK_F32 : QK_F64, n_eig, block, max_subspace, tol, seed,
+                                 maxiter, evecs);
+    for (int a = 0; a < n_eig && a < int(r.eigenvalues.size()); ++a) evals[a] = r.eigenvalues[a];
+    if (residuals)
+      for (int a = 0; a < n_eig && a < int(r.residuals.size()); ++a) residuals[a] = r.residuals[a];
+    if (info) {
+      info->iterations = r.iterations;
+      info->applies = r.applies;
+      info->restarts = r.restarts;
+      info->converged = r.converged;
+      info->seconds = r.seconds;
+    }
+    return QKRYLOV_SUCCESS;
+  });
+}
+
 int qkrylov_davidson_lowest_f64(qkrylov_hamiltonian_h h, int n_eig, int max_subspace, double tol, double* evals,
                                 double* evecs, qkrylov_davidson_result_c_t* info) {
   if (!h || !h->op || !evals || n_eig <= 0) return QKRYLOV_ERROR_INVALID_ARG;

@@ -100,6 +100,57 @@ void tridiag_first(const std::vector<Real>& alpha, const std::vector<Real>& beta
   first.assign(z.begin(), z.begin() + n);
 }
 
+// Cyclic Jacobi eigen-decomposition of a real symmetric n x n matrix A
+// (row major, overwritten): sweeps over all pairs (p, q) until the
+// off-diagonal Frobenius norm falls below 1e-15 of the total (at most 60
+// sweeps).  evals ascending; evecs row major with eigenvector k in column k.
+inline void jacobi_symmetric(std::vector<double> A, int n, std::vector<double>& evals,
+                             std::vector<double>& evecs) {
+  std::vector<double> V(size_t(n) * n, 0.0);
+  for (int i = 0; i < n; ++i) V[size_t(i) * n + i] = 1.0;
+  auto a = [&](int i, int j) -> double& { return A[size_t(i) * n + j]; };
+  double total = 0.0;
+  for (double x : A) total += x * x;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j) off += 2.0 * a(i, j) * a(i, j);
+    if (off <= 1e-30 * total || off == 0.0) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a(p, q);
+        if (apq == 0.0) continue;
+        const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::abs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; ++k) {  // columns p, q
+          const double akp = a(k, p), akq = a(k, q);
+          a(k, p) = c * akp - s * akq;
+          a(k, q) = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {  // rows p, q
+          const double apk = a(p, k), aqk = a(q, k);
+          a(p, k) = c * apk - s * aqk;
+          a(q, k) = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = V[size_t(k) * n + p], vkq = V[size_t(k) * n + q];
+          V[size_t(k) * n + p] = c * vkp - s * vkq;
+          V[size_t(k) * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](int x, int y) { return a(x, x) < a(y, y); });
+  evals.resize(n);
+  evecs.assign(size_t(n) * n, 0.0);
+  for (int k = 0; k < n; ++k) {
+    evals[k] = a(ord[k], ord[k]);
+    for (int i = 0; i < n; ++i) evecs[size_t(i) * n + k] = V[size_t(i) * n + ord[k]];
+  }
+}
+
 // Jacobi eigen-decomposition of a small Hermitian matrix H (row major);
 // eigenvalues ascending, evecs[k*n + j] = component j of eigenvector k.
 template <class Real>

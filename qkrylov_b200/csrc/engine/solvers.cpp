@@ -429,6 +429,152 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
   return out;
 }
 
+// Block Davidson for real operators on real vectors (float32 / float64).
+// Only the basis V is stored: H V_j is formed once, when v_j enters, for
+// the new column of the projection T = V^T H V, and the residuals of the
+// lowest `block` Ritz pairs are recomputed as H u - theta u from the Ritz
+// vectors u = V y.  Corrections t = r / (diag - theta) (the reference's
+// clamped preconditioner) are orthogonalised against V twice (classical
+// Gram-Schmidt) and appended; when V would exceed max_subspace it restarts
+// from the lowest 2*block Ritz vectors (T becomes diagonal).
+DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int block, int max_subspace, double tol,
+                                uint64_t seed, int maxiter, double* evecs_out) {
+  if (t != QK_F32 && t != QK_F64) throw std::invalid_argument("qkrylov_b200: block Davidson needs real vectors");
+  if (!H.all_real()) throw std::invalid_argument("qkrylov_b200: block Davidson needs a real operator");
+  const uint64_t dim = H.dim();
+  if (n_eig < 1 || block < n_eig || max_subspace < 2 * block + block || uint64_t(max_subspace) > dim || maxiter < 1 ||
+      max_subspace > 510)
+    throw std::invalid_argument("qkrylov_b200: block Davidson sizes (n_eig <= block, 3 block <= max_subspace <= dim)");
+  DavidsonBlockOut out;
+  const double t0 = now_s();
+  Dev d(H, t);
+  const int dev = H.device();
+  DevVec diag = d.vec(false);
+  H.diagonal(t, diag.data());
+  std::vector<DevVec> V;
+  V.reserve(max_subspace);
+  std::vector<DevVec> U(2 * block), R(block);
+  DevVec w = d.vec(false);
+  PtrArray P(size_t(max_subspace) + 4, dev);
+  DevVec coef(size_t(2) * (max_subspace + 8), QK_F64, dev);
+  double* cd = static_cast<double*>(coef.data());
+  std::vector<double> T;  // m x m, row major
+  int m = 0, m_proj = 0;  // basis size; columns of T filled
+  // Orthonormalise x against V[0..m) (two passes) and append it; false if
+  // it vanished (linearly dependent).
+  auto append = [&](DevVec&& x) -> bool {
+    double before = d.dot(x.data(), x.data()).real();
+    for (int pass = 0; pass < 2 && m > 0; ++pass) {
+      d.update_mdot(0, nullptr, nullptr, P, m, x.data(), cd);
+      d.mupdate(P, m, cd, x.data(), cd + 2 * (m + 1));
+    }
+    const double nn = d.dot(x.data(), x.data()).real();
+    if (!(nn > 1e-20 * std::max(before, 1e-300)) || nn == 0.0) return false;
+    d.scal(1.0 / std::sqrt(nn), x.data());
+    P.set(m, x.data(), d.c.stream);
+    V.push_back(std::move(x));
+    ++m;
+    return true;
+  };
+  for (int a = 0; a < block; ++a) {
+    DevVec x = d.vec(false);
+    qkd_check(qkd_random(t, dim, seed * 7919ull + uint64_t(a) + 1, 0, x.data(), d.c.stream), "random");
+    append(std::move(x));
+  }
+  std::vector<double> theta, Y;
+  for (int it = 0; it < maxiter; ++it) {
+    out.iterations = it + 1;
+    // new columns of T: T[i][j] = <v_i, H v_j> for the vectors added since
+    for (int j = m_proj; j < m; ++j) {
+      H.apply(t, V[j].data(), w.data());
+      ++out.applies;
+      d.update_mdot(0, nullptr, nullptr, P, j + 1, w.data(), cd);
+      const double* dots = d.c.fetch(cd, 2 * (j + 1));
+      std::vector<double> Tn(size_t(j + 1) * (j + 1), 0.0);
+      for (int r = 0; r < j; ++r)
+        for (int c = 0; c < j; ++c) Tn[size_t(r) * (j + 1) + c] = T[size_t(r) * j + c];
+      for (int i = 0; i <= j; ++i) {
+        Tn[size_t(i) * (j + 1) + j] = dots[2 * i];
+        Tn[size_t(j) * (j + 1) + i] = dots[2 * i];
+      }
+      T.swap(Tn);
+    }
+    m_proj = m;
+    jacobi_symmetric(T, m, theta, Y);
+    // Ritz vectors and residuals of the lowest nb pairs
+    const int nb = std::min(block, m);
+    std::vector<double> cz(2 * size_t(m));
+    double worst = 0.0;
+    out.residuals.assign(nb, 0.0);
+    for (int a = 0; a < nb; ++a) {
+      for (int i = 0; i < m; ++i) { cz[2 * i] = Y[size_t(i) * m + a]; cz[2 * i + 1] = 0.0; }
+      cuda_check(cudaMemcpyAsync(cd, cz.data(), sizeof(double) * 2 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
+      if (!U[a].data()) U[a] = d.vec(false);
+      if (!R[a].data()) R[a] = d.vec(false);
+      qkd_check(qkd_combine(t, dim, m, P.at(0), cd, t, U[a].data(), d.c.stream), "combine");
+      H.apply(t, U[a].data(), R[a].data());
+      ++out.applies;
+      d.axpy({-theta[a], 0.0}, U[a].data(), R[a].data());
+      out.residuals[a] = std::sqrt(d.dot(R[a].data(), R[a].data()).real());
+      if (a < n_eig) worst = std::max(worst, out.residuals[a]);
+    }
+    out.trace.push_back({it + 1, theta[0], now_s() - t0, worst});
+    out.eigenvalues.assign(theta.begin(), theta.begin() + n_eig);
+    if (worst < tol) { out.converged = true; break; }
+    if (it + 1 == maxiter) break;
+    // corrections of the unconverged pairs among the lowest nb
+    std::vector<DevVec> C;
+    for (int a = 0; a < nb; ++a) {
+      if (out.residuals[a] < tol) continue;
+      DevVec c = d.vec(false);
+      qkd_check(qkd_dav_precond(t, dim, diag.data(), theta[a], R[a].data(), c.data(), d.c.stream), "precond");
+      C.push_back(std::move(c));
+    }
+    if (m + int(C.size()) > max_subspace) {  // restart from the lowest 2*block Ritz vectors
+      const int keep = std::min(2 * block, m);
+      for (int a = nb; a < keep; ++a) {
+        for (int i = 0; i < m; ++i) { cz[2 * i] = Y[size_t(i) * m + a]; cz[2 * i + 1] = 0.0; }
+        cuda_check(cudaMemcpyAsync(cd, cz.data(), sizeof(double) * 2 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
+        if (!U[a].data()) U[a] = d.vec(false);
+        qkd_check(qkd_combine(t, dim, m, P.at(0), cd, t, U[a].data(), d.c.stream), "combine");
+      }
+      std::vector<DevVec> NV;
+      for (int a = 0; a < keep; ++a) { NV.push_back(std::move(U[a])); U[a] = DevVec(); }
+      for (int a = 0; a < keep; ++a) { U[a] = std::move(V[a]); }  // recycle storage
+      V.clear();
+      for (int a = 0; a < keep; ++a) {
+        V.push_back(std::move(NV[a]));
+        P.set(a, V[a].data(), d.c.stream);
+      }
+      for (int a = keep; a < int(U.size()); ++a) U[a] = DevVec();
+      m = keep;
+      m_proj = keep;
+      T.assign(size_t(keep) * keep, 0.0);
+      for (int a = 0; a < keep; ++a) T[size_t(a) * keep + a] = theta[a];
+      ++out.restarts;
+    }
+    int added = 0;
+    for (auto& c : C)
+      if (m < max_subspace && append(std::move(c))) ++added;
+    if (added == 0) break;  // no new direction: stagnated
+  }
+  if (evecs_out) {
+    const size_t es = qk_dtype_size(t);
+    std::vector<char> buf(dim * es);
+    for (int a = 0; a < n_eig && a < int(U.size()); ++a) {
+      if (!U[a].data()) break;
+      cuda_check(cudaMemcpyAsync(buf.data(), U[a].data(), dim * es, cudaMemcpyDeviceToHost, d.c.stream), "D2H");
+      d.c.sync();
+      for (uint64_t i = 0; i < dim; ++i)
+        evecs_out[a * dim + i] = t == QK_F64 ? reinterpret_cast<const double*>(buf.data())[i]
+                                             : double(reinterpret_cast<const float*>(buf.data())[i]);
+    }
+  }
+  d.c.sync();
+  out.seconds = now_s() - t0;
+  return out;
+}
+
 template <class Real>
 CFOut<Real> continued_fraction(const Operator& H, const std::complex<Real>* phi0, int n_iter) {
   CFOut<Real> res;

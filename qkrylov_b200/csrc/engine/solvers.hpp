@@ -118,6 +118,19 @@ FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t se
 FtlmBlockOut ftlm_loop(const Operator& H, qk_dtype t, int R, int M, uint64_t seed, const std::vector<double>& temps,
                        int nvec);
 
+// Block Davidson (SURVEY configuration: k eigenpairs, block of corrections,
+// diagonal preconditioner, bounded subspace, seeded random block start) for
+// real operators on float32 / float64 vectors, storing only the basis.
+struct DavidsonBlockOut {
+  std::vector<double> eigenvalues, residuals;
+  int iterations = 0, applies = 0, restarts = 0;
+  bool converged = false;
+  double seconds = 0;
+  std::vector<TraceEntry> trace;  // (iteration, lowest Ritz value, seconds, worst residual of the k)
+};
+DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int block, int max_subspace, double tol,
+                                uint64_t seed, int maxiter, double* evecs_out);
+
 // src/solvers/dynamics.cpp:12-59
 template <class Real>
 CFOut<Real> continued_fraction(const Operator& H, const std::complex<Real>* phi0, int n_iter);
