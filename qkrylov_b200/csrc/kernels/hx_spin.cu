@@ -813,8 +813,18 @@ k_hx_spin_owner(const SpinPlan* __restrict__ pp, const void* __restrict__ x, voi
 // size, and crossing ranks are in-class ranks of the partner's class; the
 // plan builder checks the high-bond sizes.
 constexpr int kRowThreads = 256;
+#ifndef KRH_C128
+#define KRH_C128 4
+#endif
+#ifndef KRB_C128
+#define KRB_C128 3
+#endif
+#ifndef QKD_PF_AHEAD
+#define QKD_PF_AHEAD 2
+#endif
 constexpr int kRowCoef = 32, kRowEnt = 48, kRowCross = 16, kRowCls = 4;
 template <int DT> constexpr int kRowBatch = DT == QK_C128 ? 1 : 4;  // rows per thread and pass
+template <int DT> constexpr int kRowHighRegs = DT == QK_C128 ? KRH_C128 : 8;  // high bonds held in registers
 
 __device__ __forceinline__ void sld(const double2* s, uint32_t k, double& re, double& im) {
   const double2 v = s[k]; re = v.x; im = v.y;
@@ -829,6 +839,17 @@ __device__ __forceinline__ void szero(float2& v) { v = make_float2(0.f, 0.f); }
 __device__ __forceinline__ void szero(double& v) { v = 0.0; }
 __device__ __forceinline__ void szero(float& v) { v = 0.f; }
 
+// L2 prefetch of elements [first, first + count) of a vector of `es`-byte
+// elements, rounded inward to 16-byte boundaries (bulk prefetch operands
+// must be 16-byte aligned and sized).
+__device__ __forceinline__ void l2_prefetch(const void* base, uint32_t es, uint32_t first, uint32_t count) {
+  const uintptr_t b = reinterpret_cast<uintptr_t>(base);
+  const uintptr_t lo = (b + uintptr_t(first) * es + 15) & ~uintptr_t(15);
+  const uintptr_t hi = (b + uintptr_t(first + count) * es) & ~uintptr_t(15);
+  if (hi > lo)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"(uint32_t(hi - lo)) : "memory");
+}
+
 __device__ __forceinline__ RowBlock load_block(const RowBlock* p) {
   const uint4* q = reinterpret_cast<const uint4*>(p);
   const uint4 a = __ldg(q), b = __ldg(q + 1);
@@ -840,7 +861,7 @@ __device__ __forceinline__ RowBlock load_block(const RowBlock* p) {
 }
 
 template <int DT, bool DOT>
-__global__ void __launch_bounds__(kRowThreads, DT == QK_C128 ? 3 : 4)
+__global__ void __launch_bounds__(kRowThreads, DT == QK_C128 ? KRB_C128 : 4)
 k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
                double* partials, unsigned* ticket, double* dot_out) {
   using T = VT<DT>;
@@ -875,17 +896,30 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       s_eb[threadIdx.x] = e.x;
       s_ec[threadIdx.x] = s_coef[e.y & 0xFFFFu];
       if (threadIdx.x >= nh) s_ebit[threadIdx.x - nh] = e.y >> 16;
+#ifndef QKD_NO_HIGH_PREFETCH
+      else  // high partner rows of the first row chunks into L2
+        l2_prefetch(x, sizeof(E), e.x, min(size, uint32_t(QKD_PF_AHEAD) * kRowBatch<DT> * kRowThreads));
+#endif
+#ifdef QKD_PF_CROSS
+      if (threadIdx.x >= nh) {  // crossing partner block, whole
+        const uint32_t q = threadIdx.x - nh;
+        const uint32_t hp = h ^ p.cross_hi[q];
+        const uint32_t pb = __ldg(p.A32 + hp), pe = hp + 1 < nA ? __ldg(p.A32 + hp + 1) : uint32_t(p.dim);
+        l2_prefetch(x, sizeof(E), pb, pe - pb);
+      }
+#endif
     }
     __syncthreads();
     const R dh = R(cur.dh);
     const double* __restrict__ dcol = p.dtab + size_t(cur.combo) * nll;
     const uint32_t* __restrict__ ckw = reinterpret_cast<const uint32_t*>(p.crk);
-    // block-uniform entries in registers: the first 8 high bonds, 2 crossing
-    const int nh8 = nh < 8 ? int(nh) : 8;
-    uint32_t eb[8];
-    R ec[8];
+    // block-uniform entries in registers: the first NB high bonds, 2 crossing
+    constexpr int NB = kRowHighRegs<DT>;
+    const int nh8 = nh < uint32_t(NB) ? int(nh) : NB;
+    uint32_t eb[NB];
+    R ec[NB];
     #pragma unroll
-    for (int e = 0; e < 8; ++e) {
+    for (int e = 0; e < NB; ++e) {
       eb[e] = e < nh8 ? s_eb[e] : 0u;
       ec[e] = e < nh8 ? s_ec[e] : R(0);
     }
@@ -899,6 +933,14 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
     }
     constexpr int K = kRowBatch<DT>;
     for (uint32_t r0 = threadIdx.x; r0 < size; r0 += K * kRowThreads) {
+#ifndef QKD_NO_HIGH_PREFETCH
+      // the high partner rows two chunks ahead go to L2 while this chunk runs
+      {
+        const uint32_t ahead = r0 - threadIdx.x + uint32_t(QKD_PF_AHEAD) * K * kRowThreads;
+        if (threadIdx.x < nh && ahead < size)
+          l2_prefetch(x, sizeof(E), s_eb[threadIdx.x] + ahead, min(size - ahead, uint32_t(K * kRowThreads)));
+      }
+#endif
       // K rows r0 + k * 256 per thread.  Loads that do not depend on each
       // other are issued together: row records, diagonals, crossing pairs,
       // then all high-bond values; the shared-memory low groups come last.
@@ -920,7 +962,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       #pragma unroll
       for (int k = 0; k < K; ++k) { ar[k] = R(0); ai[k] = R(0); }
       #pragma unroll
-      for (int e = 0; e < 8; ++e) {
+      for (int e = 0; e < NB; ++e) {
         #pragma unroll
         for (int k = 0; k < K; ++k) {
           if (e < nh8 && ok[k]) {
@@ -948,7 +990,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       for (int k = 0; k < K; ++k) {
         if (!ok[k]) continue;
         const uint32_t r = rk[k];
-        for (uint32_t e = 8; e < nh; ++e) {
+        for (uint32_t e = NB; e < nh; ++e) {
           R vr, vi;
           T::ld(x, s_eb[e] + r, vr, vi);
           ar[k] += s_ec[e] * vr;
