@@ -77,7 +77,10 @@ qkrylov_hamiltonian_h qkrylov_hamiltonian_create_ex(qkrylov_basis_h basis, qkryl
 int qkrylov_hamiltonian_precision(qkrylov_hamiltonian_h h);
 int qkrylov_hamiltonian_all_real(qkrylov_hamiltonian_h h);
 uint64_t qkrylov_hamiltonian_device_bytes(qkrylov_hamiltonian_h h);
-/* 1 when this handle's H.x runs the specialised two-site exchange kernel. */
+/* The H.x kernel of this handle: 1 the two-site exchange kernel (spin
+ * models in a single-charge sector), 2 the two-part kernel (operators whose
+ * terms factorise over the sector split: Hubbard, t-J, fermion hops with
+ * Jordan-Wigner signs), 0 the generic term-table kernel. */
 int qkrylov_hamiltonian_kernel(qkrylov_hamiltonian_h h);
 /* The CUDA stream (cudaStream_t) the library uses on the handle's device. */
 void* qkrylov_hamiltonian_stream(qkrylov_hamiltonian_h h);

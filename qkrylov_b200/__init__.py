@@ -422,8 +422,11 @@ class MatrixFreeHamiltonian:
 
     @property
     def kernel(self) -> str:
-        """'spin-exchange' or 'generic': the H.x kernel this operator uses."""
-        return "spin-exchange" if lib().qkrylov_hamiltonian_kernel(self._h) else "generic"
+        """The H.x kernel this operator uses: 'spin-exchange' (two-site
+        exchange in a single-charge sector), 'two-part' (any operator whose
+        terms factorise over the sector split: Hubbard, t-J, fermions) or
+        'generic' (term-table walk)."""
+        return {1: "spin-exchange", 2: "two-part"}.get(int(lib().qkrylov_hamiltonian_kernel(self._h)), "generic")
 
     @property
     def stream(self) -> int:

@@ -18,6 +18,9 @@
 namespace qkd {
 struct SpinHandle;
 SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes);
+SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes);
+bool spin_plan_is_gen(const SpinHandle* h);
+int spin_plan_set_diag(SpinHandle* h, const double* diag);
 void spin_plan_destroy(SpinHandle* h);
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out);
@@ -40,6 +43,7 @@ struct qk_plan {
   int has_diag, all_real;
   size_t bytes, smem;
   int rows_lpr[4][3];  // autotuned lanes per row of the block apply, by dtype and R = 32, 64, 128
+  double* diag_re;     // real diagonal (generic-kernel operators with a real diagonal), else null
 };
 
 namespace qkd {
@@ -50,6 +54,7 @@ constexpr int kTile = 256;
 struct DevPlan {
   int L;
   uint64_t lmask;
+  const double* __restrict__ diag_re;
   const uint64_t* __restrict__ A;
   const uint32_t* __restrict__ B;
   const uint32_t* __restrict__ llist;
@@ -61,7 +66,7 @@ struct DevPlan {
 };
 
 DevPlan dev(const qk_plan* p) {
-  return DevPlan{p->L, p->lmask, p->A, p->B, p->llist, p->terms, p->groups, p->tiles,
+  return DevPlan{p->L, p->lmask, p->diag_re, p->A, p->B, p->llist, p->terms, p->groups, p->tiles,
                  p->nterms, p->ngroups, p->ntiles, p->has_diag};
 }
 
@@ -93,6 +98,11 @@ __device__ __forceinline__ void stage_plan(const DevPlan& p, qk_term_t*& st, qk_
 }
 
 // y = H x for one row; returns (y_re, y_im) and the row's own x element.
+// The diagonal comes from the plan's precomputed real diagonal when it has
+// one, else from the diagonal term group.  Off-diagonal groups are taken
+// kGB at a time: their coefficients and targets first, then all of their
+// gathers together, so up to kGB loads of x are in flight per row.
+constexpr int kGB = 8;
 template <int DT, bool CC>
 __device__ __forceinline__ void row_apply(const DevPlan& p, const qk_term_t* st, const qk_group_t* sg,
                                           uint64_t row, uint64_t s, const void* x,
@@ -104,8 +114,11 @@ __device__ __forceinline__ void row_apply(const DevPlan& p, const qk_term_t* st,
   T::ld(x, row, xr0, xi0);
   uint32_t g0 = 0;
   if (p.has_diag) {
-    R cr, ci;
-    if (group_coef<CC, R>(st, sg[0].first, sg[0].count, s, cr, ci)) {
+    R cr = R(0), ci = R(0);
+    bool any = true;
+    if (p.diag_re) cr = R(__ldg(p.diag_re + row));
+    else any = group_coef<CC, R>(st, sg[0].first, sg[0].count, s, cr, ci);
+    if (any) {
       yr += cr * xr0;
       if (T::cplx) {
         yi += cr * xi0;
@@ -114,24 +127,40 @@ __device__ __forceinline__ void row_apply(const DevPlan& p, const qk_term_t* st,
     }
     g0 = 1;
   }
-  for (uint32_t g = g0; g < p.ngroups; ++g) {
-    const qk_group_t grp = sg[g];
-    R cr, ci;
-    if (!group_coef<CC, R>(st, grp.first, grp.count, s, cr, ci)) continue;
-    const uint64_t t = s ^ grp.flip;
-    const uint64_t a = __ldg(p.A + (t >> p.L));
-    const uint32_t b = __ldg(p.B + (t & p.lmask));
-    // Membership is re-checked for every group (one byte compare), so a
-    // gather index is always a valid row even where the compiler proved the
-    // target stays in the sector.
-    if (uint32_t(a >> 56) != (b >> 24)) continue;
-    const uint64_t col = (a & qkb::kOffsetMask) + (b & qkb::kRankMask);
-    R xr, xi;
-    T::ld(x, col, xr, xi);
-    yr += cr * xr;
-    if (T::cplx) {
-      yi += cr * xi;
-      if (CC) { yr -= ci * xi; yi += ci * xr; }
+  for (uint32_t gb = g0; gb < p.ngroups; gb += kGB) {
+    uint64_t col[kGB];
+    R cr[kGB], ci[kGB];
+    bool ok[kGB];
+    #pragma unroll
+    for (int b = 0; b < kGB; ++b) {
+      const uint32_t g = gb + b;
+      ok[b] = false; col[b] = row; cr[b] = R(0); ci[b] = R(0);
+      if (g < p.ngroups) {
+        const qk_group_t grp = sg[g];
+        if (group_coef<CC, R>(st, grp.first, grp.count, s, cr[b], ci[b])) {
+          const uint64_t t = s ^ grp.flip;
+          const uint64_t a = __ldg(p.A + (t >> p.L));
+          const uint32_t bb = __ldg(p.B + (t & p.lmask));
+          // Membership is re-checked for every group (one byte compare), so a
+          // gather index is always a valid row even where the compiler proved
+          // the target stays in the sector.
+          if (uint32_t(a >> 56) == (bb >> 24)) {
+            ok[b] = true;
+            col[b] = (a & qkb::kOffsetMask) + (bb & qkb::kRankMask);
+          }
+        }
+      }
+    }
+    #pragma unroll
+    for (int b = 0; b < kGB; ++b) {
+      if (!ok[b]) continue;
+      R vr, vi;
+      T::ld(x, col[b], vr, vi);
+      yr += cr[b] * vr;
+      if (T::cplx) {
+        yi += cr[b] * vi;
+        if (CC) { yr -= ci[b] * vi; yi += ci[b] * vr; }
+      }
     }
   }
 }
@@ -408,6 +437,36 @@ int qkd_plan_create(const qk_plan_desc* d, int device, qk_plan** out) {
     return QKD_ENOMEM;
   }
   p->spin = qkd::spin_plan_create(d, &p->bytes);
+  if (!p->spin) p->spin = qkd::gen_plan_create(d, &p->bytes);
+  // Operators on the generic kernel with a real diagonal keep it as a
+  // vector (read once per row instead of walking the diagonal terms).
+  bool diag_real = d->has_diag != 0;
+  if (diag_real)
+    for (uint32_t q = d->groups[0].first; q < d->groups[0].first + d->groups[0].count; ++q)
+      if (d->terms[q].wim != 0.0) diag_real = false;
+  const bool gen = p->spin && qkd::spin_plan_is_gen(p->spin);
+  if ((!p->spin || gen) && diag_real && d->dim > 0) {
+    if (cudaMalloc(&p->diag_re, d->dim * 8) == cudaSuccess) {
+      p->bytes += d->dim * 8;
+      qkd::SpinHandle* keep = p->spin;
+      p->spin = nullptr;  // the diagonal kernel walks the terms; the plan is not complete yet
+      const int rc = qkd_diagonal(p, QK_F64, p->diag_re, nullptr);
+      p->spin = keep;
+      if (rc != QKD_OK || cudaStreamSynchronize(nullptr) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cudaFree(p->diag_re);
+        p->diag_re = nullptr;
+      }
+    } else {
+      (void)cudaGetLastError();
+      p->diag_re = nullptr;
+    }
+  }
+  if (gen && (!p->diag_re || qkd::spin_plan_set_diag(p->spin, p->diag_re) != QKD_OK)) {
+    // without its diagonal vector the two-part kernel cannot run: generic kernel
+    qkd::spin_plan_destroy(p->spin);
+    p->spin = nullptr;
+  }
   *out = p;
   return QKD_OK;
 }
@@ -418,11 +477,15 @@ int qkd_set_kernel_policy(int policy) {
   return QKD_OK;
 }
 
-int qkd_plan_kernel(const qk_plan* p) { return (p && p->spin && g_kernel_policy == 0) ? 1 : 0; }
+int qkd_plan_kernel(const qk_plan* p) {
+  if (!p || !p->spin || g_kernel_policy != 0) return 0;
+  return qkd::spin_plan_is_gen(p->spin) ? 2 : 1;
+}
 
 int qkd_plan_destroy(qk_plan* p) {
   if (!p) return QKD_OK;
   qkd::spin_plan_destroy(p->spin);
+  cudaFree(p->diag_re);
   cudaFree(p->A); cudaFree(p->B); cudaFree(p->llist);
   cudaFree(p->terms); cudaFree(p->groups); cudaFree(p->tiles);
   delete p;

@@ -86,6 +86,11 @@ struct SpinPlan {
   int ncls, cpad, ncombo;
   uint32_t zero_slot, nllist;
   bool rows_ok;
+  // two-part operators (any factorisable group, e.g. Hubbard and t-J hops)
+  bool gen;
+  uint32_t nblocks;       // block records (all 2^H, or only the non-empty ones)
+  const uint32_t* crk32;  // [pos][ncross]: rank | lv0 << 24 | ls0 << 25 | lv1 << 26 | ls1 << 27
+  const double* diag_full;  // two-part operators: the diagonal per row, summed in term order
 };
 
 namespace {
@@ -860,7 +865,7 @@ __device__ __forceinline__ RowBlock load_block(const RowBlock* p) {
   return r;
 }
 
-template <int DT, bool DOT>
+template <int DT, bool DOT, bool GEN>
 __global__ void __launch_bounds__(kRowThreads, DT == QK_C128 ? KRB_C128 : 4)
 k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
                double* partials, unsigned* ticket, double* dot_out) {
@@ -876,7 +881,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
   for (int i = threadIdx.x; i < kRowCoef; i += blockDim.x) s_coef[i] = R(p.coef[i]);
   if (threadIdx.x < kRowCls) s_lc[threadIdx.x] = R(p.lcls[threadIdx.x]);
   if (threadIdx.x == 0) szero(sx[p.zero_slot]);
-  const uint32_t nA = 1u << p.H;
+  const uint32_t nA = p.nblocks;
   const uint32_t nll = p.nllist;
   const int ncross = p.ncross, ncls = p.ncls;
   const uint32_t cw = uint32_t(p.cpad) >> 1;  // crossing words (two u16 each) per row
@@ -894,19 +899,12 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
     if (threadIdx.x < nh + uint32_t(ncross)) {
       const uint2 e = __ldg(p.bent + cur.ebeg + threadIdx.x);
       s_eb[threadIdx.x] = e.x;
-      s_ec[threadIdx.x] = s_coef[e.y & 0xFFFFu];
-      if (threadIdx.x >= nh) s_ebit[threadIdx.x - nh] = e.y >> 16;
+      // crossing entries of two-part operators keep their raw flags
+      s_ec[threadIdx.x] = (GEN && threadIdx.x >= nh) ? R(0) : s_coef[e.y & 0xFFFFu];
+      if (threadIdx.x >= nh) s_ebit[threadIdx.x - nh] = GEN ? e.y : e.y >> 16;
 #ifndef QKD_NO_HIGH_PREFETCH
       else  // high partner rows of the first row chunks into L2
         l2_prefetch(x, sizeof(E), e.x, min(size, uint32_t(QKD_PF_AHEAD) * kRowBatch<DT> * kRowThreads));
-#endif
-#ifdef QKD_PF_CROSS
-      if (threadIdx.x >= nh) {  // crossing partner block, whole
-        const uint32_t q = threadIdx.x - nh;
-        const uint32_t hp = h ^ p.cross_hi[q];
-        const uint32_t pb = __ldg(p.A32 + hp), pe = hp + 1 < nA ? __ldg(p.A32 + hp + 1) : uint32_t(p.dim);
-        l2_prefetch(x, sizeof(E), pb, pe - pb);
-      }
 #endif
     }
     __syncthreads();
@@ -925,11 +923,12 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
     }
     uint32_t cb[2], cbit[2];
     R cc[2];
+    const int ncr = GEN ? 0 : ncross;  // crossing bonds of the exchange form (two-part: below)
     #pragma unroll
     for (int u = 0; u < 2; ++u) {
-      cb[u] = u < ncross ? s_eb[nh + u] : 0u;
-      cbit[u] = u < ncross ? s_ebit[u] : 2u;  // 2: never equal to a low bit, never valid
-      cc[u] = u < ncross ? s_ec[nh + u] : R(0);
+      cb[u] = u < ncr ? s_eb[nh + u] : 0u;
+      cbit[u] = u < ncr ? s_ebit[u] : 2u;  // 2: never equal to a low bit, never valid
+      cc[u] = u < ncr ? s_ec[nh + u] : R(0);
     }
     constexpr int K = kRowBatch<DT>;
     for (uint32_t r0 = threadIdx.x; r0 < size; r0 += K * kRowThreads) {
@@ -956,7 +955,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
         pos[k] = cur.lst + (ok[k] ? rk[k] : 0u);
         rec[k] = __ldg(p.rrec + pos[k]);
         dt[k] = __ldg(dcol + pos[k]);
-        two[k] = ncross ? __ldg(ckw + pos[k] * cw) : 0u;
+        two[k] = ncr ? __ldg(ckw + pos[k] * cw) : 0u;
       }
       R ar[K], ai[K];
       #pragma unroll
@@ -996,7 +995,31 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
           ar[k] += s_ec[e] * vr;
           if (T::cplx) ai[k] += s_ec[e] * vi;
         }
-        for (int q = 2; q < ncross; q += 2) {
+        if constexpr (GEN) {
+          // two-part crossing groups: up to two terms, each valid when its
+          // low condition (row table) and high condition (block entry) hold,
+          // with the sign of both parts' Jordan-Wigner / Sz parities
+          for (int q = 0; q < ncross; ++q) {
+            const uint32_t ent = __ldg(p.crk32 + pos[k] * uint32_t(ncross) + q);
+            const uint32_t bf = s_ebit[q];
+            R c = R(0);
+            if ((ent >> 24) & (bf >> 16) & 1u) {
+              const R w = s_coef[bf & 0xFFu];
+              c += (((ent >> 25) ^ (bf >> 17)) & 1u) ? -w : w;
+            }
+            if ((ent >> 26) & (bf >> 18) & 1u) {
+              const R w = s_coef[(bf >> 8) & 0xFFu];
+              c += (((ent >> 27) ^ (bf >> 19)) & 1u) ? -w : w;
+            }
+            if (c != R(0)) {
+              R vr, vi;
+              T::ld(x, s_eb[nh + q] + (ent & 0xFFFFFFu), vr, vi);
+              ar[k] += c * vr;
+              if (T::cplx) ai[k] += c * vi;
+            }
+          }
+        }
+        for (int q = 2; q < ncr; q += 2) {
           const uint32_t tw = __ldg(ckw + pos[k] * cw + (q >> 1));
           #pragma unroll
           for (int u = 0; u < 2; ++u) {
@@ -1027,7 +1050,8 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
         }
         R x0r, x0i;
         sld(sx, r, x0r, x0i);
-        const R d = dh + R(dt[k]);
+        // two-part operators read the full diagonal (summed in term order)
+        const R d = GEN ? R(__ldg(p.diag_full + base + r)) : dh + R(dt[k]);
         ar[k] += d * x0r;
         if (T::cplx) ai[k] += d * x0i;
         T::st(y, base + r, ar[k], ai[k]);
@@ -1051,7 +1075,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
 struct SpinHandle {
   SpinPlan host;
   SpinPlan* dev = nullptr;
-  void* bufs[17] = {};
+  void* bufs[20] = {};
   bool lean = false;  // every bond conserves the charge: warp-tile kernel
 };
 
@@ -1289,6 +1313,7 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
         h.coef[h.ncoef] = c;
         return uint32_t(h.ncoef++);
       };
+      h.nblocks = uint32_t(d->nA);
       brec.resize(d->nA);
       for (uint64_t hh = 0; hh < d->nA; ++hh) {
         RowBlock& b = brec[hh];
@@ -1368,6 +1393,201 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.dtab = static_cast<const double*>(out->bufs[14]);
     h.brec = static_cast<const RowBlock*>(out->bufs[15]);
     h.bent = static_cast<const uint2*>(out->bufs[16]);
+    out->host = h;
+    ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
+         cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (ok) *dev_bytes += sizeof(SpinPlan);
+  }
+  if (!ok) {
+    (void)cudaGetLastError();
+    spin_plan_destroy(out);
+    return nullptr;
+  }
+  return out;
+}
+
+// Two-part operators.  Every compiled term factorises over the sector
+// split: its condition (s & cmask) == cval and its sign parity
+// popcount(s & smask) are a condition and a parity of the low part times a
+// condition and a parity of the high part.  Groups whose flip and terms lie
+// in the low part become the class tables of the row kernel (their
+// coefficient is a function of l), groups inside the high part become
+// block entries (a function of h), and groups whose flip spans both parts
+// (at most two terms) keep per-row low flags and per-block high flags that
+// the kernel combines.  The diagonal is read from the plan's diagonal
+// vector (summed in term order, as the reference sums it), set with
+// spin_plan_set_diag.  This covers the Hubbard and t-J hops with their
+// Jordan-Wigner signs, U Nupdn, the t-J spin-flip and density terms, and
+// the spin models.
+SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
+  if (!d->all_real || d->dim == 0 || d->dim >= (1ull << 32) || d->nterms == 0) return nullptr;
+  const int L = d->L, H = d->nbits - d->L;
+  if (L < 1 || L > 24 || H < 0 || H > 24 || d->nbits > 48) return nullptr;
+  const uint64_t lowbits = (1ull << L) - 1;
+  auto lo = [&](uint64_t v) { return uint32_t(v & lowbits); };
+  auto hi = [&](uint64_t v) { return uint32_t(v >> L); };
+  auto par = [](uint32_t v) { return uint32_t(__builtin_popcount(v) & 1); };
+  SpinPlan h{};
+  h.L = L; h.H = H; h.dim = d->dim; h.gen = true;
+  for (uint32_t k = 0; k < d->nkeys; ++k) h.max_block = std::max(h.max_block, d->key_off[k + 1] - d->key_off[k]);
+  if (h.max_block >= 0xFFFFu || size_t(h.max_block + 1) * 16 > 200 * 1024) return nullptr;
+  auto coef_index = [&](double c) -> int {
+    for (int k = 0; k < h.ncoef; ++k) if (h.coef[k] == c) return k;
+    if (h.ncoef >= kRowCoef) return -1;
+    h.coef[h.ncoef] = c;
+    return h.ncoef++;
+  };
+  // classify the groups
+  std::vector<uint32_t> lowg, highg, crossg;
+  uint32_t g0 = 0;
+  if (d->has_diag) g0 = 1;  // the diagonal comes from the plan's diagonal vector
+  for (uint32_t gi = g0; gi < d->ngroups; ++gi) {
+    const qk_group_t& g = d->groups[gi];
+    if (g.check) return nullptr;  // targets must stay in the sector
+    uint64_t m = g.flip;
+    for (uint32_t q = g.first; q < g.first + g.count; ++q) m |= d->terms[q].cmask | d->terms[q].smask;
+    if ((g.flip >> L) == 0 && (m >> L) == 0) lowg.push_back(gi);
+    else if ((g.flip & lowbits) == 0 && (m & lowbits) == 0) highg.push_back(gi);
+    else if ((g.flip & lowbits) != 0 && (g.flip >> L) != 0 && g.count <= 2) crossg.push_back(gi);
+    else return nullptr;
+  }
+  h.ncross = int(crossg.size());
+  if (h.ncross > kRowCross || highg.size() + crossg.size() > size_t(kRowEnt)) return nullptr;
+  auto group_value = [&](const qk_group_t& g, uint32_t part, bool low) {
+    double c = 0.0;
+    for (uint32_t q = g.first; q < g.first + g.count; ++q) {
+      const qk_term_t& t = d->terms[q];
+      const uint32_t cm = low ? lo(t.cmask) : hi(t.cmask), cv = low ? lo(t.cval) : hi(t.cval);
+      const uint32_t sm = low ? lo(t.smask) : hi(t.smask);
+      if ((part & cm) == cv) c += par(part & sm) ? -t.wre : t.wre;
+    }
+    return c;
+  };
+  // class tables over llist positions
+  const uint64_t nll = d->nllist;
+  h.nllist = uint32_t(nll);
+  h.zero_slot = h.max_block;
+  h.ncombo = 1;
+  std::vector<uint2> rrec(nll), lgrp;
+  std::vector<double> dtab(nll, 0.0);
+  std::vector<uint32_t> crk32(std::max<uint64_t>(1, nll * crossg.size()), 0);
+  std::vector<double> cls;
+  std::vector<uint16_t> bucket[kRowCls];
+  for (uint64_t pos = 0; pos < nll; ++pos) {
+    const uint32_t l = d->llist[pos];
+    const uint32_t key = d->B[l] >> 24;
+    for (auto& b : bucket) b.clear();
+    for (uint32_t gi : lowg) {
+      const qk_group_t& g = d->groups[gi];
+      const double c = group_value(g, l, true);
+      if (c == 0.0) continue;
+      const uint32_t lt = l ^ lo(g.flip);
+      if ((d->B[lt] >> 24) != key) return nullptr;  // low groups must keep the low part's charges
+      int ci = -1;
+      for (int k = 0; k < int(cls.size()); ++k) if (cls[k] == c) ci = k;
+      if (ci < 0) {
+        if (int(cls.size()) == kRowCls) return nullptr;
+        cls.push_back(c);
+        ci = int(cls.size()) - 1;
+      }
+      bucket[ci].push_back(uint16_t(d->B[lt] & 0xFFFFu));
+    }
+    rrec[pos].x = uint32_t(lgrp.size());
+    uint32_t counts = 0;
+    for (int c = 0; c < kRowCls; ++c) {
+      auto& b = bucket[c];
+      if (b.empty()) continue;
+      while (b.size() % 4) b.push_back(uint16_t(h.zero_slot));
+      const uint32_t ng = uint32_t(b.size() / 4);
+      if (ng > 15) return nullptr;
+      counts |= ng << (4 * c);
+      for (uint32_t k = 0; k < ng; ++k)
+        lgrp.push_back(make_uint2(uint32_t(b[4 * k]) | (uint32_t(b[4 * k + 1]) << 16),
+                                  uint32_t(b[4 * k + 2]) | (uint32_t(b[4 * k + 3]) << 16)));
+    }
+    rrec[pos].y = counts;
+    for (size_t q = 0; q < crossg.size(); ++q) {
+      const qk_group_t& g = d->groups[crossg[q]];
+      const uint32_t lt = l ^ lo(g.flip);
+      uint32_t e = (d->B[lt] & qkb::kRankMask) & 0xFFFFFFu;
+      if ((d->B[lt] & qkb::kRankMask) > 0xFFFFFFu) return nullptr;
+      for (uint32_t k = 0; k < g.count; ++k) {
+        const qk_term_t& t = d->terms[g.first + k];
+        const uint32_t lv = (l & lo(t.cmask)) == lo(t.cval), ls = par(l & lo(t.smask));
+        e |= (lv << (24 + 2 * k)) | (ls << (25 + 2 * k));
+      }
+      crk32[pos * crossg.size() + q] = e;
+    }
+  }
+  if (lgrp.empty()) lgrp.push_back(make_uint2(0, 0));
+  h.ncls = int(cls.size());
+  for (int c = 0; c < h.ncls; ++c) h.lcls[c] = cls[c];
+  // block records of the non-empty blocks
+  std::vector<RowBlock> brec;
+  std::vector<uint2> bent;
+  for (uint64_t hh = 0; hh < d->nA; ++hh) {
+    const uint32_t need = uint32_t(d->A[hh] >> 56);
+    if (need == qkb::kEmptyBlockKey) continue;
+    const uint32_t size = d->key_off[need + 1] - d->key_off[need];
+    if (size == 0) continue;
+    RowBlock b{};
+    b.base = uint32_t(d->A[hh] & qkb::kOffsetMask);
+    b.size = size;
+    b.lst = d->key_off[need];
+    b.ebeg = uint32_t(bent.size());
+    b.dh = 0.0;
+    for (uint32_t gi : highg) {
+      const qk_group_t& g = d->groups[gi];
+      const double c = group_value(g, uint32_t(hh), false);
+      if (c == 0.0) continue;
+      const uint64_t hp = hh ^ hi(g.flip);
+      const uint32_t need2 = uint32_t(d->A[hp] >> 56);
+      if (need2 != need) return nullptr;  // high groups must keep the high part's charges
+      const int ci = coef_index(c);
+      if (ci < 0) return nullptr;
+      bent.push_back(make_uint2(uint32_t(d->A[hp] & qkb::kOffsetMask), uint32_t(ci)));
+      ++b.nh;
+    }
+    for (uint32_t gi : crossg) {
+      const qk_group_t& g = d->groups[gi];
+      const uint64_t hp = hh ^ hi(g.flip);
+      const bool pempty = uint32_t(d->A[hp] >> 56) == qkb::kEmptyBlockKey;
+      uint32_t f = 0;
+      for (uint32_t k = 0; k < g.count; ++k) {
+        const qk_term_t& t = d->terms[g.first + k];
+        const int ci = coef_index(t.wre);
+        if (ci < 0) return nullptr;
+        const uint32_t hv = !pempty && (uint32_t(hh) & hi(t.cmask)) == hi(t.cval), hs = par(uint32_t(hh) & hi(t.smask));
+        f |= (uint32_t(ci) << (8 * k)) | (hv << (16 + 2 * k)) | (hs << (17 + 2 * k));
+      }
+      bent.push_back(make_uint2(uint32_t(d->A[hp] & qkb::kOffsetMask), f));
+    }
+    brec.push_back(b);
+  }
+  if (brec.empty()) return nullptr;
+  if (bent.empty()) bent.push_back(make_uint2(0, 0));
+  h.nblocks = uint32_t(brec.size());
+  h.rows_ok = true;
+  std::vector<uint16_t> crk_dummy(2, 0);
+  auto* out = new SpinHandle;
+  out->lean = true;
+  auto up = [&](int slot, const void* src, size_t bytes) {
+    if (cudaMalloc(&out->bufs[slot], bytes) != cudaSuccess) return false;
+    *dev_bytes += bytes;
+    return cudaMemcpy(out->bufs[slot], src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+  };
+  bool ok = up(11, rrec.data(), rrec.size() * sizeof(uint2)) && up(12, lgrp.data(), lgrp.size() * sizeof(uint2)) &&
+            up(13, crk_dummy.data(), 4) && up(14, dtab.data(), dtab.size() * 8) &&
+            up(15, brec.data(), brec.size() * sizeof(RowBlock)) && up(16, bent.data(), bent.size() * sizeof(uint2)) &&
+            up(17, crk32.data(), crk32.size() * 4);
+  if (ok) {
+    h.rrec = static_cast<const uint2*>(out->bufs[11]);
+    h.lgrp = static_cast<const uint2*>(out->bufs[12]);
+    h.crk = static_cast<const uint16_t*>(out->bufs[13]);
+    h.dtab = static_cast<const double*>(out->bufs[14]);
+    h.brec = static_cast<const RowBlock*>(out->bufs[15]);
+    h.bent = static_cast<const uint2*>(out->bufs[16]);
+    h.crk32 = static_cast<const uint32_t*>(out->bufs[17]);
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1537,22 +1757,23 @@ int spin_apply_owner(const SpinHandle* h, qk_dtype t, const void* x, void* y, cu
 
 int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
                     qk_workspace* w, double* dot_out) {
-  if (!h->host.rows_ok) return QKD_EINVAL;
+  if (!h->host.rows_ok || (h->host.gen && !h->host.diag_full)) return QKD_EINVAL;
   const size_t es = (t == QK_C128) ? 16 : (t == QK_F32 ? 4 : 8);
   const size_t smem = es * (h->host.max_block + 1);  // staged block and the zero slot
   if (smem > 200 * 1024) return QKD_EINVAL;
-#define QKD_ROWS_LAUNCH(DT)                                                                               \
+#define QKD_ROWS_LAUNCH1(DT, G)                                                                           \
   {                                                                                                       \
-    auto kd = k_hx_spin_rows<DT, true>;                                                                   \
-    auto kn = k_hx_spin_rows<DT, false>;                                                                  \
+    auto kd = k_hx_spin_rows<DT, true, G>;                                                                \
+    auto kn = k_hx_spin_rows<DT, false, G>;                                                               \
     if (cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||  \
         cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)    \
       return QKD_EINVAL;                                                                                  \
-    const unsigned cap = 1u << h->host.H;                                                                 \
+    const unsigned cap = std::max(1u, h->host.nblocks);                                                   \
     if (dot_out) kd<<<resident_grid(kd, kRowThreads, smem, std::min<unsigned>(cap, kMaxG)), kRowThreads, smem, s>>>( \
         h->dev, x, y, w->partials, w->ticket, dot_out);                                                   \
     else kn<<<resident_grid(kn, kRowThreads, smem, cap), kRowThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr); \
   }
+#define QKD_ROWS_LAUNCH(DT) { if (h->host.gen) QKD_ROWS_LAUNCH1(DT, true) else QKD_ROWS_LAUNCH1(DT, false) }
   switch (t) {
     case QK_C128: QKD_ROWS_LAUNCH(QK_C128); break;
     case QK_C64: QKD_ROWS_LAUNCH(QK_C64); break;
@@ -1561,6 +1782,7 @@ int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
     default: return QKD_EINVAL;
   }
 #undef QKD_ROWS_LAUNCH
+#undef QKD_ROWS_LAUNCH1
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
@@ -1568,8 +1790,19 @@ int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
 // 0 block tiles, 1 warp tiles, 2 batched, 3 lists, 4 staged, 5 block owner, 6 rows
 static int g_spin_variant = 6;
 
+bool spin_plan_is_gen(const SpinHandle* h) { return h && h->host.gen; }
+
+// Two-part plans read the operator's diagonal vector (device, dim doubles);
+// without one they cannot run (spin_apply_rows reports QKD_EINVAL).
+int spin_plan_set_diag(SpinHandle* h, const double* diag) {
+  if (!h) return QKD_EINVAL;
+  h->host.diag_full = diag;
+  return cudaMemcpy(h->dev, &h->host, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess ? QKD_OK : QKD_ECUDA;
+}
+
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out) {
+  if (h->host.gen) return spin_apply_rows(h, t, x, y, s, w, dot_out);
   if (h->lean && g_spin_variant == 6) {
     const int rc = spin_apply_rows(h, t, x, y, s, w, dot_out);
     if (rc != QKD_EINVAL) return rc;

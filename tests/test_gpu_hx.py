@@ -189,3 +189,25 @@ def test_multi_dot_device():
         got = out[0::2] + 1j * out[1::2]
         want = np.array([torch.vdot(v.to(torch.complex128), x.to(torch.complex128)).item() for v in V])
         assert np.abs(got - want).max() <= tol * np.abs(want).max() * 10 + 1e-9
+
+
+@pytest.mark.parametrize("kind,N,sec,terms", [
+    ("hubbard", 9, dict(use_nup=1, nup=4, use_ndn=1, ndn=5), O.hubbard_square(3, 3, 1.0, 4.0)),
+    ("tj", 12, dict(use_nup=1, nup=5, use_ndn=1, ndn=5), O.tj_chain(12, 1.0, 0.4)),
+    ("fermion", 14, dict(use_n=1, n=7), [(-1.0, [("C", (i + 1) % 14), ("Cdag", i)]) for i in range(14)] +
+     [(-1.0, [("C", i), ("Cdag", (i + 1) % 14)]) for i in range(14)] + [(0.3, [("N", i), ("N", (i + 1) % 14)]) for i in range(14)]),
+])
+def test_two_part_kernel_matches_generic(kind, N, sec, terms):
+    H = ham(kind, N, sec, terms)
+    assert H.kernel == "two-part"
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(H.dimension) + 1j * rng.standard_normal(H.dimension)
+    y = H.apply(x)
+    qk.set_kernel_policy("generic")
+    try:
+        yg = H.apply(x)
+    finally:
+        qk.set_kernel_policy("auto")
+    assert rel(y, yg) < 1e-13
+    ref = O.port().hamiltonian(kind, N, sec, terms)
+    assert rel(y, ref.apply(x)) < 1e-13
