@@ -21,6 +21,8 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes);
 SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes);
 bool spin_plan_is_gen(const SpinHandle* h);
 int spin_plan_set_diag(SpinHandle* h, const double* diag);
+int spin_apply_block(const SpinHandle* h, qk_dtype t, int R, int lpr, const void* X, void* Y, double* dots,
+                     cudaStream_t s, qk_workspace* w);
 void spin_plan_destroy(SpinHandle* h);
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out);
@@ -535,6 +537,10 @@ int qkd_apply_rows(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lan
   if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
   if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
   const int lpr = lanes_per_row ? lanes_per_row : (p->rows_lpr[t][r_index(R)] ? p->rows_lpr[t][r_index(R)] : 32);
+  if (p->spin && g_kernel_policy == 0) {  // the row-kernel tables where the operator has them
+    const int rc = qkd::spin_apply_block(p->spin, t, R, lpr, X, Y, dots, s, w);
+    if (rc != QKD_EINVAL) return rc;
+  }
   if (p->all_real) { QKD_DISPATCH(t, return launch_block_shape<DT, false>(p, w, R, lpr, X, Y, diag, dots, s)); }
   if (t == QK_C128) return launch_block_shape<QK_C128, true>(p, w, R, lpr, X, Y, diag, dots, s);
   if (t == QK_C64) return launch_block_shape<QK_C64, true>(p, w, R, lpr, X, Y, diag, dots, s);

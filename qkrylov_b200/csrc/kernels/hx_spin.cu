@@ -91,6 +91,8 @@ struct SpinPlan {
   uint32_t nblocks;       // block records (all 2^H, or only the non-empty ones)
   const uint32_t* crk32;  // [pos][ncross]: rank | lv0 << 24 | ls0 << 25 | lv1 << 26 | ls1 << 27
   const double* diag_full;  // two-part operators: the diagonal per row, summed in term order
+  const uint4* btiles;      // block apply: (block record, first row, rows) runs of <= 256 rows
+  uint32_t nbtiles;
 };
 
 namespace {
@@ -1070,6 +1072,154 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
   }
 }
 
+// Block form of the row kernel for R vectors stored row-interleaved
+// (element (i, r) at i*R + r): LPR lanes share a row and each covers VPL
+// consecutive vectors with one vector load per target, so the class
+// tables, block entries and crossing flags of a row are read once for all
+// R vectors.  Same tables, same sums as k_hx_spin_rows; column dots
+// <X_r, Y_r> reduced in a fixed order.
+template <class E, int VPL>
+struct alignas(sizeof(E) * VPL) BlkPack { E v[VPL]; };
+
+template <int DT, bool GEN, int LPR, int VPL>
+__global__ void __launch_bounds__(256)
+k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, void* __restrict__ Y,
+                double* partials, unsigned* ticket, double* dots) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  using E = typename T::E;
+  using Pack = BlkPack<E, VPL>;
+  constexpr int RV = LPR * VPL, RPW = 32 / LPR;
+  const SpinPlan& p = *pp;
+  __shared__ R s_coef[kRowCoef], s_lc[kRowCls], s_ec[kRowEnt];
+  __shared__ uint32_t s_eb[kRowEnt], s_ebit[kRowCross];
+  for (int i = threadIdx.x; i < kRowCoef; i += blockDim.x) s_coef[i] = R(p.coef[i]);
+  if (threadIdx.x < kRowCls) s_lc[threadIdx.x] = R(p.lcls[threadIdx.x]);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane / LPR, l = lane % LPR;
+  const E* __restrict__ Xe = reinterpret_cast<const E*>(X);
+  E* __restrict__ Ye = reinterpret_cast<E*>(Y);
+  const uint32_t nll = p.nllist, zs = p.zero_slot;
+  const int ncross = p.ncross, ncls = p.ncls;
+  const uint32_t cpad = uint32_t(p.cpad);
+  double dr[VPL], di[VPL];
+  #pragma unroll
+  for (int v = 0; v < VPL; ++v) { dr[v] = 0.0; di[v] = 0.0; }
+  auto ldrow = [&](uint32_t row, R* re, R* im) {
+    const Pack pk = *reinterpret_cast<const Pack*>(Xe + size_t(row) * RV + l * VPL);
+    #pragma unroll
+    for (int v = 0; v < VPL; ++v) sld(pk.v, v, re[v], im[v]);
+  };
+  // Tiles of <= 256 rows in block order: the CTAs running at the same time
+  // work on a few neighbouring blocks, whose rows (the low-bond targets)
+  // then stay in L2 while they are gathered.
+  for (uint32_t ti = blockIdx.x; ti < p.nbtiles; ti += gridDim.x) {
+    const uint4 tile = __ldg(p.btiles + ti);
+    const RowBlock cur = load_block(p.brec + tile.x);
+    const uint32_t base = cur.base, size = tile.y + tile.z, nh = cur.nh;
+    __syncthreads();
+    if (threadIdx.x < nh + uint32_t(ncross)) {
+      const uint2 e = __ldg(p.bent + cur.ebeg + threadIdx.x);
+      s_eb[threadIdx.x] = e.x;
+      s_ec[threadIdx.x] = (GEN && threadIdx.x >= nh) ? R(0) : s_coef[e.y & 0xFFFFu];
+      if (threadIdx.x >= nh) s_ebit[threadIdx.x - nh] = GEN ? e.y : e.y >> 16;
+    }
+    __syncthreads();
+    const double* __restrict__ dcol = p.dtab + size_t(cur.combo) * nll;
+    for (uint32_t r = tile.y + warp * RPW + sub; r < size; r += (256 / 32) * RPW) {
+      const uint32_t pos = cur.lst + r, row = base + r;
+      R x0r[VPL], x0i[VPL], ar[VPL], ai[VPL];
+      ldrow(row, x0r, x0i);
+      const R d = GEN ? R(__ldg(p.diag_full + row)) : R(cur.dh) + R(__ldg(dcol + pos));
+      #pragma unroll
+      for (int v = 0; v < VPL; ++v) { ar[v] = d * x0r[v]; ai[v] = T::cplx ? d * x0i[v] : R(0); }
+      // low bonds: the row's target groups, by coefficient class
+      const uint2 rec = __ldg(p.rrec + pos);
+      const uint2* __restrict__ g = p.lgrp + rec.x;
+      for (int c = 0; c < ncls; ++c) {
+        const uint32_t ng = (rec.y >> (4 * c)) & 0xFu;
+        R sr[VPL], si[VPL];
+        #pragma unroll
+        for (int v = 0; v < VPL; ++v) { sr[v] = R(0); si[v] = R(0); }
+        for (uint32_t j = 0; j < ng; ++j) {
+          const uint2 q = __ldg(g + j);
+          const uint32_t kk[4] = {q.x & 0xFFFFu, q.x >> 16, q.y & 0xFFFFu, q.y >> 16};
+          #pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (kk[u] == zs) continue;  // padding of the group
+            R vr[VPL], vi[VPL];
+            ldrow(base + kk[u], vr, vi);
+            #pragma unroll
+            for (int v = 0; v < VPL; ++v) { sr[v] += vr[v]; if (T::cplx) si[v] += vi[v]; }
+          }
+        }
+        g += ng;
+        #pragma unroll
+        for (int v = 0; v < VPL; ++v) { ar[v] += s_lc[c] * sr[v]; if (T::cplx) ai[v] += s_lc[c] * si[v]; }
+      }
+      // high bonds: the same row of a partner block
+      for (uint32_t e = 0; e < nh; ++e) {
+        R vr[VPL], vi[VPL];
+        ldrow(s_eb[e] + r, vr, vi);
+        const R c = s_ec[e];
+        #pragma unroll
+        for (int v = 0; v < VPL; ++v) { ar[v] += c * vr[v]; if (T::cplx) ai[v] += c * vi[v]; }
+      }
+      // crossing bonds
+      for (int q = 0; q < ncross; ++q) {
+        R c = R(0);
+        uint32_t rank = 0;
+        if constexpr (GEN) {
+          const uint32_t ent = __ldg(p.crk32 + size_t(pos) * uint32_t(ncross) + q);
+          const uint32_t bf = s_ebit[q];
+          if ((ent >> 24) & (bf >> 16) & 1u) {
+            const R w = s_coef[bf & 0xFFu];
+            c += (((ent >> 25) ^ (bf >> 17)) & 1u) ? -w : w;
+          }
+          if ((ent >> 26) & (bf >> 18) & 1u) {
+            const R w = s_coef[(bf >> 8) & 0xFFu];
+            c += (((ent >> 27) ^ (bf >> 19)) & 1u) ? -w : w;
+          }
+          rank = ent & 0xFFFFFFu;
+        } else {
+          const uint32_t ent = __ldg(p.crk + size_t(pos) * cpad + q);
+          if ((ent >> 15) != s_ebit[q]) c = s_ec[nh + q];
+          rank = ent & 0x7FFFu;
+        }
+        if (c != R(0)) {
+          R vr[VPL], vi[VPL];
+          ldrow(s_eb[nh + q] + rank, vr, vi);
+          #pragma unroll
+          for (int v = 0; v < VPL; ++v) { ar[v] += c * vr[v]; if (T::cplx) ai[v] += c * vi[v]; }
+        }
+      }
+      Pack yv;
+      #pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        T::st(yv.v, v, ar[v], ai[v]);
+        dr[v] += double(x0r[v]) * double(ar[v]) + double(x0i[v]) * double(ai[v]);
+        di[v] += double(x0r[v]) * double(ai[v]) - double(x0i[v]) * double(ar[v]);
+      }
+      *reinterpret_cast<Pack*>(Ye + size_t(row) * RV + l * VPL) = yv;
+    }
+  }
+  __shared__ double red[2 * 256];
+  for (int v = 0; v < VPL; ++v) {
+    __syncthreads();
+    red[2 * threadIdx.x] = dr[v];
+    red[2 * threadIdx.x + 1] = di[v];
+    __syncthreads();
+    if (threadIdx.x < LPR) {
+      double sr = 0.0, si = 0.0;
+      for (int t = threadIdx.x; t < 256; t += LPR) { sr += red[2 * t]; si += red[2 * t + 1]; }
+      const int c = threadIdx.x * VPL + v;
+      partials[(size_t(c) * gridDim.x + blockIdx.x) * 2] = sr;
+      partials[(size_t(c) * gridDim.x + blockIdx.x) * 2 + 1] = si;
+    }
+  }
+  grid_finish(partials, ticket, RV, dots);
+}
+
 }  // namespace
 
 struct SpinHandle {
@@ -1084,6 +1234,15 @@ void spin_plan_destroy(SpinHandle* h) {
   for (void* b : h->bufs) cudaFree(b);
   cudaFree(h->dev);
   delete h;
+}
+
+// Runs of <= 256 rows of each non-empty block record, in record order.
+static std::vector<uint4> block_tiles(const std::vector<RowBlock>& brec) {
+  std::vector<uint4> t;
+  for (uint32_t b = 0; b < uint32_t(brec.size()); ++b)
+    for (uint32_t r = 0; r < brec[b].size; r += 256) t.push_back(make_uint4(b, r, std::min(256u, brec[b].size - r), 0));
+  if (t.empty()) t.push_back(make_uint4(0, 0, 0, 0));
+  return t;
 }
 
 // Host side: decide eligibility from the compiled plan and build the
@@ -1375,6 +1534,8 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
                             up(14, dtab.data(), dtab.size() * 8) &&
                             up(15, brec.data(), brec.size() * sizeof(RowBlock)) &&
                             up(16, bent.data(), bent.size() * sizeof(uint2))));
+  const std::vector<uint4> btl = h.rows_ok ? block_tiles(brec) : std::vector<uint4>();
+  ok = ok && (!h.rows_ok || up(18, btl.data(), btl.size() * sizeof(uint4)));
   if (ok) {
     h.A32 = static_cast<const uint32_t*>(out->bufs[0]);
     h.B16 = static_cast<const uint16_t*>(out->bufs[1]);
@@ -1393,6 +1554,8 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.dtab = static_cast<const double*>(out->bufs[14]);
     h.brec = static_cast<const RowBlock*>(out->bufs[15]);
     h.bent = static_cast<const uint2*>(out->bufs[16]);
+    h.btiles = static_cast<const uint4*>(out->bufs[18]);
+    h.nbtiles = uint32_t(btl.size());
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1580,6 +1743,8 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
             up(13, crk_dummy.data(), 4) && up(14, dtab.data(), dtab.size() * 8) &&
             up(15, brec.data(), brec.size() * sizeof(RowBlock)) && up(16, bent.data(), bent.size() * sizeof(uint2)) &&
             up(17, crk32.data(), crk32.size() * 4);
+  const std::vector<uint4> tiles = block_tiles(brec);
+  ok = ok && up(18, tiles.data(), tiles.size() * sizeof(uint4));
   if (ok) {
     h.rrec = static_cast<const uint2*>(out->bufs[11]);
     h.lgrp = static_cast<const uint2*>(out->bufs[12]);
@@ -1588,6 +1753,8 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.brec = static_cast<const RowBlock*>(out->bufs[15]);
     h.bent = static_cast<const uint2*>(out->bufs[16]);
     h.crk32 = static_cast<const uint32_t*>(out->bufs[17]);
+    h.btiles = static_cast<const uint4*>(out->bufs[18]);
+    h.nbtiles = uint32_t(tiles.size());
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1789,6 +1956,35 @@ int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
 
 // 0 block tiles, 1 warp tiles, 2 batched, 3 lists, 4 staged, 5 block owner, 6 rows
 static int g_spin_variant = 6;
+
+template <int DT, bool GEN, int LPR, int VPL>
+int launch_rows_block(const SpinHandle* h, qk_workspace* w, const void* X, void* Y, double* dots, cudaStream_t s) {
+  auto k = k_hx_rows_block<DT, GEN, LPR, VPL>;
+  const unsigned g = resident_grid(k, 256, 0, std::min<unsigned>(std::max(1u, h->host.nbtiles), kMaxG));
+  k<<<g, 256, 0, s>>>(h->dev, X, Y, w->partials, w->ticket, dots ? dots : qkd_workspace_results(w));
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
+template <int DT, bool GEN>
+int rows_block_shape(const SpinHandle* h, qk_workspace* w, int R, int lpr, const void* X, void* Y, double* dots,
+                     cudaStream_t s) {
+#define QKD_RB(RR, L, V) if (R == RR && lpr == L) return launch_rows_block<DT, GEN, L, V>(h, w, X, Y, dots, s);
+  QKD_RB(32, 32, 1) QKD_RB(32, 16, 2) QKD_RB(32, 8, 4)
+  QKD_RB(64, 32, 2) QKD_RB(64, 16, 4) QKD_RB(64, 8, 8)
+  QKD_RB(128, 32, 4) QKD_RB(128, 16, 8)
+#undef QKD_RB
+  return QKD_EINVAL;
+}
+
+// Block apply with the row-kernel tables; QKD_EINVAL when this plan has none.
+int spin_apply_block(const SpinHandle* h, qk_dtype t, int R, int lpr, const void* X, void* Y, double* dots,
+                     cudaStream_t s, qk_workspace* w) {
+  if (!h || !h->host.rows_ok || !h->host.btiles || (h->host.gen && !h->host.diag_full)) return QKD_EINVAL;
+  if (h->host.gen) { QKD_DISPATCH(t, return rows_block_shape<DT, true>(h, w, R, lpr, X, Y, dots, s)); }
+  QKD_DISPATCH(t, return rows_block_shape<DT, false>(h, w, R, lpr, X, Y, dots, s));
+  return QKD_EINVAL;
+}
 
 bool spin_plan_is_gen(const SpinHandle* h) { return h && h->host.gen; }
 
