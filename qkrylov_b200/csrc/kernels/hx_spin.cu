@@ -820,18 +820,12 @@ k_hx_spin_owner(const SpinPlan* __restrict__ pp, const void* __restrict__ x, voi
 // size, and crossing ranks are in-class ranks of the partner's class; the
 // plan builder checks the high-bond sizes.
 constexpr int kRowThreads = 256;
-#ifndef KRH_C128
-#define KRH_C128 4
-#endif
-#ifndef KRB_C128
-#define KRB_C128 3
-#endif
-#ifndef QKD_PF_AHEAD
-#define QKD_PF_AHEAD 2
-#endif
+constexpr int kRowHighC128 = 4;   // complex128: high bonds held in registers (more spill)
+constexpr int kRowMinCtaC128 = 3; // complex128: CTAs per SM the registers are sized for
+constexpr int kPrefetchAhead = 2; // row chunks of high-bond partner rows prefetched into L2
 constexpr int kRowCoef = 32, kRowEnt = 48, kRowCross = 16, kRowCls = 4;
 template <int DT> constexpr int kRowBatch = DT == QK_C128 ? 1 : 4;  // rows per thread and pass
-template <int DT> constexpr int kRowHighRegs = DT == QK_C128 ? KRH_C128 : 8;  // high bonds held in registers
+template <int DT> constexpr int kRowHighRegs = DT == QK_C128 ? kRowHighC128 : 8;  // high bonds held in registers
 
 __device__ __forceinline__ void sld(const double2* s, uint32_t k, double& re, double& im) {
   const double2 v = s[k]; re = v.x; im = v.y;
@@ -868,7 +862,7 @@ __device__ __forceinline__ RowBlock load_block(const RowBlock* p) {
 }
 
 template <int DT, bool DOT, bool GEN>
-__global__ void __launch_bounds__(kRowThreads, DT == QK_C128 ? KRB_C128 : 4)
+__global__ void __launch_bounds__(kRowThreads, DT == QK_C128 ? kRowMinCtaC128 : 4)
 k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
                double* partials, unsigned* ticket, double* dot_out) {
   using T = VT<DT>;
@@ -904,10 +898,8 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       // crossing entries of two-part operators keep their raw flags
       s_ec[threadIdx.x] = (GEN && threadIdx.x >= nh) ? R(0) : s_coef[e.y & 0xFFFFu];
       if (threadIdx.x >= nh) s_ebit[threadIdx.x - nh] = GEN ? e.y : e.y >> 16;
-#ifndef QKD_NO_HIGH_PREFETCH
       else  // high partner rows of the first row chunks into L2
-        l2_prefetch(x, sizeof(E), e.x, min(size, uint32_t(QKD_PF_AHEAD) * kRowBatch<DT> * kRowThreads));
-#endif
+        l2_prefetch(x, sizeof(E), e.x, min(size, uint32_t(kPrefetchAhead) * kRowBatch<DT> * kRowThreads));
     }
     __syncthreads();
     const R dh = R(cur.dh);
@@ -934,14 +926,12 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
     }
     constexpr int K = kRowBatch<DT>;
     for (uint32_t r0 = threadIdx.x; r0 < size; r0 += K * kRowThreads) {
-#ifndef QKD_NO_HIGH_PREFETCH
       // the high partner rows two chunks ahead go to L2 while this chunk runs
       {
-        const uint32_t ahead = r0 - threadIdx.x + uint32_t(QKD_PF_AHEAD) * K * kRowThreads;
+        const uint32_t ahead = r0 - threadIdx.x + uint32_t(kPrefetchAhead) * K * kRowThreads;
         if (threadIdx.x < nh && ahead < size)
           l2_prefetch(x, sizeof(E), s_eb[threadIdx.x] + ahead, min(size - ahead, uint32_t(K * kRowThreads)));
       }
-#endif
       // K rows r0 + k * 256 per thread.  Loads that do not depend on each
       // other are issued together: row records, diagonals, crossing pairs,
       // then all high-bond values; the shared-memory low groups come last.
