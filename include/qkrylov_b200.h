@@ -276,6 +276,11 @@ void qkrylov_b200_mlp_destroy(qkrylov_b200_mlp_h net);
 size_t qkrylov_b200_mlp_num_params(qkrylov_b200_mlp_h net);
 int qkrylov_b200_mlp_get_params(qkrylov_b200_mlp_h net, float* out);
 int qkrylov_b200_mlp_set_params(qkrylov_b200_mlp_h net, const float* in);
+/* Inference (qkrylov_b200_mlp_start_vector, qkrylov_b200_lanczos_warm) on
+ * the tensor cores (on != 0, the default: tcgen05 MMAs with BF16 weights
+ * and activations, FP32 accumulation in tensor memory) or on the CUDA cores
+ * (FP32 activations, as in training). */
+int qkrylov_b200_mlp_set_tensor_cores(qkrylov_b200_mlp_h net, int on);
 /* A real ground state psi (dimension() doubles, host) at coupling j2. */
 int qkrylov_b200_mlp_add_target(qkrylov_b200_mlp_h net, double j2, const double* psi);
 /* `steps` Adam steps (learning rate lr with cosine decay to lr/20) on

@@ -57,15 +57,17 @@ def inputs(states, j2, nsites):
     return X
 
 
-def forward(p, X, nsites, round_bf16=True):
+def forward(p, X, nsites, round_bf16=True, act_bf16=False):
+    """act_bf16: round the inputs of the two hidden-layer products to BF16,
+    as the tensor-core inference kernel does (it keeps FP32 accumulation)."""
     W1, W2, W3, b1, b2, b3 = split(np.asarray(p, np.float32), nsites)
     if round_bf16:
         W1, W2, W3 = bf16(W1), bf16(W2), bf16(W3)
     W1, W2, W3 = (np.asarray(w, np.float64) for w in (W1, W2, W3))
     b1, b2, b3 = (np.asarray(b, np.float64) for b in (b1, b2, b3))
-    Z1 = X @ W1.T + b1
+    Z1 = (bf16(X) if act_bf16 else X) @ W1.T + b1
     H1 = gelu(Z1)
-    Z2 = H1 @ W2.T + b2
+    Z2 = (bf16(H1) if act_bf16 else H1) @ W2.T + b2
     H2 = gelu(Z2)
     O = H2 @ W3.T + b3
     return dict(W1=W1, W2=W2, W3=W3, Z1=Z1, H1=H1, Z2=Z2, H2=H2, O=O)
@@ -101,9 +103,9 @@ def marshall_mask(nsites):
     return sum(1 << b for b in range(1, nsites, 2))
 
 
-def start_vector(p, states, j2, nsites):
+def start_vector(p, states, j2, nsites, act_bf16=False):
     X = inputs(states, j2, nsites)
-    O = forward(p, X, nsites)["O"]
+    O = forward(p, X, nsites, act_bf16=act_bf16)["O"]
     s = np.asarray(states, dtype=np.uint64)
     mm = np.uint64(marshall_mask(nsites))
     par = np.array([bin(int(v)).count("1") & 1 for v in (s & mm)])

@@ -631,6 +631,11 @@ class WarmStartMLP:
                                             loss.ctypes.data), "mlp train")
         return loss[:steps]
 
+    def set_tensor_cores(self, on: bool = True):
+        """Inference on the tensor cores (tcgen05, BF16 activations; default)
+        or on the CUDA cores (FP32 activations, as in training)."""
+        _check(lib().qkrylov_b200_mlp_set_tensor_cores(self._h, int(bool(on))), "mlp tensor cores")
+
     def start_vector(self, j2: float) -> np.ndarray:
         out = np.zeros(self._basis.size, np.float32)
         _check(lib().qkrylov_b200_mlp_start_vector(self._h, float(j2), out.ctypes.data, 0), "mlp start vector")

@@ -106,6 +106,7 @@ PROTOTYPES = {
     "qkrylov_b200_mlp_get_params": (_i, [_vp, _vp]),
     "qkrylov_b200_mlp_set_params": (_i, [_vp, _vp]),
     "qkrylov_b200_mlp_add_target": (_i, [_vp, _d, _vp]),
+    "qkrylov_b200_mlp_set_tensor_cores": (_i, [_vp, _i]),
     "qkrylov_b200_mlp_train": (_i, [_vp, _i, _i, _d, _u64, _d, _vp]),
     "qkrylov_b200_mlp_start_vector": (_i, [_vp, _d, _vp, _i]),
     "qkrylov_b200_mlp_loss_grad": (_i, [_vp, _i, _vp, _vp, _vp, _d, _vp, _vp]),

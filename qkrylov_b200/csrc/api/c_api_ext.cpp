@@ -389,6 +389,12 @@ int qkrylov_b200_mlp_set_params(qkrylov_b200_mlp_h h, const float* in) {
   });
 }
 
+int qkrylov_b200_mlp_set_tensor_cores(qkrylov_b200_mlp_h h, int on) {
+  if (!h) return QKRYLOV_ERROR_INVALID_ARG;
+  h->net->set_tensor_cores(on != 0);
+  return QKRYLOV_SUCCESS;
+}
+
 int qkrylov_b200_mlp_add_target(qkrylov_b200_mlp_h h, double j2, const double* psi) {
   if (!h || !psi) return QKRYLOV_ERROR_INVALID_ARG;
   return guarded([&] {

@@ -24,6 +24,9 @@ int qkd_cdf(qk_dtype t, size_t n, const void* psi, double* cdf, double* bsum, cu
 int qkd_sample(qk_dtype t, int m, size_t n, const double* cdf, const void* psi, const uint64_t* states,
                uint64_t marshall, double log_max, uint64_t seed, uint32_t* idx, float* tgt, cudaStream_t s);
 int qkd_max_f32(qk_workspace* w, size_t n, const float* x, int stride, float* out, cudaStream_t s);
+int qkd_mlp_forward_tc(int n, int nsites, const uint64_t* states, float j2, const void* w1, const void* w2,
+                       const void* w3, const float* b1, const float* b2, const float* b3, float* out, int* err,
+                       cudaStream_t s);
 }
 
 namespace qkb {
@@ -86,6 +89,7 @@ WarmStartNet::~WarmStartNet() {
   dfree(states_);
   dfree(X_); dfree(Z1_); dfree(H1_); dfree(Z2_); dfree(H2_); dfree(O_); dfree(dO_); dfree(dH_); dfree(dZ_);
   dfree(tgt_); dfree(j2_); dfree(idx_);
+  dfree(err_);
 }
 
 std::vector<float> WarmStartNet::params() const {
@@ -201,10 +205,22 @@ void WarmStartNet::start_vector(double j2, float* out) {
   ensure_batch(kChunk);
   DevVec O(2 * dim_, QK_F32, dev_, false);
   float* Oall = static_cast<float*>(O.data());
-  for (uint64_t r0 = 0; r0 < dim_; r0 += kChunk) {
-    const int n = int(std::min<uint64_t>(kChunk, dim_ - r0));
-    forward(n, nullptr, states_ + r0, nullptr, float(j2));
-    cuda_check(cudaMemcpyAsync(Oall + 2 * r0, O_, size_t(n) * 2 * 4, cudaMemcpyDeviceToDevice, c.stream), "copy");
+  if (tc_) {
+    if (!err_) dalloc(&err_, 1);
+    cuda_check(cudaMemsetAsync(err_, 0, sizeof(int), c.stream), "memset");
+    const auto* pb = static_cast<const uint16_t*>(pb_);
+    qkd_check(qkd_mlp_forward_tc(int(dim_), nsites_, states_, float(j2), pb, pb + off_w2_, pb + off_w3_,
+                                 p_ + off_b1_, p_ + off_b2_, p_ + off_b3_, Oall, err_, c.stream), "tensor-core forward");
+    int e = 0;
+    cuda_check(cudaMemcpyAsync(&e, err_, sizeof(int), cudaMemcpyDeviceToHost, c.stream), "D2H");
+    c.sync();
+    if (e) throw DeviceError("qkrylov_b200: tensor-core forward: an MMA completion wait expired");
+  } else {
+    for (uint64_t r0 = 0; r0 < dim_; r0 += kChunk) {
+      const int n = int(std::min<uint64_t>(kChunk, dim_ - r0));
+      forward(n, nullptr, states_ + r0, nullptr, float(j2));
+      cuda_check(cudaMemcpyAsync(Oall + 2 * r0, O_, size_t(n) * 2 * 4, cudaMemcpyDeviceToDevice, c.stream), "copy");
+    }
   }
   // shift by the largest log-amplitude so that exp() cannot overflow
   float* mx = reinterpret_cast<float*>(c.dres(0));

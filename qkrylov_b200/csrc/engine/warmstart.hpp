@@ -41,6 +41,10 @@ class WarmStartNet {
   // Start vector at coupling j2 over the whole basis, FP32, into device
   // memory `out` (dim floats), not normalised.
   void start_vector(double j2, float* out);
+  // Inference on the tensor cores (tcgen05, BF16 activations; default) or
+  // on the CUDA cores (FP32 activations, the training forward).
+  void set_tensor_cores(bool on) { tc_ = on; }
+  bool tensor_cores() const { return tc_; }
   // Loss and gradient (FP32, layout of params()) on explicit samples.
   double loss_grad(int n, const uint64_t* states, const double* j2, const float* targets, double c_sign,
                    std::vector<float>* grad);
@@ -65,6 +69,8 @@ class WarmStartNet {
   float *X_ = nullptr, *Z1_ = nullptr, *H1_ = nullptr, *Z2_ = nullptr, *H2_ = nullptr, *O_ = nullptr,
         *dO_ = nullptr, *dH_ = nullptr, *dZ_ = nullptr, *tgt_ = nullptr, *j2_ = nullptr;
   uint32_t* idx_ = nullptr;
+  bool tc_ = true;
+  int* err_ = nullptr;  // device flag of the tensor-core kernel
 };
 
 }  // namespace qkb

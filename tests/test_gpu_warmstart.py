@@ -40,10 +40,40 @@ def test_start_vector_matches_oracle():
     N = 10
     B = qk.SpinHalfBasis(N, sz=0)
     net = qk.WarmStartMLP(B, seed=9)
+    net.set_tensor_cores(False)   # CUDA cores: FP32 activations, as in training
     phi = net.start_vector(0.37)
     ref = mlp.start_vector(net.params, B.states(), 0.37, N)
     assert phi.dtype == np.float32
     assert np.max(np.abs(phi - ref)) <= 1e-4 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("N,j2", [(10, 0.37), (16, 0.81), (24, 0.05)])
+def test_tensor_core_inference_matches_oracle(N, j2):
+    # tcgen05 MMAs: BF16 weights and activations, FP32 accumulation in TMEM;
+    # the oracle rounds the same operands to BF16 and accumulates in FP64
+    B = qk.SpinHalfBasis(N, sz=0)
+    net = qk.WarmStartMLP(B, seed=2)
+    p = net.params
+    p[-258:] = np.random.default_rng(0).standard_normal(258).astype(np.float32) * 0.3  # non-zero biases
+    net.params = p
+    phi = net.start_vector(j2).astype(np.float64)
+    st = B.states()
+    idx = np.random.default_rng(1).choice(st.size, min(st.size, 4000), replace=False)
+    # the start vector is shifted by the largest log-amplitude over the whole basis
+    ref_all = mlp.start_vector(net.params, st, j2, N, act_bf16=True) if st.size <= 20000 else None
+    if ref_all is not None:
+        assert np.max(np.abs(phi - ref_all)) <= 2e-3 * np.max(np.abs(ref_all))
+    else:
+        X = mlp.inputs(st[idx], j2, N)
+        O = mlp.forward(net.params, X, N, act_bf16=True)["O"]
+        m = np.where(np.array([bin(int(v)).count("1") & 1 for v in (st[idx] & np.uint64(mlp.marshall_mask(N)))]) == 1,
+                     -1.0, 1.0)
+        ratio = phi[idx] / (m * np.exp(O[:, 0]) * np.tanh(O[:, 1]))   # exp(-shift), the same for every state
+        assert np.max(np.abs(ratio / np.median(ratio) - 1)) < 5e-3
+    net.set_tensor_cores(False)
+    phi32 = net.start_vector(j2).astype(np.float64)
+    cos = abs(phi @ phi32) / (np.linalg.norm(phi) * np.linalg.norm(phi32))
+    assert cos > 0.999
 
 
 def test_training_and_warm_start_gain():
