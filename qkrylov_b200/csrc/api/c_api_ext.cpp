@@ -421,16 +421,12 @@ int qkrylov_b200_mlp_start_vector(qkrylov_b200_mlp_h h, double j2, float* out, i
       h->net->start_vector(j2, out);
       return QKRYLOV_SUCCESS;
     }
-    float* d = nullptr;
-    qkb::cuda_check(cudaMalloc(&d, dim * 4), "device allocation");
-    try {
-      h->net->start_vector(j2, d);
-      qkb::cuda_check(cudaMemcpy(out, d, dim * 4, cudaMemcpyDeviceToHost), "D2H");
-    } catch (...) {
-      cudaFree(d);
-      throw;
-    }
-    cudaFree(d);
+    qkb::Context& c = qkb::Context::get(h->net->device());
+    qkb::DevVec d(dim, QK_F32, h->net->device(), false);
+    h->net->start_vector(j2, static_cast<float*>(d.data()));
+    // the start vector is written on the context's (non-blocking) stream
+    qkb::cuda_check(cudaMemcpyAsync(out, d.data(), dim * 4, cudaMemcpyDeviceToHost, c.stream), "D2H");
+    c.sync();
     return QKRYLOV_SUCCESS;
   });
 }

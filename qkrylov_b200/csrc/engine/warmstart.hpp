@@ -27,6 +27,7 @@ class WarmStartNet {
 
   int nsites() const { return nsites_; }
   uint64_t dim() const { return dim_; }
+  int device() const { return dev_; }
   size_t num_params() const { return np_; }
   size_t num_weights() const { return nw_; }
   // Parameters in FP32: W1 [128][nsites+1], W2 [128][128], W3 [2][128], b1, b2, b3.
