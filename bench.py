@@ -272,6 +272,7 @@ def warm_start(qk, N=24, eval_every=16, eval_offset=4, steps=1500, batch=8192, t
     t1 = time.perf_counter()
     loss = net.train(steps=steps, batch=batch, lr=2e-3, seed=3)
     train_s = time.perf_counter() - t1
+    net.start_vector(train_k[1] / 255.0)  # warm-up of the inference kernel (module load, shared-memory attribute)
     rows = []
     for k in range(eval_offset, 256, eval_every):
         if k % 8 == 0:
@@ -305,6 +306,7 @@ def warm_start(qk, N=24, eval_every=16, eval_offset=4, steps=1500, batch=8192, t
             "mean_iterations": {n: float(np.mean([r["iterations"][n] for r in rows]))
                                 for n in ("plain_fp64", "mixed", "mixed_warm")},
             "mean_inference_s": float(np.mean([r["inference_s"] for r in rows])),
+            "max_inference_s": float(np.max([r["inference_s"] for r in rows])),
             "wall_seconds": time.perf_counter() - t0}
 
 
