@@ -16,6 +16,8 @@ tables, term tables and repeated gathers are not counted).
          refinement, both to the explicit residual 1e-10 (wall seconds)
   batched_ftlm  t-J N=20 FTLM, 64 vectors x 100 steps x 200 temperatures:
          one block (FP32 / FP64 vectors, CUDA graph) vs the one-vector loop
+  dynamics  S(q=pi, omega) of the same chain: ground state, phi0 =
+         Sz(pi)|psi0>, 300 continued-fraction steps, 2001 omega points
   warm_start  J1-J2 N=24: network trained on 32 couplings, time-to-E0 at
          untrained couplings for plain FP64 / mixed / mixed + warm start
 
@@ -310,6 +312,42 @@ def warm_start(qk, N=24, eval_every=16, eval_offset=4, steps=1500, batch=8192, t
             "wall_seconds": time.perf_counter() - t0}
 
 
+def dynamics(qk, N, steps=300, eta=0.05, npts=2001, tol=1e-10):
+    """Dynamical structure factor of the Heisenberg chain: ground state by
+    the mixed-precision Lanczos, phi0 = Sz(q=pi)|psi0> = N^-1/2 sum_j (-1)^j
+    Sz_j |psi0> applied as an OpSum-defined operator through the same H.x
+    path, `steps` continued-fraction Lanczos steps from phi0 (host vector in,
+    coefficients out, through the reference-facing API), then S(omega) on
+    `npts` points of [0, 4] with broadening eta."""
+    B = qk.SpinHalfBasis(N, sz=0)
+    H = qk.MatrixFreeHamiltonian(B, qk.SpinHalfSite(), heisenberg_opsum(qk, N, np.float64), dtype=np.float64)
+    t0 = time.perf_counter()
+    r = qk.lanczos_mixed(H, seed=1, tol=tol, eigenvector=True)
+    t_gs = time.perf_counter() - t0
+    sz = qk.OpSum(dtype=np.float64)
+    for j in range(N):
+        sz.add_term((-1.0) ** j / np.sqrt(N), "Sz", j)
+    O = qk.MatrixFreeHamiltonian(B, qk.SpinHalfSite(), sz, dtype=np.float64)
+    t0 = time.perf_counter()
+    phi = O.apply(r.eigenvector)
+    t_phi = time.perf_counter() - t0
+    del O
+    t0 = time.perf_counter()
+    cf = qk.continued_fraction_coeffs(H, phi, steps)
+    t_cf = time.perf_counter() - t0
+    omega = np.linspace(0.0, 4.0, npts)
+    t0 = time.perf_counter()
+    S = np.array([qk.evaluate_spectral_function(cf, w, r.energy, eta) for w in omega])
+    t_s = time.perf_counter() - t0
+    return {"workload": f"heisenberg_chain_N{N}_Sz0_SzPi", "dim": H.dimension, "steps": len(cf.alphas),
+            "E0": r.energy, "ground_state_seconds": t_gs, "phi0_seconds": t_phi, "norm_phi0": cf.norm_phi0,
+            "cf_seconds": t_cf, "ms_per_cf_step": t_cf / max(1, len(cf.alphas)) * 1e3,
+            "spectral_points": npts, "spectral_seconds": t_s, "eta": eta,
+            "omega_peak": float(omega[int(np.argmax(S))]),
+            "weight_0_4": float(np.sum(S) * (omega[1] - omega[0])),
+            "note": "cf_seconds includes the host-to-device copy of phi0 (complex128, 642 MB at N=28)"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -442,6 +480,11 @@ def run_b200(args):
             line["batched_ftlm"] = batched_ftlm(qk)
         except Exception as e:
             line["batched_ftlm"] = {"error": str(e)}
+        try:
+            torch.cuda.empty_cache()
+            line["dynamics"] = dynamics(qk, N)
+        except Exception as e:
+            line["dynamics"] = {"error": str(e)}
         try:
             torch.cuda.empty_cache()
             line["warm_start"] = warm_start(qk)
