@@ -124,7 +124,6 @@ k_hx_spin(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __r
   for (int i = threadIdx.x; i < ndiag; i += blockDim.x) { sdm[i] = p.diag_smask[i]; sdw[i] = R(p.diag_w[i]); }
   __syncthreads();
   const int L = p.L;
-  const uint32_t lm = (1u << L) - 1u;
   double dr = 0.0, di = 0.0;
   for (uint32_t ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
     const qk_tile_t tile = p.tiles[ti];
