@@ -20,6 +20,8 @@ tables, term tables and repeated gathers are not counted).
          Sz(pi)|psi0>, 300 continued-fraction steps, 2001 omega points
   warm_start  J1-J2 N=24: network trained on 32 couplings, time-to-E0 at
          untrained couplings for plain FP64 / mixed / mixed + warm start
+  coupling_sweep  J1-J2 N=24 at 32 untrained couplings: one batched block
+         of 32 FP64 Lanczos recurrences vs one coupling at a time
 
 --impl reference times the reference's own CPU implementation (its
 unchanged sources, oracle/_ref, OpenMP on all host cores) on a bounded
@@ -348,6 +350,47 @@ def dynamics(qk, N, steps=300, eta=0.05, npts=2001, tol=1e-10):
             "note": "cf_seconds includes the host-to-device copy of phi0 (complex128, 642 MB at N=28)"}
 
 
+def coupling_sweep(qk, N=24, tol=1e-10):
+    """J1-J2 chain, Sz=0, at the 32 couplings J2_k = k/255, k = 4, 12, ...,
+    252: the batched sweep (one FP64 block of 32 Lanczos recurrences over
+    H0 = J1 part and H1 = unit J2 part) against the plain FP64 GPU Lanczos
+    and the mixed-precision form run one coupling at a time from random
+    starts, all to the explicit residual tol."""
+    B = qk.SpinHalfBasis(N, sz=0)
+    os0, os1 = qk.OpSum(dtype=np.float64), qk.OpSum(dtype=np.float64)
+    for d, os_ in ((1, os0), (2, os1)):
+        for i in range(N):
+            j = (i + d) % N
+            os_.add_term(1.0, "Sz", i, "Sz", j)
+            os_.add_term(0.5, "Sp", i, "Sm", j)
+            os_.add_term(0.5, "Sm", i, "Sp", j)
+    H0 = qk.MatrixFreeHamiltonian(B, qk.SpinHalfSite(), os0, dtype=np.float64)
+    H1 = qk.MatrixFreeHamiltonian(B, qk.SpinHalfSite(), os1, dtype=np.float64)
+    g = np.array([k / 255.0 for k in range(4, 256, 8)])
+    qk.lanczos_sweep(H0, H1, g, tol=1e-6)  # warm-up: block tile tuning of both operators, memory pool
+    t0 = time.perf_counter()
+    sw = qk.lanczos_sweep(H0, H1, g, tol=tol)
+    t_sweep = time.perf_counter() - t0
+    seq = {"plain_fp64": 0.0, "mixed": 0.0}
+    dE = 0.0
+    for q, j2 in enumerate(g):
+        H = qk.MatrixFreeHamiltonian(B, qk.SpinHalfSite(), j1j2_opsum(qk, N, 1.0, j2), dtype=np.float64)
+        qk.lanczos_mixed(H, seed=2, tol=tol)  # warm-up of this operator's kernels
+        for name, fn in (("plain_fp64", qk.lanczos_fp64), ("mixed", qk.lanczos_mixed)):
+            t1 = time.perf_counter()
+            r = fn(H, seed=2, tol=tol)
+            seq[name] += time.perf_counter() - t1
+            if name == "plain_fp64":
+                dE = max(dE, abs(r.energy - sw.energies[q]))
+        del H
+    return {"workload": f"j1j2_chain_N{N}_Sz0_32_couplings", "dim": B.size, "couplings": len(g), "block": sw.block,
+            "sweep_seconds": t_sweep, "sweep_steps": sw.steps, "sweep_passes": sw.passes,
+            "sweep_pass_len": 64, "sweep_memory_gb": (64 + 4) * B.size * sw.block * 8 / 1e9,
+            "sweep_max_residual": float(sw.residuals.max()), "sweep_all_converged": bool(sw.converged.all()),
+            "sequential_seconds": seq, "speedup_vs_plain_fp64": seq["plain_fp64"] / t_sweep,
+            "speedup_vs_mixed": seq["mixed"] / t_sweep, "max_dE_vs_plain_fp64": dE}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -490,6 +533,11 @@ def run_b200(args):
             line["warm_start"] = warm_start(qk)
         except Exception as e:
             line["warm_start"] = {"error": str(e)}
+        try:
+            torch.cuda.empty_cache()
+            line["coupling_sweep"] = coupling_sweep(qk)
+        except Exception as e:
+            line["coupling_sweep"] = {"error": str(e)}
     if rank == 0 and not args.no_cpu_baseline:
         try:
             cb = cpu_reference_gbs(N=24, steps=2)

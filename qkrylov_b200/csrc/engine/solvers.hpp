@@ -131,6 +131,20 @@ struct DavidsonBlockOut {
 DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int block, int max_subspace, double tol,
                                 uint64_t seed, int maxiter, double* evecs_out);
 
+// Batched coupling sweep (no counterpart in the reference): ground states
+// of H0 + g H1 for up to 128 couplings g as one row-interleaved FP64 block,
+// each column its own Lanczos recurrence kept semi-orthogonal by partial
+// reorthogonalisation, restarted from its Ritz vector (passes of at most
+// pass_len steps) until every explicit residual |H psi - E psi| / |E| <= tol.
+struct SweepOut {
+  std::vector<double> energies, residuals;
+  std::vector<int> converged;
+  int R = 0, steps = 0, passes = 0, applies = 0, reorths = 0, lanes_per_row = 0;
+  double seconds = 0;
+};
+SweepOut lanczos_sweep(const Operator& H0, const Operator& H1, const std::vector<double>& couplings, int pass_len,
+                       int max_passes, double tol, uint64_t seed);
+
 // src/solvers/dynamics.cpp:12-59
 template <class Real>
 CFOut<Real> continued_fraction(const Operator& H, const std::complex<Real>* phi0, int n_iter);

@@ -206,12 +206,173 @@ __global__ void k_block_column(size_t n, int R, const void* __restrict__ X, int 
   }
 }
 
+// Column-wise kernels of the batched coupling sweep (real vectors, element
+// type E): every thread keeps one column c = threadIdx.x % R, because the
+// block size and the grid stride are multiples of R.  Column sums go to
+// per-CTA partials partials[o * G + b] and a second launch reduces them in a
+// fixed order (deterministic results).
+constexpr int kSweepJ = 16;      // blocks combined per pass over the rows
+constexpr int kSweepMaxV = 192;  // blocks per call
+
+// sum over the threads of this CTA that hold column threadIdx.x % R,
+// written by the first R threads to partials[o * G + blockIdx.x]
+__device__ __forceinline__ void column_partial(double v, int R, size_t o_base, double* red, double* partials) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+  if (threadIdx.x < unsigned(R)) {
+    double s = 0.0;
+    for (int t = threadIdx.x; t < kBT; t += R) s += red[t];
+    partials[(o_base + threadIdx.x) * gridDim.x + blockIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// out[2 (j R + c)] = <V_j[:, c], W[:, c]> for j < nv (partials only; see k_sweep_reduce)
+template <class E>
+__global__ void __launch_bounds__(kBT)
+k_block_mdot(size_t n, int R, int nv, const void* const* __restrict__ V, const E* __restrict__ W,
+             double* __restrict__ partials) {
+  __shared__ const E* sV[kSweepMaxV];
+  __shared__ double red[kBT];
+  for (int j = threadIdx.x; j < nv; j += kBT) sV[j] = static_cast<const E*>(V[j]);
+  __syncthreads();
+  const size_t total = n * size_t(R), stride = size_t(gridDim.x) * kBT;
+  const size_t g0 = size_t(blockIdx.x) * kBT + threadIdx.x;
+  for (int j0 = 0; j0 < nv; j0 += kSweepJ) {
+    double acc[kSweepJ];
+    #pragma unroll
+    for (int u = 0; u < kSweepJ; ++u) acc[u] = 0.0;
+    for (size_t f = g0; f < total; f += stride) {
+      const double w = double(W[f]);
+      #pragma unroll
+      for (int u = 0; u < kSweepJ; ++u)
+        if (j0 + u < nv) acc[u] += double(__ldg(sV[j0 + u] + f)) * w;
+    }
+    #pragma unroll
+    for (int u = 0; u < kSweepJ; ++u)  // the condition is the same for the whole CTA
+      if (j0 + u < nv) column_partial(acc[u], R, size_t(j0 + u) * R, red, partials);
+  }
+}
+
+// W[:, c] = (keep ? W[:, c] : 0) - sum_j coef[2 (j R + c)] V_j[:, c], in j
+// order; partials of |W[:, c]|^2 (after rounding to E) when partials != NULL
+template <class E>
+__global__ void __launch_bounds__(kBT)
+k_block_mcomb(size_t n, int R, int nv, const void* const* __restrict__ V, const double* __restrict__ coef, int keep,
+              E* W, double* __restrict__ partials) {
+  __shared__ const E* sV[kSweepMaxV];
+  __shared__ double red[kBT];
+  for (int j = threadIdx.x; j < nv; j += kBT) sV[j] = static_cast<const E*>(V[j]);
+  __syncthreads();
+  const size_t total = n * size_t(R), stride = size_t(gridDim.x) * kBT;
+  const size_t g0 = size_t(blockIdx.x) * kBT + threadIdx.x;
+  const int c = int(threadIdx.x) % R;
+  double acc = 0.0;
+  for (int j0 = 0; j0 < nv; j0 += kSweepJ) {
+    double cf[kSweepJ];
+    #pragma unroll
+    for (int u = 0; u < kSweepJ; ++u) cf[u] = j0 + u < nv ? coef[2 * (size_t(j0 + u) * R + c)] : 0.0;
+    const bool zero = j0 == 0 && !keep, last = j0 + kSweepJ >= nv;
+    for (size_t f = g0; f < total; f += stride) {
+      double x = zero ? 0.0 : double(W[f]);
+      #pragma unroll
+      for (int u = 0; u < kSweepJ; ++u)
+        if (j0 + u < nv) x -= cf[u] * double(__ldg(sV[j0 + u] + f));
+      const E xe = E(x);
+      W[f] = xe;
+      if (last) acc += double(xe) * double(xe);
+    }
+  }
+  if (partials) column_partial(acc, R, 0, red, partials);
+}
+
+// Y0[:, c] += g[c] Y1[:, c]; partials of <X[:, c], Y0[:, c]>
+template <class E>
+__global__ void __launch_bounds__(kBT)
+k_block_axpy_cols(size_t n, int R, const double* __restrict__ g, const E* __restrict__ Y1, E* Y0,
+                  const E* __restrict__ X, double* __restrict__ partials) {
+  __shared__ double red[kBT];
+  const size_t total = n * size_t(R), stride = size_t(gridDim.x) * kBT;
+  const double gc = g[int(threadIdx.x) % R];
+  double acc = 0.0;
+  for (size_t f = size_t(blockIdx.x) * kBT + threadIdx.x; f < total; f += stride) {
+    const E y = E(double(Y0[f]) + gc * double(Y1[f]));
+    Y0[f] = y;
+    acc += double(X[f]) * double(y);
+  }
+  column_partial(acc, R, 0, red, partials);
+}
+
+// out[2 o] = sum_b partials[o * G + b] (lanes stride over b, then a warp
+// sum), out[2 o + 1] = 0; one warp per output
+__global__ void k_sweep_reduce(const double* __restrict__ partials, int G, int nout, double* out) {
+  const int o = blockIdx.x * (kBT / 32) + int(threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (o >= nout) return;
+  double s = 0.0;
+  for (int b = lane; b < G; b += 32) s += partials[size_t(o) * G + b];
+  s = warp_sum(s);
+  if (lane == 0) { out[2 * o] = s; out[2 * o + 1] = 0.0; }
+}
+
+inline int sweep_finish(const double* partials, unsigned G, int nout, double* out, cudaStream_t s) {
+  k_sweep_reduce<<<unsigned((nout + kBT / 32 - 1) / (kBT / 32)), kBT, 0, s>>>(partials, int(G), nout, out);
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
+
 }  // namespace
 }  // namespace qkd
 
 using namespace qkd;
 
 extern "C" {
+
+int qkd_block_partials_grid(size_t n, int R) { return int(block_grid(n * size_t(R))); }
+
+#define QKD_REAL_DISPATCH(t, ...)                          \
+  do {                                                     \
+    if ((t) == QK_F64) { using E = double; __VA_ARGS__; }  \
+    else if ((t) == QK_F32) { using E = float; __VA_ARGS__; } \
+    else return QKD_EINVAL;                                \
+  } while (0)
+
+int qkd_block_mdot(qk_dtype t, size_t n, int R, int nv, const void* const* V, const void* W, double* partials,
+                   size_t partials_cap, double* out, cudaStream_t s) {
+  if (!V || !W || !partials || !out || R <= 0 || kBT % R != 0 || nv < 1 || nv > kSweepMaxV) return QKD_EINVAL;
+  if (n == 0) return QKD_OK;
+  const unsigned G = block_grid(n * size_t(R));
+  if (size_t(nv) * R * G > partials_cap) return QKD_EINVAL;
+  QKD_REAL_DISPATCH(t, (k_block_mdot<E><<<G, kBT, 0, s>>>(n, R, nv, V, static_cast<const E*>(W), partials)));
+  QKD_LAUNCH_CHECK();
+  return sweep_finish(partials, G, nv * R, out, s);
+}
+
+int qkd_block_mcomb(qk_dtype t, size_t n, int R, int nv, const void* const* V, const double* coef, int keep, void* W,
+                    double* partials, size_t partials_cap, double* nrm2, cudaStream_t s) {
+  if (!V || !coef || !W || R <= 0 || kBT % R != 0 || nv < 1 || nv > kSweepMaxV || (nrm2 && !partials))
+    return QKD_EINVAL;
+  if (n == 0) return QKD_OK;
+  const unsigned G = block_grid(n * size_t(R));
+  if (nrm2 && size_t(R) * G > partials_cap) return QKD_EINVAL;
+  QKD_REAL_DISPATCH(t, (k_block_mcomb<E><<<G, kBT, 0, s>>>(n, R, nv, V, coef, keep, static_cast<E*>(W),
+                                                            nrm2 ? partials : nullptr)));
+  QKD_LAUNCH_CHECK();
+  return nrm2 ? sweep_finish(partials, G, R, nrm2, s) : QKD_OK;
+}
+
+int qkd_block_axpy_cols(qk_dtype t, size_t n, int R, const double* g, const void* Y1, void* Y0, const void* X,
+                        double* partials, size_t partials_cap, double* dots, cudaStream_t s) {
+  if (!g || !Y1 || !Y0 || !X || !partials || !dots || R <= 0 || kBT % R != 0) return QKD_EINVAL;
+  if (n == 0) return QKD_OK;
+  const unsigned G = block_grid(n * size_t(R));
+  if (size_t(R) * G > partials_cap) return QKD_EINVAL;
+  QKD_REAL_DISPATCH(t, (k_block_axpy_cols<E><<<G, kBT, 0, s>>>(n, R, g, static_cast<const E*>(Y1), static_cast<E*>(Y0),
+                                                                static_cast<const E*>(X), partials)));
+  QKD_LAUNCH_CHECK();
+  return sweep_finish(partials, G, R, dots, s);
+}
+
+#undef QKD_REAL_DISPATCH
 
 int qkd_block_update(qk_workspace* w, qk_dtype t, size_t n, int R, const void* V, const double* a, const void* Vp,
                      const double* b, void* W, double* nrm2, cudaStream_t s) {

@@ -160,6 +160,24 @@ int qkd_block_scale(qk_dtype t, size_t n, int R, const double* nrm2, void* W, do
                     cudaStream_t s);
 /* out (n elements) = column c of the block X. */
 int qkd_block_column(qk_dtype t, size_t n, int R, const void* X, int c, void* out, cudaStream_t s);
+/* Column-wise kernels of the batched coupling sweep on real blocks (t =
+ * QK_F64 or QK_F32; R divides 256).  Results are column sums reduced in a
+ * fixed order from per-CTA partials: partials (device) must hold
+ * count * qkd_block_partials_grid(n, R) doubles, count = nv * R for
+ * qkd_block_mdot and R otherwise (partials_cap = its size).  Outputs use
+ * the (re, im) layout out[2 o], out[2 o + 1] = 0.  V: device array of nv
+ * (<= 192) device pointers to blocks.
+ *   mdot:      out[2 (j R + c)] = <V_j[:, c], W[:, c]>
+ *   mcomb:     W[:, c] = (keep ? W[:, c] : 0) - sum_j coef[2 (j R + c)] V_j[:, c];
+ *              nrm2 (may be NULL) = column norms^2 of the result
+ *   axpy_cols: Y0[:, c] += g[c] Y1[:, c]; dots = <X[:, c], Y0[:, c]> */
+int qkd_block_partials_grid(size_t n, int R);
+int qkd_block_mdot(qk_dtype t, size_t n, int R, int nv, const void* const* V, const void* W, double* partials,
+                   size_t partials_cap, double* out, cudaStream_t s);
+int qkd_block_mcomb(qk_dtype t, size_t n, int R, int nv, const void* const* V, const double* coef, int keep, void* W,
+                    double* partials, size_t partials_cap, double* nrm2, cudaStream_t s);
+int qkd_block_axpy_cols(qk_dtype t, size_t n, int R, const double* g, const void* Y1, void* Y0, const void* X,
+                        double* partials, size_t partials_cap, double* dots, cudaStream_t s);
 /* Device scratch of the workspace: 2*kMaxK+16 doubles for small results. */
 double* qkd_workspace_results(qk_workspace* w);
 
