@@ -23,6 +23,10 @@ tables, term tables and repeated gathers are not counted).
   coupling_sweep  J1-J2 N=24 at 32 untrained couplings: one batched block
          of 32 FP64 Lanczos recurrences vs one coupling at a time
 
+cpu_baseline  the reference's own CPU H.x (oracle/_ref) at N=24; with the
+         solver legs also its Lanczos (Heisenberg N=22) and FTLM (t-J N=14,
+         one temperature) beside this build's GPU solvers on the same models
+
 --impl reference times the reference's own CPU implementation (its
 unchanged sources, oracle/_ref, OpenMP on all host cores) on a bounded
 sample of the workload, on the same metric.
@@ -185,6 +189,66 @@ def cpu_reference_gbs(N=24, steps=3, use_ref=True):
                 kind=kind, sample=f"Heisenberg N={N} Sz=0 (dim {H.dim}) complex128 H.x, median of {steps}; "
                 f"setup (basis + CSR build) {setup:.1f} s; N=28 needs ~100 GB of CSR + reserve on the host",
                 seconds_per_apply=t)
+
+
+def cpu_reference_solvers(qk, N=22, tj_N=14, R=64, M=100):
+    """The reference's own CPU solvers (its unchanged sources, oracle/_ref,
+    all host threads) beside this build's GPU solvers on the same models at
+    sizes the CPU finishes in seconds:
+      lanczos  Heisenberg chain N, Sz=0: lanczos_ground_state(maxiter 200,
+               tol 1e-12), the reference's start vector on both sides
+      ftlm     t-J chain tj_N (2 holes): the reference's ftlm at one
+               temperature (R complex Gaussian vectors, M steps) against the
+               GPU's reference-semantics ftlm at one temperature and the
+               batched block (R Rademacher vectors, M steps) at 200."""
+    import oracle as O
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    kind = "reference" if O.have_ref() else "port"
+    back = O.ref() if kind == "reference" else O.port()
+    out = {"kind": kind, "cores": int(os.environ.get("OMP_NUM_THREADS", threads))}
+    sec = dict(use_sz=1, sz2=0)
+    t0 = time.perf_counter()
+    Hc = back.hamiltonian("spin", N, sec, O.heisenberg_chain(N))
+    setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rc = Hc.lanczos(200, 1e-12, want_vector=False)
+    t_cpu = time.perf_counter() - t0
+    del Hc
+    Hg = qk.MatrixFreeHamiltonian(qk.SpinHalfBasis(N, sz=0), qk.SpinHalfSite(), heisenberg_opsum(qk, N, np.float64),
+                                  dtype=np.float64)
+    qk.lanczos_ground_state(Hg, 20, 1e-12)  # warm-up
+    t0 = time.perf_counter()
+    rg = qk.lanczos_ground_state(Hg, 200, 1e-12)
+    t_gpu = time.perf_counter() - t0
+    out["lanczos"] = {"workload": f"heisenberg_chain_N{N}_Sz0", "cpu_setup_seconds": setup, "cpu_seconds": t_cpu,
+                      "cpu_iterations": rc["iterations"], "gpu_seconds": t_gpu, "gpu_iterations": rg.iterations,
+                      "dE": abs(rc["energy"] - rg.energy), "speedup": t_cpu / t_gpu}
+    del Hg
+    ne = tj_N - 2
+    tsec = dict(use_nup=1, nup=ne // 2, use_ndn=1, ndn=ne - ne // 2)
+    Hc = back.hamiltonian("tj", tj_N, tsec, O.tj_chain(tj_N, 1.0, 0.4))
+    t0 = time.perf_counter()
+    fc = Hc.ftlm(1.0, R, M)
+    t_cpu = time.perf_counter() - t0
+    del Hc
+    B = qk.TJBasis(tj_N, conserve_nup=True, nup=ne // 2, conserve_ndn=True, ndn=ne - ne // 2)
+    Hg = qk.MatrixFreeHamiltonian(B, qk.TJSite(), tj_opsum(qk, tj_N, 1.0, 0.4), dtype=np.float64)
+    qk.ftlm(Hg, 1.0, 4, M)  # warm-up
+    t0 = time.perf_counter()
+    fg = qk.ftlm(Hg, 1.0, R, M)
+    t_one = time.perf_counter() - t0
+    T = 0.01 * 1000.0 ** (np.arange(200) / 199.0)
+    qk.ftlm_block(Hg, T, n_random=R, n_steps=M, seed=5, precision=64)  # tunes the tile shape
+    t0 = time.perf_counter()
+    qk.ftlm_block(Hg, T, n_random=R, n_steps=M, seed=5, precision=64)
+    t_blk = time.perf_counter() - t0
+    out["ftlm"] = {"workload": f"tj_chain_N{tj_N}_2holes_Sz0", "dim": Hg.dimension, "R": R, "M": M,
+                   "cpu_seconds_per_temperature": t_cpu, "gpu_seconds_per_temperature": t_one,
+                   "gpu_block_seconds_200_temperatures": t_blk,
+                   "cpu_seconds_200_temperatures": 200 * t_cpu,
+                   "U_cpu_T1": fc["U"], "U_gpu_T1": fg.internal_energy}
+    return out
 
 
 def time_to_e0(qk, N, tol=1e-10, seed=1):
@@ -542,6 +606,8 @@ def run_b200(args):
         try:
             cb = cpu_reference_gbs(N=24, steps=2)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            if not args.no_solvers:
+                line["cpu_baseline"]["solvers"] = cpu_reference_solvers(qk)
         except Exception as e:  # reported, never silently replaced
             line["cpu_baseline"] = {"value": None, "unit": "GB/s", "error": str(e)}
     if rank == 0:
