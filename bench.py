@@ -414,7 +414,7 @@ def dynamics(qk, N, steps=300, eta=0.05, npts=2001, tol=1e-10):
             "note": "cf_seconds includes the host-to-device copy of phi0 (complex128, 642 MB at N=28)"}
 
 
-def coupling_sweep(qk, N=24, tol=1e-10):
+def coupling_sweep(qk, N=24, tol=1e-10, sequential=True):
     """J1-J2 chain, Sz=0, at the 32 couplings J2_k = k/255, k = 4, 12, ...,
     252: the batched sweep (one FP64 block of 32 Lanczos recurrences over
     H0 = J1 part and H1 = unit J2 part) against the plain FP64 GPU Lanczos
@@ -435,6 +435,10 @@ def coupling_sweep(qk, N=24, tol=1e-10):
     t0 = time.perf_counter()
     sw = qk.lanczos_sweep(H0, H1, g, tol=tol)
     t_sweep = time.perf_counter() - t0
+    if not sequential:
+        return {"workload": f"j1j2_chain_N{N}_Sz0_32_couplings", "dim": B.size, "couplings": len(g),
+                "block": sw.block, "sweep_seconds": t_sweep, "sweep_steps": sw.steps, "sweep_passes": sw.passes,
+                "sweep_all_converged": bool(sw.converged.all())}
     seq = {"plain_fp64": 0.0, "mixed": 0.0}
     dE = 0.0
     for q, j2 in enumerate(g):
@@ -517,6 +521,12 @@ def run_b200(args):
         return ms, launches
 
     peak, peak_kind = peaks()
+    if args.sweep_only:
+        if rank == 0:
+            print(json.dumps({"sweep_only": True, **coupling_sweep(qk, N=args.n, sequential=False)}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.kernel_only:
         qk.set_kernel_policy(args.policy)
         code, tdt, b = {"c128": (qk.DTYPE_C128, torch.complex128, 32), "c64": (qk.DTYPE_C64, torch.complex64, 16),
@@ -630,6 +640,8 @@ def main():
     ap.add_argument("--kernel-dtype", default="c128", choices=["c128", "c64", "f64", "f32"],
                     help="vector type of --kernel-only")
     ap.add_argument("--policy", default="auto", help="H.x kernel policy of --kernel-only (qkrylov_b200.set_kernel_policy)")
+    ap.add_argument("--sweep-only", action="store_true",
+                    help="only the batched coupling sweep on the J1-J2 chain of --n sites (no one-at-a-time runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

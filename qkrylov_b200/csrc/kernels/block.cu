@@ -71,23 +71,26 @@ k_block_update(size_t n, int R, const void* __restrict__ V, const double* __rest
   grid_finish(partials, ticket, R, nrm2);
 }
 
+// The block size (256) and the grid stride are multiples of R, so each
+// thread keeps one column and computes its scale once.
 template <int DT>
-__global__ void k_block_scale(size_t n, int R, const double* __restrict__ nrm2, void* W, double* beta_out,
-                              int* len, int step) {
+__global__ void __launch_bounds__(kBT)
+k_block_scale(size_t n, int R, const double* __restrict__ nrm2, void* W, double* beta_out, int* len, int step) {
   using T = VT<DT>;
   using R_ = typename T::R;
   const size_t total = n * size_t(R);
-  for (size_t f = size_t(blockIdx.x) * blockDim.x + threadIdx.x; f < total; f += size_t(gridDim.x) * blockDim.x) {
-    const int c = int(f % size_t(R));
-    const double beta = sqrt(nrm2[2 * c]);
-    const double sc = beta < 1e-15 ? 0.0 : 1.0 / beta;
+  const size_t g0 = size_t(blockIdx.x) * kBT + threadIdx.x;
+  const int c = int(threadIdx.x) % R;
+  const double beta = sqrt(nrm2[2 * c]);
+  const double sc = beta < 1e-15 ? 0.0 : 1.0 / beta;
+  if (g0 < size_t(R)) {
+    beta_out[c] = beta;
+    if (beta < 1e-15 && len[c] > step + 1) len[c] = step + 1;
+  }
+  for (size_t f = g0; f < total; f += size_t(gridDim.x) * kBT) {
     R_ wr, wi;
     T::ld_plain(W, f, wr, wi);
     T::st(W, f, R_(double(wr) * sc), R_(double(wi) * sc));
-    if (f < size_t(R)) {
-      beta_out[c] = beta;
-      if (beta < 1e-15 && len[c] > step + 1) len[c] = step + 1;
-    }
   }
 }
 
@@ -386,7 +389,7 @@ int qkd_block_update(qk_workspace* w, qk_dtype t, size_t n, int R, const void* V
 
 int qkd_block_scale(qk_dtype t, size_t n, int R, const double* nrm2, void* W, double* beta_out, int* len, int step,
                     cudaStream_t s) {
-  if (!nrm2 || !W || !beta_out || !len || R <= 0) return QKD_EINVAL;
+  if (!nrm2 || !W || !beta_out || !len || R <= 0 || kBT % R != 0) return QKD_EINVAL;
   if (n == 0) return QKD_OK;
   QKD_DISPATCH(t, k_block_scale<DT><<<block_grid(n * size_t(R)), kBT, 0, s>>>(n, R, nrm2, W, beta_out, len, step));
   QKD_LAUNCH_CHECK();
