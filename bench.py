@@ -364,7 +364,7 @@ def warm_start(qk, N=24, eval_every=16, eval_offset=4, steps=1500, batch=8192, t
                      "converged": all(v[1].converged for v in res.values())})
         del H
     tot = {n: sum(r["seconds"][n] for r in rows) for n in ("plain_fp64", "mixed", "mixed_warm")}
-    return {"workload": f"j1j2_chain_N{N}_Sz0", "dim": B.size, "train_J2": len(train_k),
+    return net, {"workload": f"j1j2_chain_N{N}_Sz0", "dim": B.size, "train_J2": len(train_k),
             "eval_J2": [r["J2"] for r in rows], "train_steps": steps, "batch": batch,
             "train_seconds": train_s, "ground_state_seconds": gs_s, "loss_first": float(loss[:20].mean()),
             "loss_last": float(loss[-20:].mean()), "params": net.n_params,
@@ -414,12 +414,14 @@ def dynamics(qk, N, steps=300, eta=0.05, npts=2001, tol=1e-10):
             "note": "cf_seconds includes the host-to-device copy of phi0 (complex128, 642 MB at N=28)"}
 
 
-def coupling_sweep(qk, N=24, tol=1e-10, sequential=True):
+def coupling_sweep(qk, N=24, tol=1e-10, sequential=True, net=None):
     """J1-J2 chain, Sz=0, at the 32 couplings J2_k = k/255, k = 4, 12, ...,
     252: the batched sweep (one FP64 block of 32 Lanczos recurrences over
     H0 = J1 part and H1 = unit J2 part) against the plain FP64 GPU Lanczos
     and the mixed-precision form run one coupling at a time from random
-    starts, all to the explicit residual tol."""
+    starts, all to the explicit residual tol; with the warm-start network
+    (trained on k = 0, 8, ..., 248) also the sweep from its start vectors
+    (inference included)."""
     B = qk.SpinHalfBasis(N, sz=0)
     os0, os1 = qk.OpSum(dtype=np.float64), qk.OpSum(dtype=np.float64)
     for d, os_ in ((1, os0), (2, os1)):
@@ -435,10 +437,17 @@ def coupling_sweep(qk, N=24, tol=1e-10, sequential=True):
     t0 = time.perf_counter()
     sw = qk.lanczos_sweep(H0, H1, g, tol=tol)
     t_sweep = time.perf_counter() - t0
+    warm = None
+    if net is not None:
+        t0 = time.perf_counter()
+        sww = qk.lanczos_sweep(H0, H1, g, tol=tol, net=net)
+        warm = {"seconds": time.perf_counter() - t0, "steps": sww.steps, "passes": sww.passes,
+                "inference_seconds": sww.seconds_inference, "all_converged": bool(sww.converged.all()),
+                "max_dE_vs_random_start_sweep": float(np.max(np.abs(sww.energies - sw.energies)))}
     if not sequential:
         return {"workload": f"j1j2_chain_N{N}_Sz0_32_couplings", "dim": B.size, "couplings": len(g),
                 "block": sw.block, "sweep_seconds": t_sweep, "sweep_steps": sw.steps, "sweep_passes": sw.passes,
-                "sweep_all_converged": bool(sw.converged.all())}
+                "sweep_all_converged": bool(sw.converged.all()), "sweep_warm": warm}
     seq = {"plain_fp64": 0.0, "mixed": 0.0}
     dE = 0.0
     for q, j2 in enumerate(g):
@@ -456,7 +465,9 @@ def coupling_sweep(qk, N=24, tol=1e-10, sequential=True):
             "sweep_pass_len": 64, "sweep_memory_gb": (64 + 4) * B.size * sw.block * 8 / 1e9,
             "sweep_max_residual": float(sw.residuals.max()), "sweep_all_converged": bool(sw.converged.all()),
             "sequential_seconds": seq, "speedup_vs_plain_fp64": seq["plain_fp64"] / t_sweep,
-            "speedup_vs_mixed": seq["mixed"] / t_sweep, "max_dE_vs_plain_fp64": dE}
+            "speedup_vs_mixed": seq["mixed"] / t_sweep, "max_dE_vs_plain_fp64": dE,
+            "sweep_warm": warm,
+            "speedup_warm_vs_plain_fp64": seq["plain_fp64"] / warm["seconds"] if warm else None}
 
 
 def run_reference(args):
@@ -602,14 +613,15 @@ def run_b200(args):
             line["dynamics"] = dynamics(qk, N)
         except Exception as e:
             line["dynamics"] = {"error": str(e)}
+        net = None
         try:
             torch.cuda.empty_cache()
-            line["warm_start"] = warm_start(qk)
+            net, line["warm_start"] = warm_start(qk)
         except Exception as e:
             line["warm_start"] = {"error": str(e)}
         try:
             torch.cuda.empty_cache()
-            line["coupling_sweep"] = coupling_sweep(qk)
+            line["coupling_sweep"] = coupling_sweep(qk, net=net)
         except Exception as e:
             line["coupling_sweep"] = {"error": str(e)}
     if rank == 0 and not args.no_cpu_baseline:

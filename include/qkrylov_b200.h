@@ -220,35 +220,6 @@ int qkrylov_b200_davidson_block(qkrylov_hamiltonian_h h, int precision, int n_ei
                                 double tol, uint64_t seed, int maxiter, double* evals, double* residuals,
                                 double* evecs, qkrylov_b200_davidson_info_t* info);
 
-/* ---------------------------------------------------- batched coupling sweep
- * No counterpart in the reference (its lanczos_ground_state, lanczos.hpp:
- * 11-25, solves one Hamiltonian at a time).  Ground states of
- * H(g) = H0 + g H1 for n_couplings (1..128) values of g at once: h0 and h1
- * are real operators on the same basis (e.g. the J1 and the unit-J2 parts of
- * a J1-J2 chain).  The couplings are the columns of one row-interleaved
- * FP64 block (32, 64 or 128 columns; extra columns repeat the last
- * coupling); each step is one block H.X per operator (the row's tables read
- * once for all columns), a column axpy forming H(g) X, and full
- * reorthogonalisation of every column against its own Krylov vectors.
- * Each column restarts from its Ritz vector after at most pass_len (2..128)
- * steps; the run ends when every column's explicit residual
- * |H psi - E psi| / |E| is <= tol or after max_passes (1..64) passes.  Start
- * block: uniform [-1, 1) from seed.  Device memory: (pass_len + 4) blocks
- * of dimension() x block doubles.  energies, residuals, converged:
- * n_couplings entries (residuals, converged and info may be NULL). */
-typedef struct {
-  int block;          /* columns of the block: 32, 64 or 128 */
-  int steps;          /* Lanczos steps (all columns advance together) */
-  int passes;         /* residual checks (restarts + 1) */
-  int applies;        /* block H.X products (two per step and check) */
-  int lanes_per_row;  /* tuned block H.X tile shape */
-  double seconds;
-} qkrylov_b200_sweep_info_t;
-
-int qkrylov_b200_lanczos_sweep(qkrylov_hamiltonian_h h0, qkrylov_hamiltonian_h h1, int n_couplings,
-                               const double* couplings, int pass_len, int max_passes, double tol, uint64_t seed,
-                               double* energies, double* residuals, int* converged, qkrylov_b200_sweep_info_t* info);
-
 /* ---------------------------------------------------------- batched FTLM
  * No counterpart in the reference (its ftlm, ftlm.hpp:21-27, runs one
  * complex Gaussian vector at a time and one temperature per call).
@@ -330,6 +301,43 @@ int qkrylov_b200_mlp_loss_grad(qkrylov_b200_mlp_h net, int n, const uint64_t* st
  * basis. */
 int qkrylov_b200_lanczos_warm(qkrylov_hamiltonian_h h, qkrylov_b200_mlp_h net, double j2, int maxiter, double tol,
                               qkrylov_b200_mixed_result_t* result, double* seconds_inference);
+
+/* ---------------------------------------------------- batched coupling sweep
+ * No counterpart in the reference (its lanczos_ground_state, lanczos.hpp:
+ * 11-25, solves one Hamiltonian at a time).  Ground states of
+ * H(g) = H0 + g H1 for n_couplings (1..128) values of g at once: h0 and h1
+ * are real operators on the same basis (e.g. the J1 and the unit-J2 parts of
+ * a J1-J2 chain).  The couplings are the columns of one row-interleaved
+ * FP64 block (32, 64 or 128 columns; extra columns repeat the last
+ * coupling); each step is one block H.X per operator (the row's tables read
+ * once for all columns), a column axpy forming H(g) X, and the three-term
+ * update; every column is kept semi-orthogonal against its own Krylov
+ * vectors by partial reorthogonalisation (Simon's estimates, classical
+ * Gram-Schmidt of the whole block when any column needs it).
+ * Each column restarts from its Ritz vector after at most pass_len (2..128)
+ * steps; the run ends when every column's explicit residual
+ * |H psi - E psi| / |E| is <= tol or after max_passes (1..64) passes.  Start
+ * block: uniform [-1, 1) from seed; with a warm-start network (net, on the
+ * same basis, NULL for none) column q starts from the network's start
+ * vector at coupling g_q (its coupling input is g; inference time is
+ * included in seconds and reported in seconds_inference).  Device memory:
+ * (pass_len + 4) blocks of dimension() x block doubles.  energies,
+ * residuals, converged: n_couplings entries (residuals, converged and info
+ * may be NULL). */
+typedef struct {
+  int block;          /* columns of the block: 32, 64 or 128 */
+  int steps;          /* Lanczos steps (all columns advance together) */
+  int passes;         /* residual checks (restarts + 1) */
+  int applies;        /* block H.X products (two per step and check) */
+  int lanes_per_row;  /* tuned block H.X tile shape */
+  double seconds;
+  double seconds_inference;  /* start vectors from the network (0 without one) */
+} qkrylov_b200_sweep_info_t;
+
+int qkrylov_b200_lanczos_sweep(qkrylov_hamiltonian_h h0, qkrylov_hamiltonian_h h1, int n_couplings,
+                               const double* couplings, int pass_len, int max_passes, double tol, uint64_t seed,
+                               qkrylov_b200_mlp_h net, double* energies, double* residuals, int* converged,
+                               qkrylov_b200_sweep_info_t* info);
 
 #ifdef __cplusplus
 }

@@ -701,6 +701,7 @@ class SweepResult:
         self.energies, self.residuals, self.converged = energies, residuals, converged
         self.block, self.steps, self.passes = info.block, info.steps, info.passes
         self.applies, self.lanes_per_row, self.seconds = info.applies, info.lanes_per_row, info.seconds
+        self.seconds_inference = info.seconds_inference
 
     def __repr__(self):
         return (f"SweepResult({len(self.energies)} couplings, steps={self.steps}, passes={self.passes}, "
@@ -708,19 +709,23 @@ class SweepResult:
 
 
 def lanczos_sweep(H0: MatrixFreeHamiltonian, H1: MatrixFreeHamiltonian, couplings: Sequence[float],
-                  tol: float = 1e-10, pass_len: int = 64, max_passes: int = 16, seed: int = 1) -> SweepResult:
+                  tol: float = 1e-10, pass_len: int = 64, max_passes: int = 16, seed: int = 1,
+                  net: Optional["WarmStartMLP"] = None) -> SweepResult:
     """Ground states of H0 + g H1 for every g in `couplings` (at most 128)
     at once: one FP64 block of Lanczos recurrences (one column per
-    coupling, full reorthogonalisation, restarts from the Ritz vector after
-    pass_len steps) until every explicit residual |H psi - E psi| / |E|
-    is <= tol.  H0 and H1: real operators on the same basis."""
+    coupling, partial reorthogonalisation, restarts from the Ritz vector
+    after pass_len steps) until every explicit residual |H psi - E psi| / |E|
+    is <= tol.  H0 and H1: real operators on the same basis.  net: a
+    WarmStartMLP on that basis whose coupling input is g; each column then
+    starts from the network's start vector (random starts without one)."""
     g = np.ascontiguousarray(couplings, dtype=np.float64)
     n = len(g)
     e, r, cv = np.zeros(n), np.zeros(n), np.zeros(n, dtype=np.int32)
     info = _SweepInfo()
     _check(lib().qkrylov_b200_lanczos_sweep(H0._h, H1._h, n, g.ctypes.data, pass_len, max_passes, tol,
-                                            ctypes.c_uint64(seed), e.ctypes.data, r.ctypes.data, cv.ctypes.data,
-                                            ctypes.byref(info)), "lanczos_sweep")
+                                            ctypes.c_uint64(seed), net._h if net is not None else None,
+                                            e.ctypes.data, r.ctypes.data, cv.ctypes.data, ctypes.byref(info)),
+           "lanczos_sweep")
     return SweepResult(e, r, cv.astype(bool), info)
 
 
@@ -861,7 +866,7 @@ class _DavidsonBlockInfo(ctypes.Structure):
 
 class _SweepInfo(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int), ("steps", ctypes.c_int), ("passes", ctypes.c_int), ("applies", ctypes.c_int),
-                ("lanes_per_row", ctypes.c_int), ("seconds", ctypes.c_double)]
+                ("lanes_per_row", ctypes.c_int), ("seconds", ctypes.c_double), ("seconds_inference", ctypes.c_double)]
 
 
 class _FTLMInfo(ctypes.Structure):

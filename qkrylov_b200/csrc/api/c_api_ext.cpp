@@ -492,14 +492,16 @@ int qkrylov_b200_davidson_block(qkrylov_hamiltonian_h h, int precision, int n_ei
 
 int qkrylov_b200_lanczos_sweep(qkrylov_hamiltonian_h h0, qkrylov_hamiltonian_h h1, int n_couplings,
                                const double* couplings, int pass_len, int max_passes, double tol, uint64_t seed,
-                               double* energies, double* residuals, int* converged, qkrylov_b200_sweep_info_t* info) {
+                               qkrylov_b200_mlp_h net, double* energies, double* residuals, int* converged,
+                               qkrylov_b200_sweep_info_t* info) {
   if (!h0 || !h0->op || !h1 || !h1->op || !couplings || !energies || n_couplings < 1 || n_couplings > 128 ||
       pass_len < 2 || pass_len > 128 || max_passes < 1 || max_passes > 64 || !(tol > 0))
     return QKRYLOV_ERROR_INVALID_ARG;
   if (h0->op->dim() != h1->op->dim() || !h0->op->all_real() || !h1->op->all_real()) return QKRYLOV_ERROR_INVALID_ARG;
+  if (net && (!net->net || net->net->dim() != h0->op->dim())) return QKRYLOV_ERROR_INVALID_ARG;
   return guarded([&] {
     const std::vector<double> g(couplings, couplings + n_couplings);
-    auto r = qkb::lanczos_sweep(*h0->op, *h1->op, g, pass_len, max_passes, tol, seed);
+    auto r = qkb::lanczos_sweep(*h0->op, *h1->op, g, pass_len, max_passes, tol, seed, net ? net->net.get() : nullptr);
     for (int q = 0; q < n_couplings; ++q) {
       energies[q] = r.energies[q];
       if (residuals) residuals[q] = r.residuals[q];
@@ -512,6 +514,7 @@ int qkrylov_b200_lanczos_sweep(qkrylov_hamiltonian_h h0, qkrylov_hamiltonian_h h
       info->applies = r.applies;
       info->lanes_per_row = r.lanes_per_row;
       info->seconds = r.seconds;
+      info->seconds_inference = r.seconds_inference;
     }
     return QKRYLOV_SUCCESS;
   });

@@ -140,10 +140,13 @@ struct SweepOut {
   std::vector<double> energies, residuals;
   std::vector<int> converged;
   int R = 0, steps = 0, passes = 0, applies = 0, reorths = 0, lanes_per_row = 0;
-  double seconds = 0;
+  double seconds = 0, seconds_inference = 0;
 };
+class WarmStartNet;
+// net: NULL for seeded random starts, or a warm-start network on the same
+// basis whose coupling input is g (its start vector at each coupling)
 SweepOut lanczos_sweep(const Operator& H0, const Operator& H1, const std::vector<double>& couplings, int pass_len,
-                       int max_passes, double tol, uint64_t seed);
+                       int max_passes, double tol, uint64_t seed, WarmStartNet* net);
 
 // src/solvers/dynamics.cpp:12-59
 template <class Real>

@@ -30,6 +30,7 @@
 
 #include "dense.hpp"
 #include "solvers.hpp"
+#include "warmstart.hpp"
 
 namespace qkb {
 
@@ -43,7 +44,7 @@ double wall_s() {
 }  // namespace
 
 SweepOut lanczos_sweep(const Operator& H0, const Operator& H1, const std::vector<double>& couplings, int pass_len,
-                       int max_passes, double tol, uint64_t seed) {
+                       int max_passes, double tol, uint64_t seed, WarmStartNet* net) {
   const int nc = int(couplings.size());
   if (nc < 1 || nc > 128) throw std::invalid_argument("qkrylov_b200: 1 to 128 couplings");
   if (pass_len < 2 || pass_len > 128) throw std::invalid_argument("qkrylov_b200: pass_len must be in [2, 128]");
@@ -52,6 +53,8 @@ SweepOut lanczos_sweep(const Operator& H0, const Operator& H1, const std::vector
   if (H0.dim() != H1.dim() || H0.device() != H1.device())
     throw std::invalid_argument("qkrylov_b200: H0 and H1 must share the basis and the device");
   if (!H0.all_real() || !H1.all_real()) throw std::invalid_argument("qkrylov_b200: the sweep needs real operators");
+  if (net && (net->dim() != H0.dim() || net->device() != H0.device()))
+    throw std::invalid_argument("qkrylov_b200: the network's basis does not match the operators");
   const double t0 = wall_s();
   const int R = nc <= 32 ? 32 : nc <= 64 ? 64 : 128;
   const qk_dtype t = QK_F64;
@@ -104,6 +107,18 @@ SweepOut lanczos_sweep(const Operator& H0, const Operator& H1, const std::vector
     qkd_check(qkd_block_scale(t, n, R, nd, X, bd, ld, 0, c.stream), "scale");
   };
   qkd_check(qkd_random(t, n * R, seed, 0, psi.data(), c.stream), "random");
+  if (net) {
+    // learned start vectors: the network's prediction at each coupling
+    // (inference included in the run time); padding columns keep random starts
+    const double ti = wall_s();
+    DevVec phi(n, QK_F32, dev, false);
+    for (int col = 0; col < nc; ++col) {
+      net->start_vector(couplings[col], static_cast<float*>(phi.data()));
+      qkd_check(qkd_block_put_column(QK_F32, phi.data(), n, R, col, t, psi.data(), c.stream), "start column");
+    }
+    c.sync();
+    out.seconds_inference = wall_s() - ti;
+  }
   normalise(psi.data());
   qk_plan* p0 = const_cast<qk_plan*>(H0.plan());
   qk_plan* p1 = const_cast<qk_plan*>(H1.plan());

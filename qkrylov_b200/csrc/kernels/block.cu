@@ -306,6 +306,14 @@ k_block_axpy_cols(size_t n, int R, const double* __restrict__ g, const E* __rest
   column_partial(acc, R, 0, red, partials);
 }
 
+// column c of a row-interleaved block (element type Ed) from a vector of
+// n elements (type Es)
+template <class Es, class Ed>
+__global__ void k_block_put_column(size_t n, int R, const Es* __restrict__ src, int c, Ed* dst) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    dst[i * size_t(R) + c] = Ed(src[i]);
+}
+
 // out[2 o] = sum_b partials[o * G + b] (lanes stride over b, then a warp
 // sum), out[2 o + 1] = 0; one warp per output
 __global__ void k_sweep_reduce(const double* __restrict__ partials, int G, int nout, double* out) {
@@ -373,6 +381,23 @@ int qkd_block_axpy_cols(qk_dtype t, size_t n, int R, const double* g, const void
                                                                 static_cast<const E*>(X), partials)));
   QKD_LAUNCH_CHECK();
   return sweep_finish(partials, G, R, dots, s);
+}
+
+int qkd_block_put_column(qk_dtype ts, const void* src, size_t n, int R, int c, qk_dtype td, void* dst,
+                         cudaStream_t s) {
+  if (!src || !dst || R <= 0 || c < 0 || c >= R) return QKD_EINVAL;
+  if (n == 0) return QKD_OK;
+  const unsigned G = block_grid(n);
+  if (ts == QK_F32 && td == QK_F64)
+    k_block_put_column<float, double><<<G, kBT, 0, s>>>(n, R, static_cast<const float*>(src), c, static_cast<double*>(dst));
+  else if (ts == QK_F64 && td == QK_F64)
+    k_block_put_column<double, double><<<G, kBT, 0, s>>>(n, R, static_cast<const double*>(src), c, static_cast<double*>(dst));
+  else if (ts == QK_F32 && td == QK_F32)
+    k_block_put_column<float, float><<<G, kBT, 0, s>>>(n, R, static_cast<const float*>(src), c, static_cast<float*>(dst));
+  else
+    return QKD_EINVAL;
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
 }
 
 #undef QKD_REAL_DISPATCH

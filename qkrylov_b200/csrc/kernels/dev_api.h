@@ -172,6 +172,10 @@ int qkd_block_column(qk_dtype t, size_t n, int R, const void* X, int c, void* ou
  *              nrm2 (may be NULL) = column norms^2 of the result
  *   axpy_cols: Y0[:, c] += g[c] Y1[:, c]; dots = <X[:, c], Y0[:, c]> */
 int qkd_block_partials_grid(size_t n, int R);
+/* Column c of the block dst (dtype td) = the n-element vector src (dtype
+ * ts); (ts, td) = (f32, f64), (f64, f64) or (f32, f32). */
+int qkd_block_put_column(qk_dtype ts, const void* src, size_t n, int R, int c, qk_dtype td, void* dst,
+                         cudaStream_t s);
 int qkd_block_mdot(qk_dtype t, size_t n, int R, int nv, const void* const* V, const void* W, double* partials,
                    size_t partials_cap, double* out, cudaStream_t s);
 int qkd_block_mcomb(qk_dtype t, size_t n, int R, int nv, const void* const* V, const double* coef, int keep, void* W,

@@ -93,3 +93,26 @@ def test_argument_checks():
     Hc = ham("spin", 10, SZ0, terms)
     with pytest.raises(ValueError):
         qk.lanczos_sweep(Hc, H1, [0.1])
+
+
+def test_sweep_from_learned_start_vectors():
+    # the warm-start network trained on a few couplings gives each column its
+    # start vector; same acceptance, fewer steps than random starts
+    N = 16
+    B = qk.SpinHalfBasis(N, sz=0)
+    net = qk.WarmStartMLP(B, seed=0)
+    for j in (0.0, 0.15, 0.3, 0.45):
+        r = qk.lanczos_fp64(ham("spin", N, SZ0, O.j1j2_chain(N, 1.0, j)), seed=1, tol=TOL, eigenvector=True)
+        net.add_target(j, r.eigenvector)
+    net.train(steps=400, batch=4096, lr=2e-3, seed=3)
+    H0 = ham("spin", N, SZ0, O.heisenberg_chain(N))
+    H1 = ham("spin", N, SZ0, nnn_terms(N))
+    g = [0.05, 0.1, 0.2, 0.25, 0.35, 0.4]
+    w = qk.lanczos_sweep(H0, H1, g, tol=TOL, net=net)
+    c = qk.lanczos_sweep(H0, H1, g, tol=TOL)
+    assert w.converged.all() and c.converged.all() and w.seconds_inference > 0 and c.seconds_inference == 0
+    assert np.max(np.abs(w.energies - c.energies)) < 1e-10
+    assert w.steps < c.steps, (w.steps, c.steps)
+    H8 = ham("spin", 8, SZ0, O.heisenberg_chain(8))
+    with pytest.raises(ValueError):
+        qk.lanczos_sweep(H8, H8, g, net=net)   # network on another basis
