@@ -76,7 +76,7 @@ SweepOut lanczos_sweep(const Operator& H0, const Operator& H1, const std::vector
   DevVec d0(n, t, dev, false), d1(n, t, dev, false);
   H0.diagonal(t, d0.data());
   H1.diagonal(t, d1.data());
-  DevVec psi(n * R, t, dev, false), W(n * R, t, dev, false), Y1(n * R, t, dev, false);
+  DevVec psi(n * R, t, dev, false), W(n * R, t, dev, false), Y1;  // Y1: H1 X when it cannot be accumulated
   std::vector<DevVec> V;
   V.reserve(size_t(m) + 1);
   PtrArray P(size_t(m) + 2, dev);
@@ -128,13 +128,24 @@ SweepOut lanczos_sweep(const Operator& H0, const Operator& H1, const std::vector
       qkd_check(qkd_tune_rows(pl, c.ws, t, R, psi.data(), W.data(), pl == p0 ? d0.data() : d1.data(), c.stream,
                               &lanes), "tune");
   out.lanes_per_row = qkd_rows_shape(p0, t, R);
-  // Y = H(g) X, dots[2 c] = <X_c, Y_c>
+  // Y = H(g) X, dots[2 c] = <X_c, Y_c>: H1 X accumulated into H0 X by the
+  // block kernel's epilogue where the plan has row tables, else applied
+  // into Y1 and added by a column axpy
+  bool fused = true;
   auto apply = [&](const void* X, void* Y, double* dots) {
     qkd_check(qkd_apply_rows(p0, c.ws, t, R, 0, X, Y, d0.data(), nullptr, c.stream), "block apply");
+    out.applies += 2;
+    if (fused) {
+      const int rc = qkd_apply_rows_acc(p1, c.ws, t, R, 0, X, Y, static_cast<const double*>(gdev.data()), dots,
+                                        c.stream);
+      if (rc == QKD_OK) return;
+      if (rc != QKD_EINVAL) qkd_check(rc, "block apply");
+      fused = false;
+    }
+    if (!Y1.data()) Y1 = DevVec(n * R, t, dev, false);
     qkd_check(qkd_apply_rows(p1, c.ws, t, R, 0, X, Y1.data(), d1.data(), nullptr, c.stream), "block apply");
     qkd_check(qkd_block_axpy_cols(t, n, R, static_cast<const double*>(gdev.data()), Y1.data(), Y, X, pd, pcap, dots,
                                   c.stream), "column axpy");
-    out.applies += 2;
   };
   // a column whose explicit residual has met tol keeps its iterate: it is
   // locked for the rest of the run (padding columns are locked from the start)

@@ -79,6 +79,11 @@ int qkd_apply_block(const qk_plan* p, qk_dtype t, int nvec, const void* X, size_
  * walking the diagonal terms.  X, Y 16-byte aligned. */
 int qkd_apply_rows(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lanes_per_row, const void* X,
                    void* Y, const void* diag, double* dots, cudaStream_t s);
+/* Y += diag(g) (H X) column by column (g: R device doubles), with dots =
+ * <X_r, Y_r> of the result, on the row-kernel tables; QKD_EINVAL for plans
+ * without them (the caller then applies into a separate block). */
+int qkd_apply_rows_acc(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lanes_per_row, const void* X,
+                       void* Y, const double* g, double* dots, cudaStream_t s);
 /* Time every valid lanes-per-row shape on X, Y (three launches each) and
  * keep the fastest for (t, R) in the plan; *chosen receives it.  Waits for
  * the stream. */

@@ -22,7 +22,7 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes);
 bool spin_plan_is_gen(const SpinHandle* h);
 int spin_plan_set_diag(SpinHandle* h, const double* diag);
 int spin_apply_block(const SpinHandle* h, qk_dtype t, int R, int lpr, const void* X, void* Y, double* dots,
-                     cudaStream_t s, qk_workspace* w);
+                     cudaStream_t s, qk_workspace* w, const double* gacc = nullptr);
 void spin_plan_destroy(SpinHandle* h);
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out);
@@ -545,6 +545,16 @@ int qkd_apply_rows(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lan
   if (t == QK_C128) return launch_block_shape<QK_C128, true>(p, w, R, lpr, X, Y, diag, dots, s);
   if (t == QK_C64) return launch_block_shape<QK_C64, true>(p, w, R, lpr, X, Y, diag, dots, s);
   return QKD_EINVAL;
+}
+
+int qkd_apply_rows_acc(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lanes_per_row, const void* X,
+                       void* Y, const double* g, double* dots, cudaStream_t s) {
+  if (!p || !w || !X || !Y || !g || X == Y || r_index(R) < 0) return QKD_EINVAL;
+  if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
+  if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
+  if (!p->spin || g_kernel_policy != 0) return QKD_EINVAL;  // row-kernel tables only
+  const int lpr = lanes_per_row ? lanes_per_row : (p->rows_lpr[t][r_index(R)] ? p->rows_lpr[t][r_index(R)] : 32);
+  return qkd::spin_apply_block(p->spin, t, R, lpr, X, Y, dots, s, w, g);
 }
 
 int qkd_rows_shape(const qk_plan* p, qk_dtype t, int R) {

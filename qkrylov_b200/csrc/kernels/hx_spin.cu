@@ -1106,7 +1106,7 @@ struct alignas(sizeof(E) * VPL) BlkPack { E v[VPL]; };
 template <int DT, bool GEN, int LPR, int VPL>
 __global__ void __launch_bounds__(256)
 k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, void* __restrict__ Y,
-                double* partials, unsigned* ticket, double* dots) {
+                double* partials, unsigned* ticket, double* dots, const double* __restrict__ gacc) {
   using T = VT<DT>;
   using R = typename T::R;
   using E = typename T::E;
@@ -1127,6 +1127,10 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
   double dr[VPL], di[VPL];
   #pragma unroll
   for (int v = 0; v < VPL; ++v) { dr[v] = 0.0; di[v] = 0.0; }
+  // gacc != NULL: Y += diag(gacc) (H X) instead of Y = H X (column c = l * VPL + v)
+  R gcol[VPL];
+  #pragma unroll
+  for (int v = 0; v < VPL; ++v) gcol[v] = gacc ? R(gacc[l * VPL + v]) : R(1);
   auto ldrow = [&](uint32_t row, R* re, R* im) {
     const Pack pk = *reinterpret_cast<const Pack*>(Xe + size_t(row) * RV + l * VPL);
     #pragma unroll
@@ -1216,6 +1220,16 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
         }
       }
       Pack yv;
+      if (gacc) {
+        const Pack y0 = *reinterpret_cast<const Pack*>(Ye + size_t(row) * RV + l * VPL);
+        #pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          R y0r, y0i;
+          sld(y0.v, v, y0r, y0i);
+          ar[v] = y0r + gcol[v] * ar[v];
+          if (T::cplx) ai[v] = y0i + gcol[v] * ai[v];
+        }
+      }
       #pragma unroll
       for (int v = 0; v < VPL; ++v) {
         T::st(yv.v, v, ar[v], ai[v]);
@@ -2009,18 +2023,19 @@ int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
 static int g_spin_variant = 6;
 
 template <int DT, bool GEN, int LPR, int VPL>
-int launch_rows_block(const SpinHandle* h, qk_workspace* w, const void* X, void* Y, double* dots, cudaStream_t s) {
+int launch_rows_block(const SpinHandle* h, qk_workspace* w, const void* X, void* Y, double* dots, cudaStream_t s,
+                      const double* gacc) {
   auto k = k_hx_rows_block<DT, GEN, LPR, VPL>;
   const unsigned g = resident_grid(k, 256, 0, std::min<unsigned>(std::max(1u, h->host.nbtiles), kMaxG));
-  k<<<g, 256, 0, s>>>(h->dev, X, Y, w->partials, w->ticket, dots ? dots : qkd_workspace_results(w));
+  k<<<g, 256, 0, s>>>(h->dev, X, Y, w->partials, w->ticket, dots ? dots : qkd_workspace_results(w), gacc);
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
 
 template <int DT, bool GEN>
 int rows_block_shape(const SpinHandle* h, qk_workspace* w, int R, int lpr, const void* X, void* Y, double* dots,
-                     cudaStream_t s) {
-#define QKD_RB(RR, L, V) if (R == RR && lpr == L) return launch_rows_block<DT, GEN, L, V>(h, w, X, Y, dots, s);
+                     cudaStream_t s, const double* gacc) {
+#define QKD_RB(RR, L, V) if (R == RR && lpr == L) return launch_rows_block<DT, GEN, L, V>(h, w, X, Y, dots, s, gacc);
   QKD_RB(32, 32, 1) QKD_RB(32, 16, 2) QKD_RB(32, 8, 4)
   QKD_RB(64, 32, 2) QKD_RB(64, 16, 4) QKD_RB(64, 8, 8)
   QKD_RB(128, 32, 4) QKD_RB(128, 16, 8)
@@ -2029,11 +2044,12 @@ int rows_block_shape(const SpinHandle* h, qk_workspace* w, int R, int lpr, const
 }
 
 // Block apply with the row-kernel tables; QKD_EINVAL when this plan has none.
+// gacc != NULL (R device doubles): Y += diag(gacc) (H X) instead of Y = H X.
 int spin_apply_block(const SpinHandle* h, qk_dtype t, int R, int lpr, const void* X, void* Y, double* dots,
-                     cudaStream_t s, qk_workspace* w) {
+                     cudaStream_t s, qk_workspace* w, const double* gacc) {
   if (!h || !h->host.rows_ok || !h->host.btiles || (h->host.gen && !h->host.diag_full)) return QKD_EINVAL;
-  if (h->host.gen) { QKD_DISPATCH(t, return rows_block_shape<DT, true>(h, w, R, lpr, X, Y, dots, s)); }
-  QKD_DISPATCH(t, return rows_block_shape<DT, false>(h, w, R, lpr, X, Y, dots, s));
+  if (h->host.gen) { QKD_DISPATCH(t, return rows_block_shape<DT, true>(h, w, R, lpr, X, Y, dots, s, gacc)); }
+  QKD_DISPATCH(t, return rows_block_shape<DT, false>(h, w, R, lpr, X, Y, dots, s, gacc));
   return QKD_EINVAL;
 }
 
