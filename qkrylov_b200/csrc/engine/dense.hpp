@@ -21,16 +21,19 @@ namespace qkb {
 
 // d <- eigenvalues of the n x n symmetric tridiagonal (alpha, beta); when z
 // is given it receives the eigenvector matrix, z[j*n + i] = component j of
-// eigenvector i.
+// eigenvector i, for the first zrows components (all n when zrows < 0).
+// Each rotation acts on every row of z independently, so the first rows
+// come out identical whether or not the others are accumulated.
 template <class Real>
 void tridiag_ql(const std::vector<Real>& alpha, const std::vector<Real>& beta, int n,
-                std::vector<Real>& d, std::vector<Real>* z) {
+                std::vector<Real>& d, std::vector<Real>* z, int zrows = -1) {
   d.assign(alpha.begin(), alpha.begin() + n);
   std::vector<Real> e(beta.begin(), beta.begin() + std::min<size_t>(beta.size(), size_t(n)));
   e.resize(n, Real(0));
+  const int zr = (zrows < 0 || zrows > n) ? n : zrows;
   if (z) {
-    z->assign(size_t(n) * n, Real(0));
-    for (int i = 0; i < n; ++i) (*z)[size_t(i) * n + i] = Real(1);
+    z->assign(size_t(zr) * n, Real(0));
+    for (int i = 0; i < zr; ++i) (*z)[size_t(i) * n + i] = Real(1);
   }
   for (int iter = 0; iter < 1000; ++iter) {
     for (int i = 0; i < n - 1; ++i)
@@ -58,7 +61,7 @@ void tridiag_ql(const std::vector<Real>& alpha, const std::vector<Real>& beta, i
       d[i + 1] = st * h - ct * k;
       if (z) {
         Real* Z = z->data();
-        for (int j = 0; j < n; ++j) {
+        for (int j = 0; j < zr; ++j) {
           const Real z1 = Z[size_t(j) * n + i], z2 = Z[size_t(j) * n + i + 1];
           Z[size_t(j) * n + i] = ct * z1 + st * z2;
           Z[size_t(j) * n + i + 1] = st * z1 - ct * z2;
@@ -95,7 +98,7 @@ void tridiag_first(const std::vector<Real>& alpha, const std::vector<Real>& beta
   if (n == 0) return;
   if (n == 1) { evals = {alpha[0]}; first = {Real(1)}; return; }
   std::vector<Real> d, z;
-  tridiag_ql(alpha, beta, n, d, &z);
+  tridiag_ql(alpha, beta, n, d, &z, 1);  // the first components only
   evals = d;
   first.assign(z.begin(), z.begin() + n);
 }
