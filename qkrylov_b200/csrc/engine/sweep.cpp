@@ -123,10 +123,13 @@ SweepOut lanczos_sweep(const Operator& H0, const Operator& H1, const std::vector
   qk_plan* p0 = const_cast<qk_plan*>(H0.plan());
   qk_plan* p1 = const_cast<qk_plan*>(H1.plan());
   int lanes = 0;
-  for (qk_plan* pl : {p0, p1})
-    if (!qkd_rows_shape(pl, t, R))
-      qkd_check(qkd_tune_rows(pl, c.ws, t, R, psi.data(), W.data(), pl == p0 ? d0.data() : d1.data(), c.stream,
-                              &lanes), "tune");
+  if (!qkd_rows_shape(p0, t, R))
+    qkd_check(qkd_tune_rows(p0, c.ws, t, R, psi.data(), W.data(), d0.data(), c.stream, &lanes), "tune");
+  if (!qkd_rows_shape(p1, t, R)) {  // H1 runs in the accumulating form where its plan has row tables
+    const int rc = qkd_tune_rows_acc(p1, c.ws, t, R, psi.data(), W.data(), static_cast<const double*>(gdev.data()),
+                                     c.stream, &lanes);
+    if (rc != QKD_OK) qkd_check(qkd_tune_rows(p1, c.ws, t, R, psi.data(), W.data(), d1.data(), c.stream, &lanes), "tune");
+  }
   out.lanes_per_row = qkd_rows_shape(p0, t, R);
   // Y = H(g) X, dots[2 c] = <X_c, Y_c>: H1 X accumulated into H0 X by the
   // block kernel's epilogue where the plan has row tables, else applied

@@ -89,6 +89,9 @@ int qkd_apply_rows_acc(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int
  * the stream. */
 int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, const void* diag,
                   cudaStream_t s, int* chosen);
+/* The same for the accumulating form qkd_apply_rows_acc (Y is scratch). */
+int qkd_tune_rows_acc(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, const double* g,
+                      cudaStream_t s, int* chosen);
 /* The tuned lanes per row for (t, R), 0 before tuning. */
 int qkd_rows_shape(const qk_plan* p, qk_dtype t, int R);
 /* diag[i] = <i|H|i> as dtype t. */

@@ -562,41 +562,57 @@ int qkd_rows_shape(const qk_plan* p, qk_dtype t, int R) {
   return p->rows_lpr[t][r_index(R)];
 }
 
-int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, const void* diag,
-                  cudaStream_t s, int* chosen) {
+// Times every valid lanes-per-row shape launch by launch, in two
+// interleaved rounds of three launches; the fastest single launch decides
+// (robust to clock drift and to a slow first round).  g != NULL tunes the
+// accumulating form Y += diag(g) H X.
+static int tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, const void* diag,
+                     const double* g, cudaStream_t s, int* chosen) {
   if (!p || !w || r_index(R) < 0 || t < QK_C128 || t > QK_F32) return QKD_EINVAL;
+  auto launch = [&](int lpr) {
+    return g ? qkd_apply_rows_acc(p, w, t, R, lpr, X, Y, g, nullptr, s)
+             : qkd_apply_rows(p, w, t, R, lpr, X, Y, diag, nullptr, s);
+  };
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return QKD_ECUDA;
-  // every shape timed launch by launch, in two interleaved rounds of three
-  // launches; the fastest single launch decides (robust to clock drift and
-  // to a slow first round)
   const int shapes[3] = {32, 16, 8};
   float fastest[3] = {1e30f, 1e30f, 1e30f};
   for (int round = 0; round < 2; ++round)
     for (int q = 0; q < 3; ++q) {
       const int lpr = shapes[q];
       if (R / lpr > 8) continue;
-      if (round == 0 && qkd_apply_rows(p, w, t, R, lpr, X, Y, diag, nullptr, s) != QKD_OK) continue;  // warm-up
+      if (round == 0 && launch(lpr) != QKD_OK) continue;  // warm-up
       for (int i = 0; i < 3; ++i) {
         cudaEventRecord(e0, s);
-        if (qkd_apply_rows(p, w, t, R, lpr, X, Y, diag, nullptr, s) != QKD_OK) break;
+        if (launch(lpr) != QKD_OK) break;
         cudaEventRecord(e1, s);
         float ms = 0.f;
         if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) break;
         fastest[q] = std::min(fastest[q], ms);
       }
     }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  (void)cudaGetLastError();
   float best = 1e30f;
   int pick = 0;
   for (int q = 0; q < 3; ++q)
     if (fastest[q] < best) { best = fastest[q]; pick = shapes[q]; }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  (void)cudaGetLastError();
   if (!pick) return QKD_ECUDA;
   p->rows_lpr[t][r_index(R)] = pick;
   if (chosen) *chosen = pick;
   return QKD_OK;
+}
+
+int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, const void* diag,
+                  cudaStream_t s, int* chosen) {
+  return tune_rows(p, w, t, R, X, Y, diag, nullptr, s, chosen);
+}
+
+int qkd_tune_rows_acc(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, const double* g,
+                      cudaStream_t s, int* chosen) {
+  if (!g) return QKD_EINVAL;
+  return tune_rows(p, w, t, R, X, Y, nullptr, g, s, chosen);
 }
 
 int qkd_diagonal(const qk_plan* p, qk_dtype t, void* diag, cudaStream_t s) {
