@@ -118,9 +118,10 @@ FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t se
 FtlmBlockOut ftlm_loop(const Operator& H, qk_dtype t, int R, int M, uint64_t seed, const std::vector<double>& temps,
                        int nvec);
 
-// Block Davidson (SURVEY configuration: k eigenpairs, block of corrections,
-// diagonal preconditioner, bounded subspace, seeded random block start) for
-// real operators on float32 / float64 vectors, storing only the basis.
+// Block Davidson (k eigenpairs, a block of corrections per iteration,
+// diagonal preconditioner, bounded subspace, seeded random block start; the
+// form used for Hubbard 4x4 with k = 4, block 8, subspace 64) for real
+// operators on float32 / float64 vectors, storing only the basis.
 struct DavidsonBlockOut {
   std::vector<double> eigenvalues, residuals;
   int iterations = 0, applies = 0, restarts = 0;
