@@ -25,7 +25,7 @@ tables, term tables and repeated gathers are not counted).
 
 cpu_baseline  the reference's own CPU H.x (oracle/_ref) at N=24; with the
          solver legs also its Lanczos (Heisenberg N=22) and FTLM (t-J N=14,
-         one temperature) beside this build's GPU solvers on the same models
+         one temperature) beside the library's GPU solvers on the same models
 
 --impl reference times the reference's own CPU implementation (its
 unchanged sources, oracle/_ref, OpenMP on all host cores) on a bounded
@@ -193,7 +193,7 @@ def cpu_reference_gbs(N=24, steps=3, use_ref=True):
 
 def cpu_reference_solvers(qk, N=22, tj_N=14, R=64, M=100):
     """The reference's own CPU solvers (its unchanged sources, oracle/_ref,
-    all host threads) beside this build's GPU solvers on the same models at
+    all host threads) beside the library's GPU solvers on the same models at
     sizes the CPU finishes in seconds:
       lanczos  Heisenberg chain N, Sz=0: lanczos_ground_state(maxiter 200,
                tol 1e-12), the reference's start vector on both sides

@@ -1,5 +1,5 @@
 // Device selection (the same struct as qkrylov's include/qkrylov/core/device.hpp:27-80):
-// "cuda:1", "gpu:0", "gpu" or an integer id.  This build always targets
+// "cuda:1", "gpu:0", "gpu" or an integer id.  This library always targets
 // CUDA GPUs; "cpu" selects device 0, since there is no CPU back-end.
 #pragma once
 
