@@ -156,6 +156,66 @@ def tj_opsum(qk, N, t, J):
     return os_
 
 
+def hubbard_opsum(qk, Lx, Ly, t, U):
+    """Periodic Lx x Ly Hubbard model, site = x + Lx*y: directed hops -t
+    c+_i c_j written annihilator first (both spins, both directions of each
+    bond, x and y bonds), then U Nupdn on every site."""
+    os_ = qk.OpSum(dtype=np.float64)
+    for y in range(Ly):
+        for x in range(Lx):
+            i = x + Lx * y
+            for j in sorted({(x + 1) % Lx + Lx * y, x + Lx * ((y + 1) % Ly)} - {i}):
+                for (a, b) in ((i, j), (j, i)):
+                    os_.add_term(-t, "CUp", b, "CdagUp", a)
+                    os_.add_term(-t, "CDn", b, "CdagDn", a)
+    for i in range(Lx * Ly):
+        os_.add_term(U, "Nupdn", i)
+    return os_
+
+
+def hubbard_c3(qk, tol_lanczos=1e-10, tol_davidson=1e-6, davidson_iters=100):
+    """Fermi-Hubbard 4x4 torus, t=1, U=4, 8 up + 8 down (dim 165,636,900):
+    H.x (float64) timing, the mixed-precision Lanczos ground state to the
+    explicit residual tol_lanczos, and block Davidson for the 4 lowest
+    eigenpairs (block 8, diagonal preconditioner, subspace 64, FP64 vectors,
+    seeded random start)."""
+    import torch
+    B = qk.HubbardBasis(16, nup=8, ndn=8)
+    t0 = time.perf_counter()
+    H = qk.MatrixFreeHamiltonian(B, qk.HubbardSite(), hubbard_opsum(qk, 4, 4, 1.0, 4.0), dtype=np.float64)
+    setup = time.perf_counter() - t0
+    D = H.dimension
+    x = torch.randn(D, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    for _ in range(3):
+        H.apply_device(x.data_ptr(), y.data_ptr(), qk.DTYPE_F64)
+    stream = torch.cuda.ExternalStream(H.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(10):
+        H.apply_device(x.data_ptr(), y.data_ptr(), qk.DTYPE_F64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    del x, y
+    torch.cuda.empty_cache()
+    out = {"workload": "hubbard_4x4_U4_8up8dn", "dim": D, "setup_seconds": setup, "kernel": H.kernel,
+           "hx_f64_ms": ms, "hx_f64_GBs_effective": D * 16 / (ms * 1e-3) / 1e9}
+    t0 = time.perf_counter()
+    r = qk.lanczos_mixed(H, seed=1, tol=tol_lanczos)
+    out["lanczos_mixed"] = {"seconds": time.perf_counter() - t0, "energy": r.energy, "residual": r.residual,
+                            "converged": r.converged, "iterations_fp32": r.iterations_low,
+                            "iterations_fp64": r.iterations_high}
+    t0 = time.perf_counter()
+    d = qk.davidson_block(H, n_eig=4, block=8, max_subspace=64, tol=tol_davidson, seed=1, maxiter=davidson_iters,
+                          precision=64)
+    out["davidson_block"] = {"seconds": time.perf_counter() - t0, "eigenvalues": [float(v) for v in d.eigenvalues],
+                             "residuals": [float(v) for v in d.residuals], "iterations": d.iterations,
+                             "applies": d.applies, "restarts": d.restarts, "converged": d.converged, "tol": tol_davidson}
+    return out
+
+
 def heisenberg_opsum(qk, N, dtype):
     os_ = qk.OpSum(dtype=dtype)
     for i in range(N):
@@ -532,6 +592,12 @@ def run_b200(args):
         return ms, launches
 
     peak, peak_kind = peaks()
+    if args.hubbard:
+        if rank == 0:
+            print(json.dumps({"hubbard_only": True, **hubbard_c3(qk)}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.sweep_only:
         if rank == 0:
             print(json.dumps({"sweep_only": True, **coupling_sweep(qk, N=args.n, sequential=False)}), flush=True)
@@ -652,6 +718,8 @@ def main():
     ap.add_argument("--kernel-dtype", default="c128", choices=["c128", "c64", "f64", "f32"],
                     help="vector type of --kernel-only")
     ap.add_argument("--policy", default="auto", help="H.x kernel policy of --kernel-only (qkrylov_b200.set_kernel_policy)")
+    ap.add_argument("--hubbard", action="store_true",
+                    help="only the Hubbard 4x4 (8 up, 8 down) H.x, mixed-precision Lanczos and block Davidson")
     ap.add_argument("--sweep-only", action="store_true",
                     help="only the batched coupling sweep on the J1-J2 chain of --n sites (no one-at-a-time runs)")
     args = ap.parse_args()
