@@ -116,3 +116,19 @@ def test_sweep_from_learned_start_vectors():
     H8 = ham("spin", 8, SZ0, O.heisenberg_chain(8))
     with pytest.raises(ValueError):
         qk.lanczos_sweep(H8, H8, g, net=net)   # network on another basis
+
+
+def test_transverse_field_ising_sweep():
+    # single-spin flips on the full basis (no conserved charge): whichever
+    # H.X path the plans take, the sweep matches one-at-a-time Lanczos
+    N = 10
+    full = dict(use_sz=0)
+    zz = [(-1.0, [("Sz", i), ("Sz", (i + 1) % N)]) for i in range(N)]
+    x = [(-1.0, [("Sx", i)]) for i in range(N)]
+    H0, H1 = ham("spin", N, full, zz), ham("spin", N, full, x)
+    g = [0.6, 0.8, 1.0, 1.2, 1.6, 2.0]   # away from the near-degenerate ordered pair at small g
+    r = qk.lanczos_sweep(H0, H1, g, tol=TOL)
+    assert r.converged.all()
+    for q, gq in enumerate(g):
+        ref = qk.lanczos_fp64(ham("spin", N, full, zz + [(c * gq, f) for c, f in x]), seed=2, tol=TOL)
+        assert abs(r.energies[q] - ref.energy) < 1e-10, (gq, r.energies[q], ref.energy)
