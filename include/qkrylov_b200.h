@@ -269,6 +269,25 @@ int qkrylov_b200_ftlm_loop(qkrylov_hamiltonian_h h, int precision, int n_random,
  *   loss = (o0 - a)^2 + c_sign * softplus(-y o1).
  * Parameters (FP32): W1 [128][nsites+1], W2 [128][128], W3 [2][128], b1,
  * b2, b3 (20,098 values for 24 sites). */
+/* ------------------------------------------------- block continued fraction
+ * qkrylov's continued_fraction_coeffs (dynamics.cpp:12-59: normalise phi0,
+ * three-term Lanczos without reorthogonalisation, stop at beta < 1e-15) for
+ * n_vectors (32, 64 or 128) start vectors at once, e.g. Sz(q)|psi0> for
+ * every momentum q: one block H.X with fused column dots and one column
+ * recurrence per step, the n_steps (1..1000) steps captured as one CUDA
+ * graph when use_graph.  start: row-interleaved dimension() x n_vectors
+ * block (element (i, r) at i * n_vectors + r; float for precision 32,
+ * double for 64; complex interleaved for complex operators, or for real
+ * ones when complex_vectors != 0), in device memory when start_on_device,
+ * else host memory; zero columns give empty fractions.  alphas, betas: n_vectors x n_steps doubles (vector r at
+ * r * n_steps; betas[k] is the beta computed at step k); norms: |start_r|
+ * (may be NULL); lengths: steps per vector, the last being the one whose
+ * beta fell below 1e-15 when the recurrence stopped early (may be NULL).
+ * No counterpart in the reference, which runs one start vector per call. */
+int qkrylov_b200_cf_block(qkrylov_hamiltonian_h h, int precision, int complex_vectors, int n_vectors, int n_steps,
+                          const void* start, int start_on_device, int use_graph, double* alphas, double* betas,
+                          double* norms, int* lengths, qkrylov_b200_ftlm_info_t* info);
+
 typedef struct qkrylov_b200_mlp_t* qkrylov_b200_mlp_h;
 
 qkrylov_b200_mlp_h qkrylov_b200_mlp_create(qkrylov_basis_h basis, int device, uint64_t seed);

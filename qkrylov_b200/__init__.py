@@ -781,6 +781,51 @@ def continued_fraction_coeffs(H: MatrixFreeHamiltonian, phi0: np.ndarray, n_iter
     return DynamicsResult(a[:n].copy(), b[:max(n - 1, 0)].copy(), nrm.value)
 
 
+def cf_block(H: MatrixFreeHamiltonian, start, n_steps: int = 100, precision: int = 64, graph: bool = True,
+             n_vectors: Optional[int] = None, complex_vectors: bool = False) -> List[DynamicsResult]:
+    """continued_fraction_coeffs for many start vectors at once (one block
+    of three-term recurrences on the GPU).  start: a host array of shape
+    (dimension, k) (k <= 128 columns; padded with zero columns to a block of
+    32, 64 or 128; a complex array selects complex vectors), or a device
+    pointer (int) to a row-interleaved block of n_vectors columns (complex
+    when complex_vectors or the operator is complex).  Returns one
+    DynamicsResult per column."""
+    L = lib()
+    if not isinstance(start, int) and np.iscomplexobj(start):
+        complex_vectors = True
+    real = H.all_real and not complex_vectors
+    if isinstance(start, int):
+        if n_vectors not in (32, 64, 128):
+            raise ValueError("n_vectors must be 32, 64 or 128 for a device start block")
+        R, k, ptr, keep = n_vectors, n_vectors, start, None
+        on_dev = 1
+    else:
+        a = np.asarray(start)
+        if a.ndim != 2 or a.shape[0] != H.dimension or not 1 <= a.shape[1] <= 128:
+            raise ValueError("start must have shape (dimension, k) with 1 <= k <= 128")
+        k = a.shape[1]
+        R = 32 if k <= 32 else 64 if k <= 64 else 128
+        dt = (np.float32 if precision == 32 else np.float64) if real else \
+            (np.complex64 if precision == 32 else np.complex128)
+        keep = np.zeros((H.dimension, R), dtype=dt)
+        keep[:, :k] = a
+        ptr, on_dev = keep.ctypes.data, 0
+    al, be = np.zeros((R, n_steps)), np.zeros((R, n_steps))
+    nr, ln = np.zeros(R), np.zeros(R, dtype=np.int32)
+    info = _FTLMInfo()
+    _check(L.qkrylov_b200_cf_block(H._h, precision, int(complex_vectors), R, n_steps, ptr, on_dev, int(graph), al.ctypes.data,
+                                   be.ctypes.data, nr.ctypes.data, ln.ctypes.data, ctypes.byref(info)), "cf_block")
+    out = []
+    for r in range(k):
+        if nr[r] < 1e-15:  # the reference returns an empty fraction for a zero start vector
+            out.append(DynamicsResult(np.zeros(0), np.zeros(0), 0.0))
+            continue
+        n = int(ln[r])
+        nb = n if (n == n_steps and be[r, n - 1] >= 1e-15) else n - 1
+        out.append(DynamicsResult(al[r, :n].copy(), be[r, :max(nb, 0)].copy(), float(nr[r])))
+    return out
+
+
 def evaluate_spectral_function(res: DynamicsResult, omega: float, E0: float, eta: float = 0.1) -> float:
     a = np.ascontiguousarray(res.alphas, dtype=np.float64)
     b = np.ascontiguousarray(res.betas, dtype=np.float64)

@@ -112,6 +112,7 @@ PROTOTYPES = {
     "qkrylov_b200_mlp_loss_grad": (_i, [_vp, _i, _vp, _vp, _vp, _d, _vp, _vp]),
     "qkrylov_b200_lanczos_warm": (_i, [_vp, _vp, _d, _i, _d, _vp, _vp]),
     "qkrylov_b200_davidson_block": (_i, [_vp, _i, _i, _i, _i, _d, _u64, _i, _vp, _vp, _vp, _vp]),
+    "qkrylov_b200_cf_block": (_i, [_vp, _i, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "qkrylov_b200_lanczos_sweep": (_i, [_vp, _vp, _i, _vp, _i, _i, _d, _u64, _vp, _vp, _vp, _vp, _vp]),
 }
 

@@ -346,6 +346,46 @@ int qkrylov_b200_ftlm_block(qkrylov_hamiltonian_h h, int precision, int n_random
   return ftlm_common(h, true, precision, n_random, n_steps, seed, 0, n_temps, temps, logZ, U, Cv, use_graph, info);
 }
 
+int qkrylov_b200_cf_block(qkrylov_hamiltonian_h h, int precision, int complex_vectors, int n_vectors, int n_steps,
+                          const void* start, int start_on_device, int use_graph, double* alphas, double* betas,
+                          double* norms, int* lengths, qkrylov_b200_ftlm_info_t* info) {
+  if (!h || !h->op || (precision != 32 && precision != 64) || !start || !alphas || !betas ||
+      (n_vectors != 32 && n_vectors != 64 && n_vectors != 128) || n_steps < 1 || n_steps > 1000)
+    return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const qkb::Operator& H = *h->op;
+    const bool real = H.all_real() && !complex_vectors;
+    const qk_dtype t = precision == 32 ? (real ? QK_F32 : QK_C64) : (real ? QK_F64 : QK_C128);
+    const size_t count = size_t(H.dim()) * n_vectors;
+    qkb::DevVec staged;
+    const void* dstart = start;
+    if (!start_on_device) {
+      qkb::Context& c = H.ctx();
+      c.activate();
+      staged = qkb::DevVec(count, t, H.device(), false);
+      qkb::cuda_check(cudaMemcpyAsync(staged.data(), start, staged.bytes(), cudaMemcpyHostToDevice, c.stream), "H2D");
+      dstart = staged.data();
+    }
+    auto r = qkb::cf_block(H, t, n_vectors, n_steps, dstart, use_graph != 0);
+    std::copy(r.alphas.begin(), r.alphas.end(), alphas);
+    std::copy(r.betas.begin(), r.betas.end(), betas);
+    for (int q = 0; q < n_vectors; ++q) {
+      if (norms) norms[q] = std::sqrt(r.norm2[q]);
+      if (lengths) lengths[q] = r.len[q];
+    }
+    if (info) {
+      info->seconds = r.seconds;
+      info->seconds_device = r.seconds_device;
+      info->e_min = 0.0;
+      info->lanes_per_row = r.lanes_per_row;
+      info->graph = r.graph;
+      info->vectors = r.R;
+      info->steps = r.M;
+    }
+    return QKRYLOV_SUCCESS;
+  });
+}
+
 int qkrylov_b200_ftlm_loop(qkrylov_hamiltonian_h h, int precision, int n_random, int n_steps, uint64_t seed,
                            int n_vectors, int n_temps, const double* temps, double* logZ, double* U, double* Cv,
                            qkrylov_b200_ftlm_info_t* info) {

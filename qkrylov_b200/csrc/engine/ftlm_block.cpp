@@ -58,20 +58,19 @@ void thermo(FtlmBlockOut& out, const std::vector<double>& temps) {
 }
 }  // namespace
 
-FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t seed, const std::vector<double>& temps,
-                        bool use_graph) {
-  if (R != 32 && R != 64 && R != 128) throw std::invalid_argument("qkrylov_b200: block size must be 32, 64 or 128");
-  if (M < 1 || M > 1000) throw std::invalid_argument("qkrylov_b200: n_steps must be in [1, 1000]");
-  if (!qk_dtype_complex(t) && !H.all_real()) throw std::invalid_argument("qkrylov_b200: complex operator needs complex vectors");
-  for (double T : temps) if (!(T > 0)) throw std::invalid_argument("qkrylov_b200: temperatures must be positive");
-  const double t0 = wall();
-  FtlmBlockOut out;
+// R three-term Lanczos recurrences (no reorthogonalisation) from the
+// columns of B0 (row-interleaved, dtype t, unnormalised; overwritten): M
+// steps of block H.X with fused column dots and one column recurrence,
+// captured once as a CUDA graph when use_graph.  Fills out.R, M, alphas,
+// betas, len, norm2 (|column|^2 of B0), lanes_per_row, graph and
+// seconds_device.
+static void block_recurrence(const Operator& H, qk_dtype t, int R, int M, DevVec& B0, bool use_graph,
+                             FtlmBlockOut& out) {
   out.R = R; out.M = M;
   const uint64_t n = H.dim();
   Context& c = H.ctx();
-  c.activate();
   const int dev = H.device();
-  DevVec B0(n * R, t, dev, false), B1(n * R, t, dev, false), B2(n * R, t, dev, false);
+  DevVec B1(n * R, t, dev, false), B2(n * R, t, dev, false);
   DevVec* B[3] = {&B0, &B1, &B2};
   DevVec dots(size_t(M) * 2 * R, QK_F64, dev), alpha(size_t(M) * R, QK_F64, dev), beta(size_t(M) * R, QK_F64, dev),
       scale(size_t(M + 1) * R, QK_F64, dev), nrm(2 * size_t(R), QK_F64, dev), diag(n, t, dev, false);
@@ -85,10 +84,9 @@ FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t se
   double* nd = static_cast<double*>(nrm.data());
   int* ld = static_cast<int*>(len.data());
   // H's diagonal once (the block apply reads it instead of walking the
-  // diagonal terms); Rademacher start block and its column norms.  The
-  // vectors stay unnormalised: v_k = s_k U_k.
+  // diagonal terms); column norms of the start block.  The vectors stay
+  // unnormalised: v_k = s_k U_k.
   H.diagonal(t, diag.data());
-  qkd_check(qkd_random(t, n * R, seed, 1, B0.data(), c.stream), "random");
   qkd_check(qkd_block_update(c.ws, t, n, R, nullptr, nullptr, nullptr, nullptr, B0.data(), nd, c.stream), "norms");
   const double* n2 = c.fetch(nd, 2 * R);
   out.norm2.resize(R);
@@ -157,7 +155,38 @@ FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t se
       out.alphas[size_t(r) * M + k] = ha[size_t(k) * R + r];
       out.betas[size_t(r) * M + k] = hb[size_t(k) * R + r];
     }
+}
+
+FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t seed, const std::vector<double>& temps,
+                        bool use_graph) {
+  if (R != 32 && R != 64 && R != 128) throw std::invalid_argument("qkrylov_b200: block size must be 32, 64 or 128");
+  if (M < 1 || M > 1000) throw std::invalid_argument("qkrylov_b200: n_steps must be in [1, 1000]");
+  if (!qk_dtype_complex(t) && !H.all_real()) throw std::invalid_argument("qkrylov_b200: complex operator needs complex vectors");
+  for (double T : temps) if (!(T > 0)) throw std::invalid_argument("qkrylov_b200: temperatures must be positive");
+  const double t0 = wall();
+  FtlmBlockOut out;
+  Context& c = H.ctx();
+  c.activate();
+  DevVec B0(H.dim() * R, t, H.device(), false);
+  qkd_check(qkd_random(t, H.dim() * R, seed, 1, B0.data(), c.stream), "random");  // Rademacher start block
+  block_recurrence(H, t, R, M, B0, use_graph, out);
   thermo(out, temps);
+  out.seconds = wall() - t0;
+  return out;
+}
+
+FtlmBlockOut cf_block(const Operator& H, qk_dtype t, int R, int M, const void* start, bool use_graph) {
+  if (R != 32 && R != 64 && R != 128) throw std::invalid_argument("qkrylov_b200: block size must be 32, 64 or 128");
+  if (M < 1 || M > 1000) throw std::invalid_argument("qkrylov_b200: n_steps must be in [1, 1000]");
+  if (!start) throw std::invalid_argument("qkrylov_b200: no start block");
+  if (!qk_dtype_complex(t) && !H.all_real()) throw std::invalid_argument("qkrylov_b200: complex operator needs complex vectors");
+  const double t0 = wall();
+  FtlmBlockOut out;
+  Context& c = H.ctx();
+  c.activate();
+  DevVec B0(H.dim() * R, t, H.device(), false);
+  qkd_check(qkd_copy(t, H.dim() * R, start, B0.data(), c.stream), "copy");
+  block_recurrence(H, t, R, M, B0, use_graph, out);
   out.seconds = wall() - t0;
   return out;
 }

@@ -117,6 +117,12 @@ FtlmBlockOut ftlm_block(const Operator& H, qk_dtype t, int R, int M, uint64_t se
                         bool use_graph);
 FtlmBlockOut ftlm_loop(const Operator& H, qk_dtype t, int R, int M, uint64_t seed, const std::vector<double>& temps,
                        int nvec);
+// Block continued fraction (dynamics.cpp:12-59 of qkrylov for R start
+// vectors at once): the three-term recurrence without reorthogonalisation
+// from each column of `start` (device, row-interleaved dim x R of dtype t,
+// unnormalised; copied), M steps, a column stopping at beta < 1e-15.
+// alphas / betas [r][M] of the normalised recurrences, len, norm2.
+FtlmBlockOut cf_block(const Operator& H, qk_dtype t, int R, int M, const void* start, bool use_graph);
 
 // Block Davidson (k eigenpairs, a block of corrections per iteration,
 // diagonal preconditioner, bounded subspace, seeded random block start; the
