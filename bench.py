@@ -17,7 +17,8 @@ tables, term tables and repeated gathers are not counted).
   batched_ftlm  t-J N=20 FTLM, 64 vectors x 100 steps x 200 temperatures:
          one block (FP32 / FP64 vectors, CUDA graph) vs the one-vector loop
   dynamics  S(q=pi, omega) of the same chain: ground state, phi0 =
-         Sz(pi)|psi0>, 300 continued-fraction steps, 2001 omega points
+         Sz(pi)|psi0>, 300 continued-fraction steps, 2001 omega points;
+         and at N=24 every momentum at once (block continued fraction)
   warm_start  J1-J2 N=24: network trained on 32 couplings, time-to-E0 at
          untrained couplings for plain FP64 / mixed / mixed + warm start
   coupling_sweep  J1-J2 N=24 at 32 untrained couplings: one batched block
@@ -530,6 +531,51 @@ def coupling_sweep(qk, N=24, tol=1e-10, sequential=True, net=None):
             "speedup_warm_vs_plain_fp64": seq["plain_fp64"] / warm["seconds"] if warm else None}
 
 
+def dynamics_all_momenta(qk, N=24, steps=300):
+    """S(q, omega) for every momentum q = 2 pi k / N (k = 1 .. N/2) of the
+    Heisenberg chain: the real start vectors cos- and sin-weighted
+    sum_j Sz_j |psi0> / sqrt(N) (their fractions add up to the complex
+    Sz(q)|psi0> one) as one block continued fraction (FP64 and FP32
+    vectors), against one complex continued fraction per momentum (four
+    timed, scaled to N/2)."""
+    H = qk.MatrixFreeHamiltonian(qk.SpinHalfBasis(N, sz=0), qk.SpinHalfSite(), heisenberg_opsum(qk, N, np.float64),
+                                 dtype=np.float64)
+    g = qk.lanczos_fp64(H, seed=1, tol=1e-10, eigenvector=True)
+    st = qk.SpinHalfBasis(N, sz=0).states()
+    cols, pairs = [], []
+    for k in range(1, N // 2 + 1):
+        q = 2 * np.pi * k / N
+        pair = []
+        for w in (np.cos(q * np.arange(N)), np.sin(q * np.arange(N))):
+            w[np.abs(w) < 1e-12] = 0.0
+            if not w.any():
+                continue
+            acc = np.zeros(len(st))
+            for j in range(N):
+                if w[j]:
+                    acc += w[j] * (((st >> np.uint64(j)) & np.uint64(1)).astype(np.float64) - 0.5)
+            pair.append(len(cols))
+            cols.append(g.eigenvector * acc / np.sqrt(N))
+        pairs.append(pair)
+    X = np.stack(cols, 1)
+    out = {"workload": f"heisenberg_chain_N{N}_Sz0_all_q", "momenta": N // 2, "columns": X.shape[1], "steps": steps}
+    for prec in (64, 32):
+        qk.cf_block(H, X, 20, precision=prec)  # warm-up (tile tuning)
+        t0 = time.perf_counter()
+        qk.cf_block(H, X, steps, precision=prec)
+        out[f"block_fp{prec}_seconds"] = time.perf_counter() - t0
+    qk.continued_fraction_coeffs(H, X[:, 0].astype(np.complex128), 20)  # warm-up
+    t0 = time.perf_counter()
+    for p in pairs[:4]:
+        z = X[:, p[0]] + (1j * X[:, p[1]] if len(p) > 1 else 0)
+        qk.continued_fraction_coeffs(H, z.astype(np.complex128), steps)
+    one = (time.perf_counter() - t0) / 4
+    out["one_at_a_time_seconds"] = one * (N // 2)
+    out["speedup_block_fp64"] = out["one_at_a_time_seconds"] / out["block_fp64_seconds"]
+    out["speedup_block_fp32"] = out["one_at_a_time_seconds"] / out["block_fp32_seconds"]
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -677,6 +723,7 @@ def run_b200(args):
         try:
             torch.cuda.empty_cache()
             line["dynamics"] = dynamics(qk, N)
+            line["dynamics"]["all_momenta"] = dynamics_all_momenta(qk)
         except Exception as e:
             line["dynamics"] = {"error": str(e)}
         net = None
