@@ -1013,11 +1013,30 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       for (int k = 0; k < K; ++k) {
         if (!ok[k]) continue;
         const uint32_t r = rk[k];
-        for (uint32_t e = NB; e < nh; ++e) {
-          R vr, vi;
-          T::ld(x, s_eb[e] + r, vr, vi);
-          ar[k] += s_ec[e] * vr;
-          if (T::cplx) ai[k] += s_ec[e] * vi;
+        if constexpr (K == 1) {
+          // one row per thread: the remaining high bonds four loads at a time
+          for (uint32_t e0 = NB; e0 < nh; e0 += 4) {
+            R vr[4], vi[4];
+            #pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              vr[u] = R(0);
+              vi[u] = R(0);
+              if (e0 + u < nh) T::ld(x, s_eb[e0 + u] + r, vr[u], vi[u]);
+            }
+            #pragma unroll
+            for (int u = 0; u < 4; ++u)
+              if (e0 + u < nh) {
+                ar[k] += s_ec[e0 + u] * vr[u];
+                if (T::cplx) ai[k] += s_ec[e0 + u] * vi[u];
+              }
+          }
+        } else {
+          for (uint32_t e = NB; e < nh; ++e) {
+            R vr, vi;
+            T::ld(x, s_eb[e] + r, vr, vi);
+            ar[k] += s_ec[e] * vr;
+            if (T::cplx) ai[k] += s_ec[e] * vi;
+          }
         }
         if constexpr (GEN) {
           // two-part crossing groups: up to two terms, each valid when its
