@@ -2,7 +2,7 @@
  *
  * qkrylov's own C ABI (qkrylov_c_api.h) runs in single precision.  The
  * functions here add: double-precision Hamiltonians and solvers (the
- * reference's fp64 C++ namespace, src/solvers/*.cpp compiled with
+ * reference's fp64 C++ namespace: its src/solvers sources compiled with
  * QKRYLOV_DOUBLE_PRECISION), device-pointer H.x for callers that keep
  * vectors in HBM, a multi-temperature FTLM, the OpSum compiler's output for
  * inspection, and library diagnostics.  They reuse the opaque handles of

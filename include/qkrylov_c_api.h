@@ -3,11 +3,11 @@
  * Every declaration below is the entry point of the same name in qkrylov's
  * include/qkrylov/c_api.h (the line range is given with each group), with
  * the same argument meaning, float precision, status codes and handle
- * ownership, so its FFI callers (the Julia package's ccall wrappers in
- * bindings/julia/src/*.jl) bind this library unchanged.  Differences in
- * behaviour are listed in INTEGRATION.md; the main one is that
- * qkrylov_hamiltonian_diagonal returns real diagonal entries from device
- * memory correctly on GPU builds.
+ * ownership, so its FFI callers (the Julia package's ccall wrappers under
+ * bindings/julia/src) bind this library unchanged.  The main difference in
+ * behaviour is that qkrylov_hamiltonian_diagonal returns real diagonal
+ * entries from device memory correctly on GPU builds; the others are
+ * noted at the declarations they concern.
  *
  * Extended entry points (double precision, device pointers, batched and
  * mixed-precision solvers) are in qkrylov_b200.h.
@@ -77,7 +77,13 @@ int qkrylov_opsum_add_term_nbody(qkrylov_opsum_h opsum, float coeff_real, float 
                                  const char** ops, const int* sites);
 
 /* Matrix-free Hamiltonian (c_api.h:81-100).  Vectors are host arrays of
- * dimension() complex floats. */
+ * dimension() complex floats.  Differences a caller can see: an unknown
+ * operator name, or a site whose bit would not fit a 64-bit state, makes
+ * qkrylov_hamiltonian_create return NULL (the reference fails at the first
+ * state that reaches the factor); the host-pointer applies reuse device
+ * staging buffers held by the handle, so calls on one handle are
+ * serialised; qkrylov_hamiltonian_diagonal copies the diagonal from device
+ * memory (the reference reads a device View from the host). */
 qkrylov_hamiltonian_h qkrylov_hamiltonian_create(qkrylov_basis_h basis, qkrylov_site_h site,
                                                 qkrylov_opsum_h opsum);
 void qkrylov_hamiltonian_destroy(qkrylov_hamiltonian_h h);
