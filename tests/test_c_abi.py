@@ -103,3 +103,14 @@ def test_opsum_nbody_validation():
     assert L.qkrylov_opsum_add_term_nbody(o, 0.1, 0.0, 2, bad, sites) == -1
     assert L.qkrylov_opsum_size(o) == 1
     L.qkrylov_opsum_destroy(o)
+
+
+def test_extension_entry_points_reject_bad_arguments():
+    # the batched entry points check their arguments before touching a GPU
+    L = qk.lib()
+    g = (ctypes.c_double * 2)(0.1, 0.2)
+    e = (ctypes.c_double * 2)()
+    assert L.qkrylov_b200_lanczos_sweep(None, None, 2, g, 64, 16, 1e-10, 1, None, e, None, None, None) == -1
+    assert L.qkrylov_b200_cf_block(None, 64, 0, 32, 10, g, 0, 1, e, e, None, None, None) == -1
+    assert L.qkrylov_b200_ftlm_block(None, 64, 32, 10, 1, 1, g, None, None, None, 1, None) == -1
+    assert L.qkrylov_b200_davidson_block(None, 64, 1, 8, 64, 1e-6, 1, 10, e, None, None, None) == -1
