@@ -35,8 +35,11 @@ def build_port():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def build_ref(ref_dir="/root/reference"):
-    if not os.path.isdir(ref_dir):
+def build_ref(ref_dir=None):
+    """Build oracle/_ref from a qkrylov reference checkout: ``ref_dir`` or
+    the QKRYLOV_REFERENCE environment variable (no default path)."""
+    ref_dir = ref_dir or os.environ.get("QKRYLOV_REFERENCE")
+    if not ref_dir or not os.path.isdir(ref_dir):
         return False
     subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8", f"REF={ref_dir}"], check=True)
     return True

@@ -1,7 +1,7 @@
 """Generate the golden fixtures from the qkrylov reference's own code.
 
 Runs the reference's unchanged sources (oracle/_ref/liboracle_ref.so, built
-by ``make -C oracle ref`` from the read-only reference checkout) on small
+by ``make -C oracle ref REF=<reference checkout>``) on small
 problems and writes:
 
   golden.json        scalar results, basis digests, small COO matrices
