@@ -227,9 +227,48 @@ def heisenberg_opsum(qk, N, dtype):
     return os_
 
 
-def cpu_reference_gbs(N=24, steps=3, use_ref=True):
-    """Reference CPU H.x (its CSR SpMV through the host-pointer apply) on
-    all host threads; returns GB/s on the same effective-bytes metric."""
+def mem_available_gb():
+    """Host memory available to this process (MemAvailable), in GB."""
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024 / 1e9
+    except OSError:
+        pass
+    return 0.0
+
+
+# Peak host memory of the reference's H.x set-up on the Heisenberg chain at
+# N sites, Sz=0 (its CSR build: the int32/complex128 `reserve(dim * terms)`
+# of matrix_free_hamiltonian.cpp:45-94, the final CSR and the hashed basis),
+# in GB: about 100 GB at N = 28, 25 GB at N = 26, 6 GB at N = 24.
+def reference_peak_gb(N):
+    from math import comb
+    dim = comb(N, N // 2)
+    return dim * (3 * N * 20 + 43 * 20 + 64) / 1e9
+
+
+def reference_sizes(force_n=None):
+    """Sizes of the reference arm: N = 28 (the headline configuration) when
+    its CSR fits with a 2.5x margin in the available host memory, else the
+    two largest that do among 26 and 24.  Returns (sizes, infeasible-or-None)."""
+    if force_n:
+        return [int(force_n)], None
+    mem = mem_available_gb()
+    if mem >= 2.5 * reference_peak_gb(28):
+        return [28], None
+    sizes = [n for n in (26, 24) if mem >= 2.5 * reference_peak_gb(n)] or [24]
+    return sizes, {"N": 28, "reason": f"the reference's CSR set-up needs ~{reference_peak_gb(28):.0f} GB of host "
+                   f"memory (2.5x margin: {2.5 * reference_peak_gb(28):.0f} GB), MemAvailable {mem:.0f} GB",
+                   "mem_available_gb": round(mem, 1)}
+
+
+def cpu_reference_gbs(N=24, steps=5, warmup=1, use_ref=True):
+    """Reference CPU H.x (its CSR SpMV through the host-pointer apply,
+    matrix_free_hamiltonian.cpp:173-201) on all host threads, `steps`
+    timed applies after `warmup`; returns GB/s on the same effective-bytes
+    metric (mean over the timed applies)."""
     import oracle as O
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
@@ -238,18 +277,25 @@ def cpu_reference_gbs(N=24, steps=3, use_ref=True):
     t0 = time.perf_counter()
     H = back.hamiltonian("spin", N, dict(use_sz=1, sz2=0), O.heisenberg_chain(N))
     setup = time.perf_counter() - t0
-    x = np.random.default_rng(0).standard_normal(H.dim) + 1j * np.random.default_rng(1).standard_normal(H.dim)
-    H.apply(x)
-    ts = []
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(H.dim) + 1j * rng.standard_normal(H.dim)
+    y = np.zeros_like(x)
+    for _ in range(max(1, warmup)):
+        H.apply_into(x, y)
+    t0 = time.perf_counter()
     for _ in range(steps):
-        t0 = time.perf_counter()
-        H.apply(x)
-        ts.append(time.perf_counter() - t0)
-    t = float(np.median(ts))
-    return dict(value=H.dim * 32 / t / 1e9, unit="GB/s", cores=int(os.environ.get("OMP_NUM_THREADS", threads)),
-                kind=kind, sample=f"Heisenberg N={N} Sz=0 (dim {H.dim}) complex128 H.x, median of {steps}; "
-                f"setup (basis + CSR build) {setup:.1f} s; N=28 needs ~100 GB of CSR + reserve on the host",
-                seconds_per_apply=t)
+        H.apply_into(x, y)
+    t = (time.perf_counter() - t0) / steps
+    del H
+    return dict(value=H_dim_bytes(N) / t / 1e9, unit="GB/s", cores=int(os.environ.get("OMP_NUM_THREADS", threads)),
+                kind=kind, sample=f"Heisenberg N={N} Sz=0 complex128 H.x, {steps} timed applies after {warmup}; "
+                f"setup (basis + CSR build) {setup:.1f} s",
+                seconds_per_apply=t, setup_seconds=setup, N=N)
+
+
+def H_dim_bytes(N):
+    from math import comb
+    return comb(N, N // 2) * 32
 
 
 def cpu_reference_solvers(qk, N=22, tj_N=14, R=64, M=100):
@@ -331,17 +377,24 @@ def time_to_e0(qk, N, tol=1e-10, seed=1):
                      "iterations_fp32": r.iterations_low, "iterations_fp64": r.iterations_high,
                      "restarts": r.restarts}
     out["dE_mixed_vs_plain"] = abs(out["mixed"]["energy"] - out["plain_fp64"]["energy"])
+    try:  # the independent FP64 oracle of this model: the Bethe-ansatz energy
+        from oracle import bethe
+        eb = bethe.ground_energy(N)
+        out["E0_bethe"] = eb
+        out["dE_vs_bethe"] = {k: abs(out[k]["energy"] - eb) for k in ("plain_fp64", "mixed")}
+    except Exception as e:
+        out["E0_bethe"] = {"error": str(e)}
     out["speedup_mixed"] = out["plain_fp64"]["seconds"] / out["mixed"]["seconds"]
     del H
     return out
 
 
-def batched_ftlm(qk, N=20, R=64, M=100, loop_vectors=4, seed=5):
+def batched_ftlm(qk, N=20, R=64, M=100, loop_vectors=64, seed=5):
     """Batched FTLM (R Rademacher vectors as one block, FP32 vectors, FP64
     dots, CUDA graph) vs the one-vector FP64 loop on the same vectors, on
     the periodic t-J chain (2 holes, Sz=0), 200 temperatures in [0.01, 10].
-    The loop is timed on its first `loop_vectors` vectors and scaled to R
-    (the vectors are independent and equal in cost)."""
+    The loop runs all R vectors (loop_vectors < R times the first ones and
+    scales to R; the vectors are independent and equal in cost)."""
     ne = N - 2
     B = qk.TJBasis(N, conserve_nup=True, nup=ne // 2, conserve_ndn=True, ndn=ne - ne // 2)
     H = qk.MatrixFreeHamiltonian(B, qk.TJSite(), tj_opsum(qk, N, 1.0, 0.4), dtype=np.float64)
@@ -379,7 +432,7 @@ def j1j2_opsum(qk, N, J1, J2):
     return os_
 
 
-def warm_start(qk, N=24, eval_every=16, eval_offset=4, steps=1500, batch=8192, tol=1e-10):
+def warm_start(qk, N=24, eval_every=1, eval_offset=1, steps=1500, batch=8192, tol=1e-10):
     """J1-J2 chain, Sz=0: plain FP64 Lanczos ground states at J2_k = k/255
     for k = 0, 8, ..., 248 train the warm-start network on the GPU; at the
     untrained couplings k = eval_offset, eval_offset + eval_every, ... the
@@ -425,8 +478,19 @@ def warm_start(qk, N=24, eval_every=16, eval_offset=4, steps=1500, batch=8192, t
                      "converged": all(v[1].converged for v in res.values())})
         del H
     tot = {n: sum(r["seconds"][n] for r in rows) for n in ("plain_fp64", "mixed", "mixed_warm")}
+    regimes = {}
+    for name, sel in (("J2_below_0.5", lambda j: j < 0.5), ("J2_from_0.5", lambda j: j >= 0.5)):
+        rr = [r for r in rows if sel(r["J2"])]
+        if rr:
+            t = {n: sum(r["seconds"][n] for r in rr) for n in ("plain_fp64", "mixed", "mixed_warm")}
+            regimes[name] = {"couplings": len(rr), "speedup_mixed_warm": t["plain_fp64"] / t["mixed_warm"],
+                             "speedup_mixed": t["plain_fp64"] / t["mixed"],
+                             "mean_iterations": {n: float(np.mean([r["iterations"][n] for r in rr]))
+                                                 for n in ("plain_fp64", "mixed", "mixed_warm")}}
     return net, {"workload": f"j1j2_chain_N{N}_Sz0", "dim": B.size, "train_J2": len(train_k),
-            "eval_J2": [r["J2"] for r in rows], "train_steps": steps, "batch": batch,
+            "eval_J2": {"count": len(rows), "first": rows[0]["J2"] if rows else None,
+                        "last": rows[-1]["J2"] if rows else None}, "regimes": regimes,
+            "train_steps": steps, "batch": batch,
             "train_seconds": train_s, "ground_state_seconds": gs_s, "loss_first": float(loss[:20].mean()),
             "loss_last": float(loss[-20:].mean()), "params": net.n_params,
             "total_seconds": tot, "speedup_mixed": tot["plain_fp64"] / tot["mixed"],
@@ -536,8 +600,8 @@ def dynamics_all_momenta(qk, N=24, steps=300):
     Heisenberg chain: the real start vectors cos- and sin-weighted
     sum_j Sz_j |psi0> / sqrt(N) (their fractions add up to the complex
     Sz(q)|psi0> one) as one block continued fraction (FP64 and FP32
-    vectors), against one complex continued fraction per momentum (four
-    timed, scaled to N/2)."""
+    vectors), against one complex continued fraction per momentum (all N/2
+    timed)."""
     H = qk.MatrixFreeHamiltonian(qk.SpinHalfBasis(N, sz=0), qk.SpinHalfSite(), heisenberg_opsum(qk, N, np.float64),
                                  dtype=np.float64)
     g = qk.lanczos_fp64(H, seed=1, tol=1e-10, eigenvector=True)
@@ -566,29 +630,40 @@ def dynamics_all_momenta(qk, N=24, steps=300):
         out[f"block_fp{prec}_seconds"] = time.perf_counter() - t0
     qk.continued_fraction_coeffs(H, X[:, 0].astype(np.complex128), 20)  # warm-up
     t0 = time.perf_counter()
-    for p in pairs[:4]:
+    for p in pairs:
         z = X[:, p[0]] + (1j * X[:, p[1]] if len(p) > 1 else 0)
         qk.continued_fraction_coeffs(H, z.astype(np.complex128), steps)
-    one = (time.perf_counter() - t0) / 4
-    out["one_at_a_time_seconds"] = one * (N // 2)
+    out["one_at_a_time_seconds"] = time.perf_counter() - t0
     out["speedup_block_fp64"] = out["one_at_a_time_seconds"] / out["block_fp64_seconds"]
     out["speedup_block_fp32"] = out["one_at_a_time_seconds"] / out["block_fp32_seconds"]
     return out
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU H.x (oracle/_ref, its
+    unchanged sources, OpenMP on all host threads) on the headline workload
+    where the host memory allows, else on the largest Heisenberg chains that
+    fit (the line says which and why)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cb = cpu_reference_gbs(N=24, steps=max(1, min(args.steps, 5)))
+    sizes, infeasible = reference_sizes(args.ref_n)
+    runs = [cpu_reference_gbs(N=n, steps=max(1, args.steps), warmup=max(1, args.warmup)) for n in sizes]
+    cb = runs[0]
+    same = cb["N"] == 28
     line = {"metric": "Hx effective HBM GB/s (Heisenberg N=28 Sz=0)", "value": cb["value"], "unit": "GB/s",
             "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": cb["seconds_per_apply"] * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": {"workload": "heisenberg_chain_N28_Sz0_Hx", "N": 28, "dim": 40116600,
-                       "sample_N": 24, "parallelism": "cpu-openmp"},
+                       "sample_N": cb["N"], "same_config": same, "parallelism": "cpu-openmp"},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if infeasible:
+        line["infeasible"] = infeasible
+    if len(runs) > 1:
+        line["other_samples"] = [{k: r[k] for k in ("N", "value", "seconds_per_apply", "setup_seconds")}
+                                 for r in runs[1:]]
     print(json.dumps(line), flush=True)
 
 
@@ -737,18 +812,49 @@ def run_b200(args):
             line["coupling_sweep"] = coupling_sweep(qk, net=net)
         except Exception as e:
             line["coupling_sweep"] = {"error": str(e)}
+        del net
+        try:
+            torch.cuda.empty_cache()
+            line["hubbard_c3"] = hubbard_c3(qk)
+        except Exception as e:
+            line["hubbard_c3"] = {"error": str(e)}
     if rank == 0 and not args.no_cpu_baseline:
         try:
-            cb = cpu_reference_gbs(N=24, steps=2)
+            cb = cpu_reference_gbs(N=24, steps=5)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
             if not args.no_solvers:
                 line["cpu_baseline"]["solvers"] = cpu_reference_solvers(qk)
         except Exception as e:  # reported, never silently replaced
             line["cpu_baseline"] = {"value": None, "unit": "GB/s", "error": str(e)}
     if rank == 0:
+        line["summary"] = summary(line)  # last key: the headline numbers of every leg, compactly
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def summary(line):
+    """The headline figure of each leg in a few short keys (None where a leg
+    did not run or failed)."""
+    def get(*path):
+        v = line
+        for k in path:
+            if not isinstance(v, dict) or k not in v:
+                return None
+            v = v[k]
+        return round(v, 4) if isinstance(v, float) else v
+    return {"hx_c128_frac": get("roofline", "frac"), "hx_f32_ms": get("variants", "f32", "ms_per_apply"),
+            "e2e_GBs": get("e2e", "value"),
+            "t2e0_mixed_vs_fp64": get("time_to_e0", "speedup_mixed"),
+            "dE_bethe": get("time_to_e0", "dE_vs_bethe"),
+            "ftlm_fp64_vs_loop": get("batched_ftlm", "speedup_block_fp64"),
+            "ftlm_fp32_vs_loop": get("batched_ftlm", "speedup_block_fp32"),
+            "warm_vs_fp64": get("warm_start", "speedup_mixed_warm"),
+            "sweep_vs_fp64": get("coupling_sweep", "speedup_vs_plain_fp64"),
+            "cf_all_q_vs_one": get("dynamics", "all_momenta", "speedup_block_fp64"),
+            "hubbard_hx_ms": get("hubbard_c3", "hx_f64_ms"),
+            "hubbard_davidson_ok": get("hubbard_c3", "davidson_block", "converged"),
+            "cpu_ref_GBs": get("cpu_baseline", "value")}
 
 
 def main():
@@ -758,6 +864,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=28)
+    ap.add_argument("--ref-n", type=int, default=None,
+                    help="reference arm: chain length (default: 28 when its CSR fits in host memory, else 26/24)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solvers", action="store_true", help="skip the time-to-E0 Lanczos comparison")
     ap.add_argument("--kernel-only", action="store_true",

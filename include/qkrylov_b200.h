@@ -30,12 +30,11 @@ const char* qkrylov_b200_last_error(void);
 /* Kernels launched by this library since it was loaded. */
 uint64_t qkrylov_b200_launch_count(void);
 int qkrylov_b200_device_count(void);
-/* 0 (default): H.x uses the specialised two-site exchange kernel (one CTA
- * per sector block, x of the block staged in shared memory, per-row class
- * tables) wherever the compiled operator qualifies; 1: the generic kernel
- * everywhere; 2-7: earlier exchange-kernel variants (block tiles, warp
- * tiles, batched gathers, target lists, staged blocks, block owner with
- * register row accumulators).  For comparisons; process-wide. */
+/* 0 (default): H.x uses the specialised row kernels (one CTA per sector
+ * block, x of the block staged in shared memory, per-row class tables)
+ * wherever the compiled operator has their tables; 1: the generic kernel
+ * everywhere.  For comparisons; process-wide.  Other values:
+ * QKRYLOV_ERROR_INVALID_ARG. */
 int qkrylov_b200_set_kernel_policy(int policy);
 
 /* Select which of N_up / N_dn a sector conserves after

@@ -186,6 +186,13 @@ class _PortHam:
             self.back._err()
         return y
 
+    def apply_into(self, x, y):
+        """y = H x into caller-owned complex128 arrays (no allocation here)."""
+        assert x.dtype == y.dtype == np.complex128 and x.flags.c_contiguous and y.flags.c_contiguous
+        if self.L.qko_ham_apply(self.h, x.ctypes.data, y.ctypes.data):
+            self.back._err()
+        return y
+
     def coo(self):
         n = self.L.qko_ham_coo_count(self.h)
         if n < 0:
@@ -354,6 +361,13 @@ class _RefHam:
     def apply(self, x):
         x = np.ascontiguousarray(x, dtype=np.complex128)
         y = np.zeros(self.dim, dtype=np.complex128)
+        if self.L.refb_ham_apply(self.h, x.ctypes.data, y.ctypes.data):
+            self.back._err()
+        return y
+
+    def apply_into(self, x, y):
+        """y = H x into caller-owned complex128 arrays (no allocation here)."""
+        assert x.dtype == y.dtype == np.complex128 and x.flags.c_contiguous and y.flags.c_contiguous
         if self.L.refb_ham_apply(self.h, x.ctypes.data, y.ctypes.data):
             self.back._err()
         return y

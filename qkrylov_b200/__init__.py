@@ -857,11 +857,9 @@ def ftlm(H: MatrixFreeHamiltonian, beta: float, n_random: int = 50, n_steps: int
 
 
 def set_kernel_policy(policy: str):
-    """'auto' (specialised kernels where eligible), 'generic', or one of the
-    earlier exchange-kernel variants 'exchange-block', 'exchange-warp',
-    'exchange-batched', 'exchange-list', 'exchange-staged', 'exchange-owner'."""
-    codes = {"auto": 0, "generic": 1, "exchange-block": 2, "exchange-warp": 3, "exchange-batched": 4,
-             "exchange-list": 5, "exchange-staged": 6, "exchange-owner": 7}
+    """'auto' (the specialised row kernels where the operator has their
+    tables) or 'generic' (the term-walk kernel only, for comparisons)."""
+    codes = {"auto": 0, "generic": 1}
     _check(lib().qkrylov_b200_set_kernel_policy(codes[policy]), "set_kernel_policy")
 
 

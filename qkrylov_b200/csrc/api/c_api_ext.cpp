@@ -41,12 +41,10 @@ int qkrylov_b200_device_count(void) {
 }
 
 int qkrylov_b200_set_kernel_policy(int policy) {
-  // 0 auto, 1 generic only, 2..7: exchange kernel with block tiles / warp
-  // tiles / batched gathers / target lists / staged blocks / block owner
-  if (policy < 0 || policy > 7) return QKRYLOV_ERROR_INVALID_ARG;
-  qkd_set_kernel_policy(policy == 1 ? 1 : 0);
-  static const int variant[8] = {6, 6, 0, 1, 2, 3, 4, 5};
-  qkd_set_spin_variant(variant[policy]);
+  // 0 auto (the specialised kernels where the operator has their tables),
+  // 1 the generic term-walk kernel only
+  if (policy < 0 || policy > 1) return QKRYLOV_ERROR_INVALID_ARG;
+  qkd_set_kernel_policy(policy);
   return QKRYLOV_SUCCESS;
 }
 

@@ -57,9 +57,6 @@ size_t qkd_plan_device_bytes(const qk_plan* p);
 /* 0: use specialised kernels where the operator qualifies (default);
  * 1: generic kernel only (for comparisons). */
 int qkd_set_kernel_policy(int policy);
-/* Exchange-kernel variant: 0 block tiles, 1 warp tiles, 2 warp tiles with
- * batched gathers (default); for comparisons. */
-int qkd_set_spin_variant(int variant);
 /* 1 when applies of this plan run the specialised two-site spin kernel. */
 int qkd_plan_kernel(const qk_plan* p);
 

@@ -43,29 +43,17 @@ struct SpinPlan {
   int L, H;
   uint64_t dim;
   int nbonds, ndiag;
-  // bond classes for the warp-tile kernel
+  // bond classes (host-side, for building the row tables)
   int nlow, nhigh, ncross, ndcross;
   uint32_t low_mask[kMaxBonds], high_mask[kMaxBonds], cross_lo[kMaxBonds], cross_hi[kMaxBonds];
   uint8_t low_i[kMaxBonds], high_i[kMaxBonds], cross_li[kMaxBonds];
   double low_c01[kMaxBonds], low_c10[kMaxBonds], high_c01[kMaxBonds], high_c10[kMaxBonds];
   double cross_c01[kMaxBonds], cross_c10[kMaxBonds];   // c01: low bit 0 / high bit 1
-  // merged bond list of the batched kernel (any of low / high / crossing)
-  int nall;
-  uint32_t all_lo[kMaxBonds], all_hi[kMaxBonds], all_ilo[kMaxBonds], all_ihi[kMaxBonds];
-  double all_c01[kMaxBonds], all_c10[kMaxBonds];
-  // per-part target lists of the list kernel
-  const uint32_t* loff;    // nllist + 1 offsets into lent (by llist position)
-  const uint32_t* lent;    // (in-class rank of l ^ m) << 8 | coefficient index
-  const uint32_t* hoff;    // 2^H + 1 offsets into hent
-  const uint2* hent;       // (A[h ^ m], coefficient index)
-  const uint32_t* hlst;    // 2^H: llist position of block h's first low part
   uint32_t max_block;      // largest block size
   double coef[2 * kMaxBonds];
   int ncoef;
   uint32_t dcross_mask[kMaxDiag];
   double dcross_w[kMaxDiag];
-  const double* dhi;     // 2^H: diagonal terms inside the high part
-  const double* dlo;     // aligned with llist: diagonal terms inside the low part
   SpinBond bonds[kMaxBonds];
   uint32_t diag_smask[kMaxDiag];
   double diag_w[kMaxDiag];
@@ -181,619 +169,6 @@ k_hx_spin(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __r
   }
   if (DOT) {
     __shared__ double sbuf[2 * (kSpinThreads / 32)];
-    block_sum2(dr, di, sbuf);
-    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
-    grid_finish(partials, ticket, 1, dot_out);
-  }
-}
-
-// Warp-tile kernel for charge-conserving exchange bonds (only the 01 <-> 10
-// combinations are valid).  A warp owns 32 consecutive rows of one sector
-// block (lane = row), so the block index h, the diagonal of the high part
-// and the validity and target base of every high bond are warp-uniform; no
-// block-wide barrier is needed after the tables are staged.
-template <int DT, bool DOT>
-__global__ void __launch_bounds__(256)
-k_hx_spin_lean(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
-               double* partials, unsigned* ticket, double* dot_out) {
-  using T = VT<DT>;
-  using R = typename T::R;
-  extern __shared__ __align__(16) unsigned char sm[];
-  const SpinPlan& p = *pp;
-  const int nB = 1 << p.L;
-  const uint64_t dim = p.dim;
-  uint16_t* sB = reinterpret_cast<uint16_t*>(sm);
-  __shared__ uint32_t s_lm[kMaxBonds], s_hm[kMaxBonds], s_clo[kMaxBonds], s_chi[kMaxBonds], s_dm[kMaxDiag];
-  __shared__ uint8_t s_li[kMaxBonds], s_hi[kMaxBonds], s_ci[kMaxBonds];
-  __shared__ R s_l01[kMaxBonds], s_l10[kMaxBonds], s_h01[kMaxBonds], s_h10[kMaxBonds], s_c01[kMaxBonds],
-      s_c10[kMaxBonds], s_dw[kMaxDiag];
-  const int nlow = p.nlow, nhigh = p.nhigh, ncross = p.ncross, ndc = p.ndcross, L = p.L;
-  for (int i = threadIdx.x; i < nB; i += blockDim.x) sB[i] = p.B16[i];
-  for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
-    s_lm[i] = p.low_mask[i]; s_hm[i] = p.high_mask[i]; s_clo[i] = p.cross_lo[i]; s_chi[i] = p.cross_hi[i];
-    s_li[i] = p.low_i[i]; s_hi[i] = p.high_i[i]; s_ci[i] = p.cross_li[i];
-    s_l01[i] = R(p.low_c01[i]); s_l10[i] = R(p.low_c10[i]); s_h01[i] = R(p.high_c01[i]);
-    s_h10[i] = R(p.high_c10[i]); s_c01[i] = R(p.cross_c01[i]); s_c10[i] = R(p.cross_c10[i]);
-  }
-  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { s_dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
-  __syncthreads();
-  const uint32_t* __restrict__ A = p.A32;
-  const int lane = threadIdx.x & 31;
-  const uint32_t wglobal = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
-  const uint32_t nsub = p.ntiles * (kSpinThreads / 32);  // 32-row sub-tiles of the 512-row tiles
-  double dr = 0.0, di = 0.0;
-  for (uint32_t w = wglobal; w < nsub; w += nwarps) {
-    const qk_tile_t tile = p.tiles[w / (kSpinThreads / 32)];
-    const uint32_t sub = (w % (kSpinThreads / 32)) * 32;
-    if (sub >= tile.count) continue;
-    const uint32_t j = sub + lane;
-    const bool active = j < tile.count;
-    const uint32_t h = tile.h;
-    const uint64_t base = __ldg(A + h);
-    const uint64_t row = tile.row0 + j;
-    const uint64_t rank_in_block = row - base;
-    const uint32_t l = active ? uint32_t(__ldg(p.lrow + tile.lstart + j)) : 0u;
-    R xr0 = R(0), xi0 = R(0);
-    R d = R(0);
-    if (active) {
-      T::ld(x, row, xr0, xi0);
-      d = R(__ldg(p.dhi + h)) + R(__ldg(p.dlo + tile.lstart + j));
-    }
-    const uint32_t s = (h << L) | l;
-    for (int q = 0; q < ndc; ++q) d += (__popc(s & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
-    R yr = d * xr0, yi = d * xi0;
-    if (active) {
-      for (int q = 0; q < nhigh; ++q) {  // warp-uniform
-        const uint32_t m = s_hm[q], v = h & m;
-        if (v == 0 || v == m) continue;
-        const R c = ((v >> s_hi[q]) & 1u) ? s_h10[q] : s_h01[q];
-        const uint64_t col = uint64_t(__ldg(A + (h ^ m))) + rank_in_block;
-        if (col >= dim) continue;  // never taken for charge-conserving bonds; bounds every load
-        R xr, xi;
-        T::ld(x, col, xr, xi);
-        yr += c * xr;
-        if (T::cplx) yi += c * xi;
-      }
-      for (int q = 0; q < nlow; ++q) {
-        const uint32_t m = s_lm[q], v = l & m;
-        if (v == 0 || v == m) continue;
-        const R c = ((v >> s_li[q]) & 1u) ? s_l10[q] : s_l01[q];
-        const uint64_t col = base + sB[l ^ m];
-        if (col >= dim) continue;
-        R xr, xi;
-        T::ld(x, col, xr, xi);
-        yr += c * xr;
-        if (T::cplx) yi += c * xi;
-      }
-      for (int q = 0; q < ncross; ++q) {
-        const uint32_t bl = (l >> s_ci[q]) & 1u, bh = (h & s_chi[q]) ? 1u : 0u;
-        if (bl == bh) continue;
-        const R c = bl ? s_c10[q] : s_c01[q];
-        const uint64_t col = uint64_t(__ldg(A + (h ^ s_chi[q]))) + sB[l ^ s_clo[q]];
-        if (col >= dim) continue;
-        R xr, xi;
-        T::ld(x, col, xr, xi);
-        yr += c * xr;
-        if (T::cplx) yi += c * xi;
-      }
-      T::st(y, row, yr, yi);
-      if (DOT) {
-        dr += double(xr0) * double(yr) + double(xi0) * double(yi);
-        di += double(xr0) * double(yi) - double(xi0) * double(yr);
-      }
-    }
-  }
-  if (DOT) {
-    __shared__ double sbuf[2 * (256 / 32)];
-    block_sum2(dr, di, sbuf);
-    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
-    grid_finish(partials, ticket, 1, dot_out);
-  }
-}
-
-
-// Batched-gather kernel.  For a warp's 32 rows the block index h is fixed,
-// so for every bond the target block base A[h ^ hi] and the high-part
-// popcount are warp-uniform: lane q computes them for bond q once per tile
-// and the warp reads them from its slice of shared memory.  Per row and
-// bond only the low-part rank B[l ^ lo] is a lane-dependent lookup; the
-// bonds are walked four at a time so four gathers are in flight per lane.
-template <int DT, bool DOT>
-__global__ void __launch_bounds__(256)
-k_hx_spin_batched(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
-                  double* partials, unsigned* ticket, double* dot_out) {
-  using T = VT<DT>;
-  using R = typename T::R;
-  extern __shared__ __align__(16) unsigned char sm[];
-  const SpinPlan& p = *pp;
-  const int nB = 1 << p.L;
-  const uint64_t dim = p.dim;
-  uint16_t* sB = reinterpret_cast<uint16_t*>(sm);
-  __shared__ uint32_t s_lo[kMaxBonds], s_ilo[kMaxBonds], s_dm[kMaxDiag];
-  __shared__ R s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
-  __shared__ uint32_t s_wbase[256 / 32][kMaxBonds];   // per warp: A[h ^ hi] of bond q
-  __shared__ uint8_t s_whv[256 / 32][kMaxBonds];      // per warp: popcount(h & hi), bit-i-in-high flag << 4
-  const int nall = p.nall, ndc = p.ndcross, L = p.L;
-  for (int i = threadIdx.x; i < nB; i += blockDim.x) sB[i] = p.B16[i];
-  for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
-    s_lo[i] = p.all_lo[i]; s_ilo[i] = p.all_ilo[i];
-    s_c01[i] = R(p.all_c01[i]); s_c10[i] = R(p.all_c10[i]);
-  }
-  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { s_dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
-  __syncthreads();
-  const uint32_t* __restrict__ A = p.A32;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t wglobal = blockIdx.x * (blockDim.x >> 5) + wib;
-  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
-  const uint32_t nsub = p.ntiles * (kSpinThreads / 32);
-  double dr = 0.0, di = 0.0;
-  for (uint32_t w = wglobal; w < nsub; w += nwarps) {
-    const qk_tile_t tile = p.tiles[w / (kSpinThreads / 32)];
-    const uint32_t sub = (w % (kSpinThreads / 32)) * 32;
-    if (sub >= tile.count) continue;
-    const uint32_t h = tile.h;
-    for (int q = lane; q < nall; q += 32) {
-      const uint32_t hm = p.all_hi[q];
-      s_wbase[wib][q] = __ldg(A + (h ^ hm));
-      s_whv[wib][q] = uint8_t(__popc(h & hm) | ((h & p.all_ihi[q]) ? 16u : 0u));
-    }
-    __syncwarp();
-    const uint32_t j = sub + lane;
-    if (j < tile.count) {
-      const uint64_t row = tile.row0 + j;
-      const uint32_t base = __ldg(A + h);
-      const uint32_t r = uint32_t(row - base);
-      const uint32_t l = uint32_t(__ldg(p.lrow + tile.lstart + j));
-      R xr0, xi0;
-      T::ld(x, row, xr0, xi0);
-      R d = R(__ldg(p.dhi + h)) + R(__ldg(p.dlo + tile.lstart + j));
-      const uint32_t st = (h << L) | l;
-      for (int q = 0; q < ndc; ++q) d += (__popc(st & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
-      R yr = d * xr0, yi = d * xi0;
-      for (int q0 = 0; q0 < nall; q0 += 4) {
-        uint64_t col[4];
-        R c[4];
-        bool ok[4];
-        #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int q = q0 + u;
-          ok[u] = false; col[u] = 0; c[u] = R(0);
-          if (q < nall) {
-            const uint32_t lo = s_lo[q];
-            const uint32_t hv = s_whv[wib][q];
-            const uint32_t nset = __popc(l & lo) + (hv & 15u);
-            const bool iset = (l & s_ilo[q]) || (hv & 16u);
-            ok[u] = (nset == 1u);
-            c[u] = iset ? s_c10[q] : s_c01[q];
-            col[u] = uint64_t(s_wbase[wib][q]) + (lo ? uint32_t(sB[l ^ lo]) : r);
-            ok[u] = ok[u] && col[u] < dim;  // never false for conserving bonds; bounds every load
-          }
-        }
-        R xr[4], xi[4];
-        #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          xr[u] = R(0); xi[u] = R(0);
-          if (ok[u]) T::ld(x, col[u], xr[u], xi[u]);
-        }
-        #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          yr += c[u] * xr[u];
-          if (T::cplx) yi += c[u] * xi[u];
-        }
-      }
-      T::st(y, row, yr, yi);
-      if (DOT) {
-        dr += double(xr0) * double(yr) + double(xi0) * double(yi);
-        di += double(xr0) * double(yi) - double(xi0) * double(yr);
-      }
-    }
-    __syncwarp();
-  }
-  if (DOT) {
-    __shared__ double sbuf[2 * (256 / 32)];
-    block_sum2(dr, di, sbuf);
-    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
-    grid_finish(partials, ticket, 1, dot_out);
-  }
-}
-
-
-
-// Batched gathers of the list kernels: up to kBatch list entries are loaded,
-// then all their x gathers are issued, then accumulated, so kBatch loads are
-// in flight per lane instead of one dependent chain per bond.
-constexpr int kBatch = 8;
-
-template <int DT>
-__device__ __forceinline__ void gather_high(const uint2* __restrict__ hent, uint32_t hbeg, uint32_t hend,
-                                            uint32_t r, uint64_t dim, const void* __restrict__ x,
-                                            const typename VT<DT>::R* coef, typename VT<DT>::R& yr,
-                                            typename VT<DT>::R& yi) {
-  using T = VT<DT>;
-  using R = typename T::R;
-  for (uint32_t e0 = hbeg; e0 < hend; e0 += kBatch) {
-    uint2 ent[kBatch];
-    #pragma unroll
-    for (int u = 0; u < kBatch; ++u) ent[u] = (e0 + u < hend) ? __ldg(hent + e0 + u) : make_uint2(0xFFFFFFFFu, 0u);
-    R xr[kBatch], xi[kBatch];
-    #pragma unroll
-    for (int u = 0; u < kBatch; ++u) {
-      xr[u] = R(0); xi[u] = R(0);
-      const uint64_t col = uint64_t(ent[u].x) + r;
-      if (e0 + u < hend && col < dim) T::ld(x, col, xr[u], xi[u]);
-    }
-    #pragma unroll
-    for (int u = 0; u < kBatch; ++u) {
-      if (e0 + u < hend) {
-        const R c = coef[ent[u].y];
-        yr += c * xr[u];
-        if (T::cplx) yi += c * xi[u];
-      }
-    }
-  }
-}
-
-template <int DT>
-__device__ __forceinline__ void gather_low(const uint32_t* __restrict__ lent, uint32_t lbeg, uint32_t lend,
-                                           uint32_t base, uint64_t dim, const void* __restrict__ x,
-                                           const typename VT<DT>::R* coef, typename VT<DT>::R& yr,
-                                           typename VT<DT>::R& yi) {
-  using T = VT<DT>;
-  using R = typename T::R;
-  for (uint32_t e0 = lbeg; e0 < lend; e0 += kBatch) {
-    uint32_t ent[kBatch];
-    #pragma unroll
-    for (int u = 0; u < kBatch; ++u) ent[u] = (e0 + u < lend) ? __ldg(lent + e0 + u) : 0u;
-    R xr[kBatch], xi[kBatch];
-    #pragma unroll
-    for (int u = 0; u < kBatch; ++u) {
-      xr[u] = R(0); xi[u] = R(0);
-      const uint64_t col = uint64_t(base) + (ent[u] >> 8);
-      if (e0 + u < lend && col < dim) T::ld(x, col, xr[u], xi[u]);
-    }
-    #pragma unroll
-    for (int u = 0; u < kBatch; ++u) {
-      if (e0 + u < lend) {
-        const R c = coef[ent[u] & 0xFFu];
-        yr += c * xr[u];
-        if (T::cplx) yi += c * xi[u];
-      }
-    }
-  }
-}
-
-// List kernel: for each low part l (and each high part h) the valid bond
-// targets are precomputed, so a row visits only the bonds it actually has.
-// Low-bond targets live in a small table shared by every block of the same
-// charge class (rank of l ^ m inside the class); high-bond target bases are
-// per h and warp-uniform.  Crossing bonds (few) are evaluated directly.
-template <int DT, bool DOT>
-__global__ void __launch_bounds__(256)
-k_hx_spin_list(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
-               double* partials, unsigned* ticket, double* dot_out) {
-  using T = VT<DT>;
-  using R = typename T::R;
-  extern __shared__ __align__(16) unsigned char sm[];
-  const SpinPlan& p = *pp;
-  const int nB = 1 << p.L;
-  const uint64_t dim = p.dim;
-  uint16_t* sB = reinterpret_cast<uint16_t*>(sm);
-  __shared__ R s_coef[2 * kMaxBonds];
-  __shared__ uint32_t s_clo[kMaxBonds], s_chi[kMaxBonds], s_dm[kMaxDiag];
-  __shared__ uint8_t s_ci[kMaxBonds];
-  __shared__ R s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
-  __shared__ uint32_t s_cbase[256 / 32][kMaxBonds];
-  const int ncross = p.ncross, ndc = p.ndcross, L = p.L;
-  for (int i = threadIdx.x; i < nB; i += blockDim.x) sB[i] = p.B16[i];
-  for (int i = threadIdx.x; i < 2 * kMaxBonds; i += blockDim.x) s_coef[i] = R(p.coef[i]);
-  for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
-    s_clo[i] = p.cross_lo[i]; s_chi[i] = p.cross_hi[i]; s_ci[i] = p.cross_li[i];
-    s_c01[i] = R(p.cross_c01[i]); s_c10[i] = R(p.cross_c10[i]);
-  }
-  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { s_dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
-  __syncthreads();
-  const uint32_t* __restrict__ A = p.A32;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t wglobal = blockIdx.x * (blockDim.x >> 5) + wib;
-  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
-  const uint32_t nsub = p.ntiles * (kSpinThreads / 32);
-  double dr = 0.0, di = 0.0;
-  for (uint32_t w = wglobal; w < nsub; w += nwarps) {
-    const qk_tile_t tile = p.tiles[w / (kSpinThreads / 32)];
-    const uint32_t sub = (w % (kSpinThreads / 32)) * 32;
-    if (sub >= tile.count) continue;
-    const uint32_t h = tile.h;
-    for (int q = lane; q < ncross; q += 32) s_cbase[wib][q] = __ldg(A + (h ^ s_chi[q]));
-    __syncwarp();
-    const uint32_t hbeg = __ldg(p.hoff + h), hend = __ldg(p.hoff + h + 1);
-    const uint32_t j = sub + lane;
-    if (j < tile.count) {
-      const uint64_t row = tile.row0 + j;
-      const uint32_t base = __ldg(A + h);
-      const uint32_t r = uint32_t(row - base);
-      const uint32_t pos = tile.lstart + j;
-      const uint32_t l = uint32_t(__ldg(p.lrow + pos));
-      R xr0, xi0;
-      T::ld(x, row, xr0, xi0);
-      R d = R(__ldg(p.dhi + h)) + R(__ldg(p.dlo + pos));
-      const uint32_t st = (h << L) | l;
-      for (int q = 0; q < ndc; ++q) d += (__popc(st & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
-      R yr = d * xr0, yi = d * xi0;
-      // high bonds: warp-uniform list, consecutive lanes gather consecutive
-      // rows; eight entries, then their eight gathers, are in flight at once
-      gather_high<DT>(p.hent, hbeg, hend, r, dim, x, s_coef, yr, yi);
-      // low bonds: the row's own list, batched the same way
-      const uint32_t lbeg = __ldg(p.loff + pos), lend = __ldg(p.loff + pos + 1);
-      gather_low<DT>(p.lent, lbeg, lend, base, dim, x, s_coef, yr, yi);
-      for (int q = 0; q < ncross; ++q) {
-        const uint32_t bl = (l >> s_ci[q]) & 1u, bh = (h & s_chi[q]) ? 1u : 0u;
-        if (bl == bh) continue;
-        const R c = bl ? s_c10[q] : s_c01[q];
-        const uint64_t col = uint64_t(s_cbase[wib][q]) + sB[l ^ s_clo[q]];
-        if (col >= dim) continue;
-        R xr, xi;
-        T::ld(x, col, xr, xi);
-        yr += c * xr;
-        if (T::cplx) yi += c * xi;
-      }
-      T::st(y, row, yr, yi);
-      if (DOT) {
-        dr += double(xr0) * double(yr) + double(xi0) * double(yi);
-        di += double(xr0) * double(yi) - double(xi0) * double(yr);
-      }
-    }
-    __syncwarp();
-  }
-  if (DOT) {
-    __shared__ double sbuf[2 * (256 / 32)];
-    block_sum2(dr, di, sbuf);
-    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
-    grid_finish(partials, ticket, 1, dot_out);
-  }
-}
-
-
-// Block-staged list kernel: one CTA owns a whole sector block h at a time.
-// It stages x_h in shared memory, so every low-bond gather (targets inside
-// the block) is a shared-memory load; high-bond targets are whole rows of
-// other blocks at the same in-block rank, read coalesced from global; the
-// few crossing bonds gather from global.
-template <int DT, bool DOT>
-__global__ void __launch_bounds__(256, 4)
-k_hx_spin_staged(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
-                 double* partials, unsigned* ticket, double* dot_out) {
-  using T = VT<DT>;
-  using R = typename T::R;
-  extern __shared__ __align__(16) unsigned char sm[];
-  const SpinPlan& p = *pp;
-  const uint64_t dim = p.dim;
-  R* sxr = reinterpret_cast<R*>(sm);
-  R* sxi = sxr + p.max_block;
-  __shared__ R s_coef[2 * kMaxBonds];
-  __shared__ uint32_t s_clo[kMaxBonds], s_chi[kMaxBonds], s_dm[kMaxDiag], s_cbase[kMaxBonds];
-  __shared__ uint8_t s_ci[kMaxBonds];
-  __shared__ R s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
-  const int ncross = p.ncross, ndc = p.ndcross, L = p.L;
-  for (int i = threadIdx.x; i < 2 * kMaxBonds; i += blockDim.x) s_coef[i] = R(p.coef[i]);
-  for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
-    s_clo[i] = p.cross_lo[i]; s_chi[i] = p.cross_hi[i]; s_ci[i] = p.cross_li[i];
-    s_c01[i] = R(p.cross_c01[i]); s_c10[i] = R(p.cross_c10[i]);
-  }
-  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { s_dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
-  const uint32_t* __restrict__ A = p.A32;
-  const uint32_t nA = 1u << p.H;
-  double dr = 0.0, di = 0.0;
-  for (uint32_t h = blockIdx.x; h < nA; h += gridDim.x) {
-    const uint32_t base = __ldg(A + h);
-    const uint32_t size = (h + 1 < nA ? __ldg(A + h + 1) : uint32_t(dim)) - base;
-    if (size == 0) continue;
-    __syncthreads();  // previous block's readers are done with sx
-    for (uint32_t r = threadIdx.x; r < size; r += blockDim.x) {
-      R xr, xi;
-      T::ld(x, uint64_t(base) + r, xr, xi);
-      sxr[r] = xr;
-      if (T::cplx) sxi[r] = xi;
-    }
-    for (int q = threadIdx.x; q < ncross; q += blockDim.x) s_cbase[q] = __ldg(A + (h ^ s_chi[q]));
-    __syncthreads();
-    const uint32_t hbeg = __ldg(p.hoff + h), hend = __ldg(p.hoff + h + 1);
-    const uint32_t lst = __ldg(p.hlst + h);
-    const R dh = R(__ldg(p.dhi + h));
-    for (uint32_t r = threadIdx.x; r < size; r += blockDim.x) {
-      const uint32_t pos = lst + r;
-      const uint32_t l = uint32_t(__ldg(p.lrow + pos));
-      const R xr0 = sxr[r], xi0 = T::cplx ? sxi[r] : R(0);
-      R d = dh + R(__ldg(p.dlo + pos));
-      const uint32_t st = (h << L) | l;
-      for (int q = 0; q < ndc; ++q) d += (__popc(st & s_dm[q]) & 1) ? -s_dw[q] : s_dw[q];
-      R yr = d * xr0, yi = d * xi0;
-      gather_high<DT>(p.hent, hbeg, hend, r, dim, x, s_coef, yr, yi);
-      const uint32_t lbeg = __ldg(p.loff + pos), lend = __ldg(p.loff + pos + 1);
-      for (uint32_t e0 = lbeg; e0 < lend; e0 += kBatch) {
-        uint32_t ent[kBatch];
-        #pragma unroll
-        for (int u = 0; u < kBatch; ++u) ent[u] = (e0 + u < lend) ? __ldg(p.lent + e0 + u) : 0xFFFFFFFFu;
-        #pragma unroll
-        for (int u = 0; u < kBatch; ++u) {
-          const uint32_t k = ent[u] >> 8;
-          if (e0 + u < lend && k < size) {
-            const R c = s_coef[ent[u] & 0xFFu];
-            yr += c * sxr[k];
-            if (T::cplx) yi += c * sxi[k];
-          }
-        }
-      }
-      for (int q = 0; q < ncross; ++q) {
-        const uint32_t bl = (l >> s_ci[q]) & 1u, bh = (h & s_chi[q]) ? 1u : 0u;
-        if (bl == bh) continue;
-        const R c = bl ? s_c10[q] : s_c01[q];
-        const uint64_t col = uint64_t(s_cbase[q]) + __ldg(p.B16 + (l ^ s_clo[q]));
-        if (col >= dim) continue;
-        R xr, xi;
-        T::ld(x, col, xr, xi);
-        yr += c * xr;
-        if (T::cplx) yi += c * xi;
-      }
-      T::st(y, uint64_t(base) + r, yr, yi);
-      if (DOT) {
-        dr += double(xr0) * double(yr) + double(xi0) * double(yi);
-        di += double(xr0) * double(yi) - double(xi0) * double(yr);
-      }
-    }
-  }
-  if (DOT) {
-    __shared__ double sbuf[2 * (256 / 32)];
-    block_sum2(dr, di, sbuf);
-    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
-    grid_finish(partials, ticket, 1, dot_out);
-  }
-}
-
-
-// Block-owner kernel: a 512-thread CTA owns one sector block h at a time and
-// each thread keeps register accumulators for its rows r = tid + 512 k,
-// k < K, with K (1, 2, 4 or 8) the smallest that covers the block.
-// x_h is staged in shared memory (all low-bond targets), every valid high
-// bond is a block-wide coalesced AXPY from another block at the same
-// in-block rank with K independent loads per thread in flight, and the few
-// crossing bonds gather from global memory.
-constexpr int kOwnThreads = 512;
-constexpr int kOwnRows = 8;  // blocks up to 4096 rows
-
-struct OwnShared {
-  uint32_t clo[kMaxBonds], chi[kMaxBonds], dm[kMaxDiag], cbase[kMaxBonds];
-  uint8_t ci[kMaxBonds];
-  uint2 hent[kMaxBonds];
-};
-
-template <int DT, int K>
-__device__ __forceinline__ void own_block(const SpinPlan& p, const OwnShared& S, const typename VT<DT>::R* coef,
-                                          const typename VT<DT>::R* c01, const typename VT<DT>::R* c10,
-                                          const typename VT<DT>::R* dw, const typename VT<DT>::R* sxr,
-                                          const typename VT<DT>::R* sxi, uint32_t h, uint32_t base, uint32_t size,
-                                          uint32_t hbeg, uint32_t nh, const void* __restrict__ x,
-                                          void* __restrict__ y, bool dot, double& dr, double& di) {
-  using T = VT<DT>;
-  using R = typename T::R;
-  const uint64_t dim = p.dim;
-  const int ncross = p.ncross, ndc = p.ndcross, L = p.L;
-  const uint32_t lst = __ldg(p.hlst + h);
-  const R dh = R(__ldg(p.dhi + h));
-  R yr[K], yi[K];
-  #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const uint32_t r = threadIdx.x + k * kOwnThreads;
-    yr[k] = R(0); yi[k] = R(0);
-    if (r >= size) continue;
-    const uint32_t pos = lst + r;
-    const uint32_t l = uint32_t(__ldg(p.lrow + pos));
-    R d = dh + R(__ldg(p.dlo + pos));
-    const uint32_t st = (h << L) | l;
-    for (int q = 0; q < ndc; ++q) d += (__popc(st & S.dm[q]) & 1) ? -dw[q] : dw[q];
-    yr[k] = d * sxr[r];
-    yi[k] = T::cplx ? d * sxi[r] : R(0);
-    const uint32_t lbeg = __ldg(p.loff + pos), lend = __ldg(p.loff + pos + 1);
-    for (uint32_t e = lbeg; e < lend; ++e) {
-      const uint32_t ent = __ldg(p.lent + e);
-      const uint32_t kk = ent >> 8;
-      if (kk >= size) continue;
-      const R c = coef[ent & 0xFFu];
-      yr[k] += c * sxr[kk];
-      if (T::cplx) yi[k] += c * sxi[kk];
-    }
-    for (int q = 0; q < ncross; ++q) {
-      const uint32_t bl = (l >> S.ci[q]) & 1u, bh = (h & S.chi[q]) ? 1u : 0u;
-      if (bl == bh) continue;
-      const R c = bl ? c10[q] : c01[q];
-      const uint64_t col = uint64_t(S.cbase[q]) + __ldg(p.B16 + (l ^ S.clo[q]));
-      if (col >= dim) continue;
-      R xr, xi;
-      T::ld(x, col, xr, xi);
-      yr[k] += c * xr;
-      if (T::cplx) yi[k] += c * xi;
-    }
-  }
-  for (uint32_t e = 0; e < nh; ++e) {
-    const uint2 ent = (e < uint32_t(kMaxBonds)) ? S.hent[e] : __ldg(p.hent + hbeg + e);
-    const R c = coef[ent.y];
-    R xr[K], xi[K];
-    #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const uint32_t r = threadIdx.x + k * kOwnThreads;
-      xr[k] = R(0); xi[k] = R(0);
-      const uint64_t col = uint64_t(ent.x) + r;
-      if (r < size && col < dim) T::ld(x, col, xr[k], xi[k]);
-    }
-    #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      yr[k] += c * xr[k];
-      if (T::cplx) yi[k] += c * xi[k];
-    }
-  }
-  #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const uint32_t r = threadIdx.x + k * kOwnThreads;
-    if (r < size) {
-      T::st(y, uint64_t(base) + r, yr[k], yi[k]);
-      if (dot) {
-        const double x0r = double(sxr[r]), x0i = T::cplx ? double(sxi[r]) : 0.0;
-        dr += x0r * double(yr[k]) + x0i * double(yi[k]);
-        di += x0r * double(yi[k]) - x0i * double(yr[k]);
-      }
-    }
-  }
-}
-
-template <int DT, bool DOT>
-__global__ void __launch_bounds__(kOwnThreads, 2)
-k_hx_spin_owner(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
-                double* partials, unsigned* ticket, double* dot_out) {
-  using T = VT<DT>;
-  using R = typename T::R;
-  extern __shared__ __align__(16) unsigned char sm[];
-  const SpinPlan& p = *pp;
-  const uint64_t dim = p.dim;
-  R* sxr = reinterpret_cast<R*>(sm);
-  R* sxi = sxr + p.max_block;
-  __shared__ OwnShared S;
-  __shared__ R s_coef[2 * kMaxBonds], s_c01[kMaxBonds], s_c10[kMaxBonds], s_dw[kMaxDiag];
-  const int ncross = p.ncross;
-  for (int i = threadIdx.x; i < 2 * kMaxBonds; i += blockDim.x) s_coef[i] = R(p.coef[i]);
-  for (int i = threadIdx.x; i < kMaxBonds; i += blockDim.x) {
-    S.clo[i] = p.cross_lo[i]; S.chi[i] = p.cross_hi[i]; S.ci[i] = p.cross_li[i];
-    s_c01[i] = R(p.cross_c01[i]); s_c10[i] = R(p.cross_c10[i]);
-  }
-  for (int i = threadIdx.x; i < kMaxDiag; i += blockDim.x) { S.dm[i] = p.dcross_mask[i]; s_dw[i] = R(p.dcross_w[i]); }
-  const uint32_t* __restrict__ A = p.A32;
-  const uint32_t nA = 1u << p.H;
-  double dr = 0.0, di = 0.0;
-  for (uint32_t h = blockIdx.x; h < nA; h += gridDim.x) {
-    const uint32_t base = __ldg(A + h);
-    const uint32_t size = (h + 1 < nA ? __ldg(A + h + 1) : uint32_t(dim)) - base;
-    if (size == 0) continue;
-    const uint32_t hbeg = __ldg(p.hoff + h), nh = __ldg(p.hoff + h + 1) - hbeg;
-    __syncthreads();  // the previous block is finished with the staging
-    for (uint32_t r = threadIdx.x; r < size; r += kOwnThreads) {
-      R a, b;
-      T::ld(x, uint64_t(base) + r, a, b);
-      sxr[r] = a;
-      if (T::cplx) sxi[r] = b;
-    }
-    for (int q = threadIdx.x; q < ncross; q += blockDim.x) S.cbase[q] = __ldg(A + (h ^ S.chi[q]));
-    for (uint32_t e = threadIdx.x; e < nh && e < uint32_t(kMaxBonds); e += blockDim.x) S.hent[e] = __ldg(p.hent + hbeg + e);
-    __syncthreads();
-    if (size <= kOwnThreads)
-      own_block<DT, 1>(p, S, s_coef, s_c01, s_c10, s_dw, sxr, sxi, h, base, size, hbeg, nh, x, y, DOT, dr, di);
-    else if (size <= 2 * kOwnThreads)
-      own_block<DT, 2>(p, S, s_coef, s_c01, s_c10, s_dw, sxr, sxi, h, base, size, hbeg, nh, x, y, DOT, dr, di);
-    else if (size <= 4 * kOwnThreads)
-      own_block<DT, 4>(p, S, s_coef, s_c01, s_c10, s_dw, sxr, sxi, h, base, size, hbeg, nh, x, y, DOT, dr, di);
-    else
-      own_block<DT, 8>(p, S, s_coef, s_c01, s_c10, s_dw, sxr, sxi, h, base, size, hbeg, nh, x, y, DOT, dr, di);
-  }
-  if (DOT) {
-    __shared__ double sbuf[2 * (kOwnThreads / 32)];
     block_sum2(dr, di, sbuf);
     if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
     grid_finish(partials, ticket, 1, dot_out);
@@ -1393,20 +768,6 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
       h.cross_c10[h.ncross] = b.c[1]; h.cross_c01[h.ncross] = b.c[2]; ++h.ncross;
     }
   }
-  if (lean) {
-    for (int q = 0; q < h.nbonds; ++q) {
-      const SpinBond& b = h.bonds[q];
-      const uint64_t mi = 1ull << b.bi, mj = 1ull << b.bj, lowbits = (1ull << L) - 1;
-      const uint64_t m = mi | mj;
-      h.all_lo[h.nall] = uint32_t(m & lowbits);
-      h.all_hi[h.nall] = uint32_t(m >> L);
-      h.all_ilo[h.nall] = uint32_t(mi & lowbits);   // bit i (the lower one) in the low part
-      h.all_ihi[h.nall] = uint32_t((mi & ~lowbits) >> L);
-      h.all_c10[h.nall] = b.c[1];                    // bit i set, bit j clear
-      h.all_c01[h.nall] = b.c[2];
-      ++h.nall;
-    }
-  }
   std::vector<double> dhi(d->nA, 0.0), dlo(d->nllist, 0.0);
   if (lean) {
     const uint32_t lowbits = (1u << L) - 1u;
@@ -1423,7 +784,7 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     }
   }
 
-  // coefficient table and per-part target lists (list kernel)
+  // coefficient table and the per-part target lists the row tables are built from
   std::vector<uint32_t> loff, lent, hoff, hlst;
   std::vector<uint2> hent;
   if (lean) {
@@ -1606,10 +967,6 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
   };
   bool ok = up(0, A32.data(), A32.size() * 4) && up(1, B16.data(), B16.size() * 2) &&
             up(2, l16.data(), l16.size() * 2) && up(3, tiles.data(), tiles.size() * sizeof(qk_tile_t)) &&
-            up(4, dhi.data(), dhi.size() * 8) && up(5, dlo.data(), dlo.size() * 8) &&
-            (!lean || (up(6, loff.data(), loff.size() * 4) && up(7, lent.data(), lent.size() * 4) &&
-                       up(8, hoff.data(), hoff.size() * 4) && up(9, hent.data(), hent.size() * sizeof(uint2)) &&
-                       up(10, hlst.data(), hlst.size() * 4))) &&
             (!h.rows_ok || (up(11, rrec.data(), rrec.size() * sizeof(uint2)) &&
                             up(12, lgrp.data(), lgrp.size() * sizeof(uint2)) && up(13, crk.data(), crk.size() * 2) &&
                             up(14, dtab.data(), dtab.size() * 8) &&
@@ -1625,13 +982,6 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.B16 = static_cast<const uint16_t*>(out->bufs[1]);
     h.lrow = static_cast<const uint16_t*>(out->bufs[2]);
     h.tiles = static_cast<const qk_tile_t*>(out->bufs[3]);
-    h.dhi = static_cast<const double*>(out->bufs[4]);
-    h.dlo = static_cast<const double*>(out->bufs[5]);
-    h.loff = static_cast<const uint32_t*>(out->bufs[6]);
-    h.lent = static_cast<const uint32_t*>(out->bufs[7]);
-    h.hoff = static_cast<const uint32_t*>(out->bufs[8]);
-    h.hent = static_cast<const uint2*>(out->bufs[9]);
-    h.hlst = static_cast<const uint32_t*>(out->bufs[10]);
     h.rrec = static_cast<const uint2*>(out->bufs[11]);
     h.lgrp = static_cast<const uint2*>(out->bufs[12]);
     h.crk = static_cast<const uint16_t*>(out->bufs[13]);
@@ -1852,160 +1202,6 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
   return out;
 }
 
-int spin_apply_lean(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
-                    qk_workspace* w, double* dot_out) {
-  const size_t smem = size_t(1u << h->host.L) * 2;
-#define QKD_LEAN_LAUNCH(DT)                                                                              \
-  {                                                                                                      \
-    if (dot_out) {                                                                                       \
-      const unsigned g = resident_grid(k_hx_spin_lean<DT, true>, 256, smem, kMaxG);                      \
-      k_hx_spin_lean<DT, true><<<g, 256, smem, s>>>(h->dev, x, y, w->partials, w->ticket, dot_out);      \
-    } else {                                                                                             \
-      const unsigned g = resident_grid(k_hx_spin_lean<DT, false>, 256, smem, 1u << 20);                  \
-      k_hx_spin_lean<DT, false><<<g, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);           \
-    }                                                                                                    \
-  }
-  switch (t) {
-    case QK_C128: QKD_LEAN_LAUNCH(QK_C128); break;
-    case QK_C64: QKD_LEAN_LAUNCH(QK_C64); break;
-    case QK_F64: QKD_LEAN_LAUNCH(QK_F64); break;
-    case QK_F32: QKD_LEAN_LAUNCH(QK_F32); break;
-    default: return QKD_EINVAL;
-  }
-#undef QKD_LEAN_LAUNCH
-  QKD_LAUNCH_CHECK();
-  return QKD_OK;
-}
-
-int spin_apply_batched(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
-                       qk_workspace* w, double* dot_out) {
-  const size_t smem = size_t(1u << h->host.L) * 2;
-#define QKD_BATCH_LAUNCH(DT)                                                                               \
-  {                                                                                                        \
-    if (dot_out) {                                                                                         \
-      const unsigned g = resident_grid(k_hx_spin_batched<DT, true>, 256, smem, kMaxG);                     \
-      k_hx_spin_batched<DT, true><<<g, 256, smem, s>>>(h->dev, x, y, w->partials, w->ticket, dot_out);     \
-    } else {                                                                                               \
-      const unsigned g = resident_grid(k_hx_spin_batched<DT, false>, 256, smem, 1u << 20);                 \
-      k_hx_spin_batched<DT, false><<<g, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);          \
-    }                                                                                                      \
-  }
-  switch (t) {
-    case QK_C128: QKD_BATCH_LAUNCH(QK_C128); break;
-    case QK_C64: QKD_BATCH_LAUNCH(QK_C64); break;
-    case QK_F64: QKD_BATCH_LAUNCH(QK_F64); break;
-    case QK_F32: QKD_BATCH_LAUNCH(QK_F32); break;
-    default: return QKD_EINVAL;
-  }
-#undef QKD_BATCH_LAUNCH
-  QKD_LAUNCH_CHECK();
-  return QKD_OK;
-}
-
-int spin_apply_list(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
-                    qk_workspace* w, double* dot_out) {
-  const size_t smem = size_t(1u << h->host.L) * 2;
-#define QKD_LIST_LAUNCH(DT)                                                                              \
-  {                                                                                                      \
-    if (dot_out) {                                                                                       \
-      const unsigned g = resident_grid(k_hx_spin_list<DT, true>, 256, smem, kMaxG);                      \
-      k_hx_spin_list<DT, true><<<g, 256, smem, s>>>(h->dev, x, y, w->partials, w->ticket, dot_out);      \
-    } else {                                                                                             \
-      const unsigned g = resident_grid(k_hx_spin_list<DT, false>, 256, smem, 1u << 20);                  \
-      k_hx_spin_list<DT, false><<<g, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);           \
-    }                                                                                                    \
-  }
-  switch (t) {
-    case QK_C128: QKD_LIST_LAUNCH(QK_C128); break;
-    case QK_C64: QKD_LIST_LAUNCH(QK_C64); break;
-    case QK_F64: QKD_LIST_LAUNCH(QK_F64); break;
-    case QK_F32: QKD_LIST_LAUNCH(QK_F32); break;
-    default: return QKD_EINVAL;
-  }
-#undef QKD_LIST_LAUNCH
-  QKD_LAUNCH_CHECK();
-  return QKD_OK;
-}
-
-int spin_apply_staged(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
-                      qk_workspace* w, double* dot_out) {
-  const size_t es = (t == QK_C128 || t == QK_F64) ? 8 : 4;
-  const size_t planes = (t == QK_C128 || t == QK_C64) ? 2 : 1;
-  const size_t smem = es * planes * h->host.max_block;
-  if (smem > 200 * 1024) return QKD_EINVAL;
-  // Persistent grid: exactly the CTAs that fit at once (a second wave would
-  // only start after the first finished its whole share).
-  auto resident = [&](auto kern) {
-    int nb = 0;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 256, smem) != cudaSuccess || nb < 1) {
-      (void)cudaGetLastError();
-      nb = 1;
-    }
-    return unsigned(nb);
-  };
-  unsigned per_sm = 1;
-  switch (t) {
-    case QK_C128: per_sm = resident(k_hx_spin_staged<QK_C128, true>); break;
-    case QK_C64: per_sm = resident(k_hx_spin_staged<QK_C64, true>); break;
-    case QK_F64: per_sm = resident(k_hx_spin_staged<QK_F64, true>); break;
-    default: per_sm = resident(k_hx_spin_staged<QK_F32, true>); break;
-  }
-  const unsigned grid = std::min<unsigned>(1u << h->host.H, unsigned(sm_count(0)) * per_sm);
-#define QKD_STAGED_LAUNCH(DT)                                                                             \
-  {                                                                                                       \
-    auto kd = k_hx_spin_staged<DT, true>;                                                                 \
-    auto kn = k_hx_spin_staged<DT, false>;                                                                \
-    if (cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||  \
-        cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)    \
-      return QKD_EINVAL;                                                                                  \
-    if (dot_out) kd<<<std::min<unsigned>(grid, kMaxG), 256, smem, s>>>(h->dev, x, y, w->partials, w->ticket, \
-                                                                       dot_out);                          \
-    else kn<<<grid, 256, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);                             \
-  }
-  switch (t) {
-    case QK_C128: QKD_STAGED_LAUNCH(QK_C128); break;
-    case QK_C64: QKD_STAGED_LAUNCH(QK_C64); break;
-    case QK_F64: QKD_STAGED_LAUNCH(QK_F64); break;
-    case QK_F32: QKD_STAGED_LAUNCH(QK_F32); break;
-    default: return QKD_EINVAL;
-  }
-#undef QKD_STAGED_LAUNCH
-  QKD_LAUNCH_CHECK();
-  return QKD_OK;
-}
-
-int spin_apply_owner(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
-                     qk_workspace* w, double* dot_out) {
-  if (h->host.max_block > uint32_t(kOwnThreads * kOwnRows)) return QKD_EINVAL;
-  const size_t es = (t == QK_C128 || t == QK_F64) ? 8 : 4;
-  const size_t planes = (t == QK_C128 || t == QK_C64) ? 2 : 1;
-  const size_t smem = es * planes * h->host.max_block;
-  if (smem > 200 * 1024) return QKD_EINVAL;
-#define QKD_OWNER_LAUNCH(DT)                                                                              \
-  {                                                                                                       \
-    auto kd = k_hx_spin_owner<DT, true>;                                                                  \
-    auto kn = k_hx_spin_owner<DT, false>;                                                                 \
-    if (cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||  \
-        cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)    \
-      return QKD_EINVAL;                                                                                  \
-    const unsigned cap = 1u << h->host.H;                                                                 \
-    if (dot_out) kd<<<resident_grid(kd, kOwnThreads, smem, std::min<unsigned>(cap, kMaxG)), kOwnThreads, smem, s>>>( \
-        h->dev, x, y, w->partials, w->ticket, dot_out);                                                   \
-    else kn<<<resident_grid(kn, kOwnThreads, smem, cap), kOwnThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr); \
-  }
-  switch (t) {
-    case QK_C128: QKD_OWNER_LAUNCH(QK_C128); break;
-    case QK_C64: QKD_OWNER_LAUNCH(QK_C64); break;
-    case QK_F64: QKD_OWNER_LAUNCH(QK_F64); break;
-    case QK_F32: QKD_OWNER_LAUNCH(QK_F32); break;
-    default: return QKD_EINVAL;
-  }
-#undef QKD_OWNER_LAUNCH
-  QKD_LAUNCH_CHECK();
-  return QKD_OK;
-}
-
 int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
                     qk_workspace* w, double* dot_out) {
   if (!h->host.rows_ok || (h->host.gen && !h->host.diag_full)) return QKD_EINVAL;
@@ -2037,9 +1233,6 @@ int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
-
-// 0 block tiles, 1 warp tiles, 2 batched, 3 lists, 4 staged, 5 block owner, 6 rows
-static int g_spin_variant = 6;
 
 template <int DT, bool GEN, int LPR, int VPL>
 int launch_rows_block(const SpinHandle* h, qk_workspace* w, const void* X, void* Y, double* dots, cudaStream_t s,
@@ -2085,21 +1278,10 @@ int spin_plan_set_diag(SpinHandle* h, const double* diag) {
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out) {
   if (h->host.gen) return spin_apply_rows(h, t, x, y, s, w, dot_out);
-  if (h->lean && g_spin_variant == 6) {
+  if (h->lean) {  // the row kernel where its tables exist; otherwise the bond kernel below
     const int rc = spin_apply_rows(h, t, x, y, s, w, dot_out);
     if (rc != QKD_EINVAL) return rc;
   }
-  if (h->lean && g_spin_variant >= 5) {
-    const int rc = spin_apply_owner(h, t, x, y, s, w, dot_out);
-    if (rc != QKD_EINVAL) return rc;
-  }
-  if (h->lean && g_spin_variant >= 4) {
-    const int rc = spin_apply_staged(h, t, x, y, s, w, dot_out);
-    if (rc != QKD_EINVAL) return rc;  // block too large for shared memory: use the list kernel
-  }
-  if (h->lean && g_spin_variant >= 3) return spin_apply_list(h, t, x, y, s, w, dot_out);
-  if (h->lean && g_spin_variant == 2) return spin_apply_batched(h, t, x, y, s, w, dot_out);
-  if (h->lean && g_spin_variant == 1) return spin_apply_lean(h, t, x, y, s, w, dot_out);
   const size_t smem = h->host.smem;
   const unsigned grid = std::max(1u, std::min<unsigned>(h->host.ntiles, unsigned(sm_count(0)) * 1));
 #define QKD_SPIN_LAUNCH(DT)                                                                             \
@@ -2129,12 +1311,5 @@ int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStre
   return QKD_OK;
 }
 
-int spin_set_variant(int v) {
-  if (v < 0 || v > 6) return QKD_EINVAL;
-  g_spin_variant = v;
-  return QKD_OK;
-}
-
 }  // namespace qkd
 
-extern "C" int qkd_set_spin_variant(int v) { return qkd::spin_set_variant(v); }

@@ -264,7 +264,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_fwd_tc(TcArgs a) {
     group_sync(g);  // the next tile overwrites the activation tile and the accumulator
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
-  if (!ok && t == 0) atomicExch(a.err, 1);
+  if (!ok) {
+    if (t == 0) atomicExch(a.err, 1);
+    // the MMAs behind the expired wait may still be writing this group's
+    // columns: one more bounded wait on their commit before the columns are
+    // released (the host discards the results and reports the error either way)
+    (void)mbar_wait(mbar, phase);
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");

@@ -105,23 +105,28 @@ std::mutex g_setup_mu;
 unsigned char* g_scratch_addr[64] = {nullptr};
 
 // Once per device, with the device current: the array's device address.
-int scratch_address(int device, cudaStream_t s, unsigned char** out) {
+// Returns the CUDA error of a failed set-up step (cudaSuccess otherwise).
+cudaError_t scratch_address(int device, cudaStream_t s, unsigned char** out) {
   std::lock_guard<std::mutex> lk(g_setup_mu);
   if (!g_scratch_addr[device]) {
     void* ptr = nullptr;
-    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e == cudaSuccess && !ptr) e = cudaErrorInvalidSymbol;
+    if (e != cudaSuccess) {
       (void)cudaGetLastError();
-      return QKD_ECUDA;
+      return e;
     }
     unsigned char* base = static_cast<unsigned char*>(ptr);
-    if (cudaMemsetAsync(base + kTicketOff, 0, 256, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+    e = cudaMemsetAsync(base + kTicketOff, 0, 256, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
       (void)cudaGetLastError();
-      return QKD_ECUDA;
+      return e;
     }
     g_scratch_addr[device] = base;
   }
   *out = g_scratch_addr[device];
-  return QKD_OK;
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -145,20 +150,26 @@ extern "C" int qkrylov_b200_multi_dot_noalloc(int device, int dtype, size_t n, i
   }
   for (int j = 0; j < k; ++j)
     if (!V[j]) { qkapi::set_error("multi_dot_noalloc: null vector"); return -1; }
-  int prev = 0;
-  if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device >= ndev) {
     (void)cudaGetLastError();
-    qkapi::set_error("multi_dot_noalloc: cannot select the device");
+    qkapi::set_error("multi_dot_noalloc: invalid argument (device " + std::to_string(device) + " of " +
+                     std::to_string(ndev) + ")");
+    return -1;
+  }
+  int prev = 0;
+  cudaError_t e = cudaGetDevice(&prev);
+  if (e == cudaSuccess) e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    qkapi::set_error(std::string("multi_dot_noalloc: cannot select the device: ") + cudaGetErrorString(e));
     return -2;
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  int rc = QKD_OK;
   unsigned char* base = nullptr;
-  rc = scratch_address(device, s, &base);
-  if (rc == QKD_OK &&
-      cudaMemcpyAsync(base + kPtrOff, V, sizeof(void*) * k, cudaMemcpyHostToDevice, s) != cudaSuccess)
-    rc = QKD_ECUDA;
-  if (rc == QKD_OK) {
+  e = scratch_address(device, s, &base);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + kPtrOff, V, sizeof(void*) * k, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
     const size_t need = (n + 2047) / 2048;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
@@ -170,15 +181,14 @@ extern "C" int qkrylov_b200_multi_dot_noalloc(int device, int dtype, size_t n, i
       default: k_mdot_noalloc<QK_F32><<<G, kThreadsNA, 0, s>>>(n, k, x); break;
     }
     count_launch();
-    if (cudaPeekAtLastError() != cudaSuccess) rc = QKD_ECUDA;
+    e = cudaPeekAtLastError();
   }
-  if (rc == QKD_OK &&
-      (cudaMemcpyAsync(out, base + kResultOff, sizeof(double) * 2 * k, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-       cudaStreamSynchronize(s) != cudaSuccess))
-    rc = QKD_ECUDA;
-  if (rc != QKD_OK) {
-    qkapi::set_error(std::string("multi_dot_noalloc: ") + cudaGetErrorString(cudaGetLastError()));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, base + kResultOff, sizeof(double) * 2 * k, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    qkapi::set_error(std::string("multi_dot_noalloc: ") + cudaGetErrorString(e));
   }
   cudaSetDevice(prev);
-  return rc == QKD_OK ? 0 : -2;
+  return e == cudaSuccess ? 0 : -2;
 }

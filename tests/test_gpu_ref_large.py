@@ -1,0 +1,73 @@
+"""The GPU solvers against the reference's own CPU solvers (oracle/_ref: its
+unchanged sources) at sizes beyond the golden fixtures, on the GPU box:
+
+* continued fraction of S(q = pi, omega) on the periodic Heisenberg chain
+  N = 24 (dim 2,704,156; the reference's CSR is ~2.3 GB): the same start
+  vector phi0 = Sz(pi)|psi0> fed to the reference's
+  continued_fraction_coeffs (src/solvers/dynamics.cpp:12-59) and to the
+  library's, 300 steps; S(omega) on [0, 4] at eta = 0.05 with
+  evaluate_spectral_function semantics (dynamics.cpp:61-89);
+* FTLM on the t-J chain N = 14, 2 holes (dim 84,084) at several
+  temperatures with the reference's Gaussian stream (src/solvers/ftlm.cpp:
+  122-170): Z, U, Cv within 1e-10 relative.
+
+Skipped where oracle/_ref was not built (no reference checkout)."""
+import numpy as np
+import pytest
+
+import oracle as O
+import qkrylov_b200 as qk
+from oracle import bethe
+from test_gpu_hx import ham
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref (the reference's own build) is absent")]
+
+
+def szq_vector(states, N, q):
+    bits = ((states[:, None] >> np.arange(N, dtype=np.uint64)[None, :]) & np.uint64(1)).astype(np.float64)
+    sz = bits - 0.5
+    phase = np.exp(1j * q * np.arange(N))
+    return (sz * phase[None, :]).sum(axis=1) / np.sqrt(N)
+
+
+def test_structure_factor_n24_matches_reference():
+    N = 24
+    sec = dict(use_sz=1, sz2=0)
+    H = ham("spin", N, sec, O.heisenberg_chain(N))
+    gs = qk.lanczos_fp64(H, seed=7, tol=1e-12, eigenvector=True)
+    assert gs.converged and abs(gs.energy - bethe.ground_energy(N)) < 1e-10
+    states = qk.SpinHalfBasis(N, sz=0).states()
+    phi = szq_vector(states, N, np.pi) * gs.eigenvector
+    ref = O.ref().hamiltonian("spin", N, sec, O.heisenberg_chain(N))
+    c_ref = ref.cf(phi, 300)
+    del ref
+    c = qk.continued_fraction_coeffs(H, phi, 300)
+    assert len(c.alphas) == len(c_ref["alphas"]) == 300
+    assert abs(c.norm_phi0 - c_ref["norm_phi0"]) <= 1e-14 * c_ref["norm_phi0"]
+    # the leading coefficients fix the low moments of the spectral measure
+    a, b = np.asarray(c.alphas), np.asarray(c.betas)
+    ar, br = np.asarray(c_ref["alphas"]), np.asarray(c_ref["betas"])
+    assert np.abs(a[:20] - ar[:20]).max() <= 1e-10 and np.abs(b[:20] - br[:20]).max() <= 1e-10
+    omega = np.linspace(0.0, 4.0, 2001)
+    E0 = gs.energy
+    S = np.array([qk.evaluate_spectral_function(c, w, E0, 0.05) for w in omega])
+    S_ref = np.array([O.ref().spectral(ar, br, c_ref["norm_phi0"], w, E0, 0.05) for w in omega])
+    assert np.abs(S - S_ref).max() <= 1e-10 * np.abs(S_ref).max()
+
+
+def test_ftlm_tj14_matches_reference_at_several_temperatures():
+    N, ne = 14, 12
+    sec = dict(use_nup=1, nup=ne // 2, use_ndn=1, ndn=ne - ne // 2)
+    terms = O.tj_chain(N, 1.0, 0.4)
+    betas = [0.1, 1.0, 4.0, 10.0]
+    R, M = 16, 60
+    ref = O.ref().hamiltonian("tj", N, sec, terms)
+    want = [ref.ftlm(b, R, M) for b in betas]
+    del ref
+    H = ham("tj", N, sec, terms)
+    got = qk.ftlm_sweep(H, betas, R, M)
+    for f, r in zip(want, got):
+        assert abs(r.partition_function - f["Z"]) <= 1e-10 * abs(f["Z"])
+        assert abs(r.internal_energy - f["U"]) <= 1e-10 * max(1.0, abs(f["U"]))
+        assert abs(r.specific_heat - f["Cv"]) <= 1e-10 * max(1.0, abs(f["Cv"]))
