@@ -32,10 +32,15 @@ uint64_t qkrylov_b200_launch_count(void);
 int qkrylov_b200_device_count(void);
 /* 0 (default): H.x uses the specialised row kernels (one CTA per sector
  * block, x of the block staged in shared memory, per-row class tables)
- * wherever the compiled operator has their tables; 1: the generic kernel
- * everywhere.  For comparisons; process-wide.  Other values:
- * QKRYLOV_ERROR_INVALID_ARG. */
+ * wherever the compiled operator has their tables, with per-die work queues
+ * on a two-die GPU; 1: the generic kernel everywhere; 2: as 0 with the
+ * blocks handed out in one grid-stride order (no per-die queues).  For
+ * comparisons; process-wide.  Other values: QKRYLOV_ERROR_INVALID_ARG. */
 int qkrylov_b200_set_kernel_policy(int policy);
+/* Dies of the current device as the row kernels' topology probe measured
+ * them (2 on a B200, 1 where the probe saw one) and the SMs of each (first
+ * call on a device: a few probe launches; later calls: cached). */
+int qkrylov_b200_die_count(int* sms_die0, int* sms_die1);
 
 /* Select which of N_up / N_dn a sector conserves after
  * qkrylov_sector_set_hubbard_particles (c_api.h:33), which always sets
@@ -95,6 +100,18 @@ int qkrylov_hamiltonian_diagonal_complex_f64(qkrylov_hamiltonian_h h, double* di
  * (matrix_free_hamiltonian.hpp:38) as a C entry point. */
 int qkrylov_hamiltonian_apply_device(qkrylov_hamiltonian_h h, int dtype, const void* x, void* y, void* stream);
 int qkrylov_hamiltonian_diagonal_device(qkrylov_hamiltonian_h h, int dtype, void* diag, void* stream);
+/* Row sharding of H.x over several GPUs (no counterpart in the reference;
+ * it parallelises the row loop of matrix_free_hamiltonian.cpp:140-168
+ * within one device).  qkrylov_b200_basis_shard_bounds writes nshards + 1
+ * row bounds at sector-block boundaries (bounds[0] = 0, bounds[nshards] =
+ * dim, shard k = [bounds[k], bounds[k+1]), rows as even as block
+ * boundaries allow); host only, no GPU needed.
+ * qkrylov_hamiltonian_apply_range_device computes rows [row_lo, row_hi) of
+ * y = H x from the complete x (the other rows of y are not written); the
+ * bounds must be block boundaries (QKRYLOV_ERROR_INVALID_ARG otherwise). */
+int qkrylov_b200_basis_shard_bounds(qkrylov_basis_h basis, int nshards, uint64_t* bounds_out);
+int qkrylov_hamiltonian_apply_range_device(qkrylov_hamiltonian_h h, int dtype, const void* x, void* y,
+                                           uint64_t row_lo, uint64_t row_hi, void* stream);
 
 /* ------------------------------------------------------ device vector ops
  * Multi-vector dot out[2j..2j+1] = <V_j, x> = sum_i conj(V_j[i]) x[i] for
@@ -142,9 +159,44 @@ int qkrylov_davidson_lowest_f64(qkrylov_hamiltonian_h h, int n_eig, int max_subs
 int qkrylov_continued_fraction_coeffs_f64(qkrylov_hamiltonian_h h, const double* phi0_complex, int n_iter,
                                           double* alphas_out, double* betas_out, double* norm_phi0_out,
                                           int* n_alpha_out, int* n_beta_out);
+/* continued_fraction_coeffs with a checkpoint of its state, for long runs
+ * that must survive an interruption.  No counterpart in the reference (its
+ * examples/hdf5_storage.py stores final results only).  Starts from
+ * phi0_complex, or, when resume_dir is not NULL, continues the run saved
+ * there (phi0 is then ignored); runs until n_iter steps in total (or
+ * beta < 1e-15); when save_dir is not NULL writes the state there as .npy
+ * files numpy reads: alphas.npy, betas.npy, norm_phi0.npy, state.npy
+ * ([steps, stopped]) and the current and previous Lanczos vectors v.npy,
+ * v_prev.npy (complex128).  A run resumed from a checkpoint gives the same
+ * coefficients, bit for bit, as one uninterrupted run.  alphas_out and
+ * betas_out hold n_iter doubles; the directories must exist. */
+int qkrylov_b200_cf_checkpointed(qkrylov_hamiltonian_h h, const double* phi0_complex, const char* resume_dir,
+                                 int n_iter, const char* save_dir, double* alphas_out, double* betas_out,
+                                 double* norm_phi0_out, int* n_alpha_out, int* n_beta_out);
 /* evaluate_spectral_function (dynamics.hpp:28-38); betas has n-1 entries */
 double qkrylov_evaluate_spectral_function_f64(const double* alphas, const double* betas, size_t n,
                                               double norm_phi0, double omega, double E0, double eta);
+/* evaluate_spectral_function (dynamics.cpp:61-89) for ncols continued
+ * fractions at n_omega frequencies in one call, evaluated on `device`
+ * (one GPU thread per fraction and frequency, FP64).  Fraction c has its
+ * alphas and betas at c*ld (betas: its first lengths[c]-1 entries),
+ * lengths[c] <= ld coefficients (lengths NULL: ld each) and norm
+ * norm_phi0[c] (NULL: 1); out[c*n_omega + k] = S_c(omegas[k]).  Host
+ * arrays; waits for the result.  No counterpart in the reference (it
+ * evaluates one frequency of one fraction per call). */
+int qkrylov_b200_spectral_function_batch(int device, int ncols, int ld, const double* alphas, const double* betas,
+                                         const int* lengths, const double* norm_phi0, size_t n_omega,
+                                         const double* omegas, double E0, double eta, double* out);
+/* Apply the operator an OpSum defines on a basis to a device vector, once:
+ * y = O x with the reference's H.x convention (y[a] = sum over terms of
+ * conj(amplitude) x[T a], matrix_free_hamiltonian.cpp:45-91 and 140-168),
+ * without keeping a Hamiltonian handle; e.g. Sz(q)|psi> for a dynamical
+ * structure factor, or with `expectation` (2 doubles, may be NULL) the
+ * value <x|y> of a correlation function.  x, y: dim elements of dtype on
+ * `device` (real dtypes need a real operator); waits for the result.  No
+ * counterpart in the reference's C ABI. */
+int qkrylov_b200_apply_operator(qkrylov_basis_h basis, qkrylov_site_h site, qkrylov_opsum_h opsum, int device,
+                                int dtype, const void* x, void* y, double* expectation);
 /* ftlm (ftlm.hpp:21-27) at n_beta inverse temperatures from one set of
  * random-vector tridiagonals; entry q equals ftlm(h, betas[q], ...). */
 int qkrylov_ftlm_sweep_f64(qkrylov_hamiltonian_h h, int n_beta, const double* betas, int n_random, int n_steps,

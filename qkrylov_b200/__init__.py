@@ -760,8 +760,30 @@ class DynamicsResult:
         self.alphas, self.betas, self.norm_phi0 = np.asarray(alphas), np.asarray(betas), norm_phi0
 
 
-def continued_fraction_coeffs(H: MatrixFreeHamiltonian, phi0: np.ndarray, n_iter: int = 100) -> DynamicsResult:
+def continued_fraction_coeffs(H: MatrixFreeHamiltonian, phi0: Optional[np.ndarray], n_iter: int = 100,
+                              save: Optional[str] = None, resume: Optional[str] = None) -> DynamicsResult:
+    """The reference's continued_fraction_coeffs.  With `save` and/or
+    `resume` (directories; FP64 operators only) the run writes / continues
+    a checkpoint of its state (.npy files: alphas, betas, norm_phi0, state,
+    v, v_prev); `n_iter` counts all steps, a resumed run matches an
+    uninterrupted one bit for bit."""
     L = lib()
+    if save is not None or resume is not None:
+        if H.dtype != np.float64:
+            raise ValueError("checkpointed continued fractions run on FP64 operators")
+        p = None if resume is not None else np.ascontiguousarray(phi0, dtype=np.complex128)
+        if p is not None and p.shape != (H.dimension,):
+            raise ValueError("phi0 vector size does not match Hamiltonian dimension")
+        a, b = np.zeros(n_iter), np.zeros(n_iter)
+        nrm, na, nb = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        if save is not None:
+            os.makedirs(save, exist_ok=True)
+        _check(L.qkrylov_b200_cf_checkpointed(H._h, p.ctypes.data if p is not None else None,
+                                              resume.encode() if resume is not None else None, n_iter,
+                                              save.encode() if save is not None else None, a.ctypes.data,
+                                              b.ctypes.data, ctypes.byref(nrm), ctypes.byref(na), ctypes.byref(nb)),
+               "continued_fraction_coeffs")
+        return DynamicsResult(a[:na.value].copy(), b[:nb.value].copy(), nrm.value)
     phi0 = np.ascontiguousarray(phi0, dtype=H.cdtype)
     if phi0.shape != (H.dimension,):
         raise ValueError("phi0 vector size does not match Hamiltonian dimension")
@@ -835,6 +857,87 @@ def evaluate_spectral_function(res: DynamicsResult, omega: float, E0: float, eta
                                                         res.norm_phi0, omega, E0, eta)
 
 
+def spectral_function_batch(results, omegas, E0: float, eta: float = 0.1, device: int = 0) -> np.ndarray:
+    """evaluate_spectral_function for many continued fractions at many
+    frequencies in one GPU call.  `results`: a DynamicsResult or a sequence
+    of them (fractions of different lengths allowed).  Returns S with shape
+    (len(omegas),) for one result, (len(results), len(omegas)) otherwise."""
+    single = isinstance(results, DynamicsResult)
+    rs = [results] if single else list(results)
+    w = np.ascontiguousarray(omegas, dtype=np.float64)
+    ld = max([len(r.alphas) for r in rs] + [1])
+    A = np.zeros((len(rs), ld))
+    Bt = np.zeros((len(rs), ld))
+    lens = np.zeros(len(rs), dtype=np.int32)
+    nrm = np.zeros(len(rs))
+    for c, r in enumerate(rs):
+        n = len(r.alphas)
+        A[c, :n] = r.alphas
+        nb = min(len(r.betas), max(n - 1, 0))
+        Bt[c, :nb] = np.asarray(r.betas, dtype=np.float64)[:nb]
+        lens[c] = n
+        nrm[c] = r.norm_phi0
+    out = np.zeros((len(rs), len(w)))
+    _check(lib().qkrylov_b200_spectral_function_batch(device, len(rs), ld, A.ctypes.data, Bt.ctypes.data,
+                                                      lens.ctypes.data, nrm.ctypes.data, len(w), w.ctypes.data,
+                                                      E0, eta, out.ctypes.data), "spectral_function_batch")
+    return out[0] if single else out
+
+
+def apply_operator(basis: "Basis", site: "Site", ops: "OpSum", x, expectation: bool = False, device: int = 0):
+    """y = O x for the operator an OpSum defines on `basis` (the reference's
+    H.x convention), without keeping a Hamiltonian.  `x`: a numpy vector
+    (copied to the GPU and back; complex128, or float64 for a real
+    operator) or a torch CUDA tensor (used in place; the result is a tensor
+    of the same dtype).  With expectation=True also returns <x|O x>."""
+    codes = {"complex128": DTYPE_C128, "complex64": DTYPE_C64, "float64": DTYPE_F64, "float32": DTYPE_F32}
+    is_torch = hasattr(x, "data_ptr")
+    if is_torch:
+        import torch
+        xt = x.contiguous()
+        code = codes[str(xt.dtype).replace("torch.", "")]
+    else:
+        import torch
+        xa = np.ascontiguousarray(x)
+        if xa.dtype not in (np.complex128, np.float64):
+            xa = xa.astype(np.complex128)
+        xt = torch.from_numpy(xa).to(f"cuda:{device}")
+        code = codes[str(xa.dtype)]
+    yt = torch.empty_like(xt)
+    e = np.zeros(2)
+    _check(lib().qkrylov_b200_apply_operator(basis._h, site._handle(), ops._handle(), device, code,
+                                             ctypes.c_void_p(xt.data_ptr()), ctypes.c_void_p(yt.data_ptr()),
+                                             e.ctypes.data if expectation else None), "apply_operator")
+    y = yt if is_torch else yt.cpu().numpy()
+    return (y, complex(e[0], e[1])) if expectation else y
+
+
+def save_result(path: str, result) -> None:
+    """Store a ground-state or Davidson result under `path` (a directory)
+    with the dataset names of the reference's examples/hdf5_storage.py:5-13
+    (energy and eigenvector; eigenvalues and eigenvector_<i>), one .npy file
+    per dataset (h5py is not a dependency of this package)."""
+    os.makedirs(path, exist_ok=True)
+    if hasattr(result, "eigenvalues"):
+        np.save(os.path.join(path, "eigenvalues.npy"), np.asarray(result.eigenvalues, dtype=np.float64))
+        for i, v in enumerate(getattr(result, "eigenvectors", None) or []):
+            np.save(os.path.join(path, f"eigenvector_{i}.npy"), np.asarray(v))
+    else:
+        np.save(os.path.join(path, "energy.npy"), np.float64(result.energy))
+        if getattr(result, "eigenvector", None) is not None:
+            np.save(os.path.join(path, "eigenvector.npy"), np.asarray(result.eigenvector))
+
+
+def load_result(path: str) -> dict:
+    """The datasets save_result wrote, as a dict of numpy values."""
+    out = {}
+    for f in sorted(os.listdir(path)):
+        if f.endswith(".npy"):
+            v = np.load(os.path.join(path, f))
+            out[f[:-4]] = v.item() if v.shape == () else v
+    return out
+
+
 class FTLMResult:
     def __init__(self, beta, Z, U, Cv):
         self.beta, self.partition_function, self.internal_energy, self.specific_heat = beta, Z, U, Cv
@@ -856,10 +959,20 @@ def ftlm(H: MatrixFreeHamiltonian, beta: float, n_random: int = 50, n_steps: int
     return FTLMResult(r.beta, r.partition_function, r.internal_energy, r.specific_heat)
 
 
+def die_count():
+    """(dies, SMs on die 0, SMs on die 1) of the current device as the row
+    kernels' topology probe measured them; (1, 0, 0) where it saw one die."""
+    a, b = ctypes.c_int(0), ctypes.c_int(0)
+    n = lib().qkrylov_b200_die_count(ctypes.byref(a), ctypes.byref(b))
+    return int(n), a.value, b.value
+
+
 def set_kernel_policy(policy: str):
     """'auto' (the specialised row kernels where the operator has their
-    tables) or 'generic' (the term-walk kernel only, for comparisons)."""
-    codes = {"auto": 0, "generic": 1}
+    tables, per-die work queues on a two-die GPU), 'generic' (the term-walk
+    kernel only) or 'no-die-queues' (auto with one grid-stride order), for
+    comparisons."""
+    codes = {"auto": 0, "generic": 1, "no-die-queues": 2}
     _check(lib().qkrylov_b200_set_kernel_policy(codes[policy]), "set_kernel_policy")
 
 

@@ -73,6 +73,7 @@ PROTOTYPES = {
     "qkrylov_b200_device_count": (_i, []),
     "qkrylov_b200_sector_set_species": (_i, [_vp, _i, _i]),
     "qkrylov_b200_set_kernel_policy": (_i, [_i]),
+    "qkrylov_b200_die_count": (_i, [_vp, _vp]),
     "qkrylov_hamiltonian_kernel": (_i, [_vp]),
     "qkrylov_b200_site_apply": (_i, [_vp, _cp, _i, _u64, _vp, _vp, _vp]),
     "qkrylov_basis_states": (_i, [_vp, _u64, _u64, _vp]),
@@ -95,6 +96,11 @@ PROTOTYPES = {
     "qkrylov_davidson_lowest_f64": (_i, [_vp, _i, _i, _d, _vp, _vp, _vp]),
     "qkrylov_continued_fraction_coeffs_f64": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "qkrylov_evaluate_spectral_function_f64": (_d, [_vp, _vp, _sz, _d, _d, _d, _d]),
+    "qkrylov_b200_spectral_function_batch": (_i, [_i, _i, _i, _vp, _vp, _vp, _vp, _sz, _vp, _d, _d, _vp]),
+    "qkrylov_b200_apply_operator": (_i, [_vp, _vp, _vp, _i, _i, _vp, _vp, _vp]),
+    "qkrylov_b200_cf_checkpointed": (_i, [_vp, _vp, _cp, _i, _cp, _vp, _vp, _vp, _vp, _vp]),
+    "qkrylov_b200_basis_shard_bounds": (_i, [_vp, _i, _vp]),
+    "qkrylov_hamiltonian_apply_range_device": (_i, [_vp, _i, _vp, _vp, _u64, _u64, _vp]),
     "qkrylov_ftlm_sweep_f64": (_i, [_vp, _i, _vp, _i, _i, _vp, _vp, _vp]),
     "qkrylov_b200_lanczos_mixed": (_i, [_vp, _u64, _vp, _i, _i, _d, _vp, _vp, _i, _vp, _vp, _vp]),
     "qkrylov_b200_lanczos_fp64": (_i, [_vp, _u64, _vp, _i, _i, _d, _vp, _vp, _i, _vp, _vp, _vp]),

@@ -42,11 +42,13 @@ int qkrylov_b200_device_count(void) {
 
 int qkrylov_b200_set_kernel_policy(int policy) {
   // 0 auto (the specialised kernels where the operator has their tables),
-  // 1 the generic term-walk kernel only
-  if (policy < 0 || policy > 1) return QKRYLOV_ERROR_INVALID_ARG;
+  // 1 the generic term-walk kernel only, 2 auto without per-die work queues
+  if (policy < 0 || policy > 2) return QKRYLOV_ERROR_INVALID_ARG;
   qkd_set_kernel_policy(policy);
   return QKRYLOV_SUCCESS;
 }
+
+int qkrylov_b200_die_count(int* sms_die0, int* sms_die1) { return qkd_die_count(sms_die0, sms_die1); }
 
 int qkrylov_hamiltonian_kernel(qkrylov_hamiltonian_h h) { return (h && h->op) ? qkd_plan_kernel(h->op->plan()) : 0; }
 
@@ -194,6 +196,33 @@ int qkrylov_hamiltonian_apply_device(qkrylov_hamiltonian_h h, int dtype, const v
   });
 }
 
+int qkrylov_b200_basis_shard_bounds(qkrylov_basis_h basis, int nshards, uint64_t* bounds_out) {
+  if (!basis || !basis->table || nshards < 1 || !bounds_out) return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    const std::vector<uint64_t> b = basis->table->shard_bounds(nshards);
+    std::copy(b.begin(), b.end(), bounds_out);
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_hamiltonian_apply_range_device(qkrylov_hamiltonian_h h, int dtype, const void* x, void* y,
+                                           uint64_t row_lo, uint64_t row_hi, void* stream) {
+  if (!h || !h->op || !x || !y || !valid_dtype(dtype) || row_lo > row_hi || row_hi > h->op->dim())
+    return QKRYLOV_ERROR_INVALID_ARG;
+  if (!h->op->basis().is_block_start(row_lo) || !h->op->basis().is_block_start(row_hi)) {
+    qkapi::set_error("apply_range: the row bounds are not sector-block boundaries (qkrylov_b200_basis_shard_bounds)");
+    return QKRYLOV_ERROR_INVALID_ARG;
+  }
+  return guarded([&] {
+    auto& c = h->op->ctx();
+    const int rc = qkd_apply_range(h->op->plan(), qk_dtype(dtype), x, y, row_lo, row_hi,
+                                   stream ? cudaStream_t(stream) : c.stream);
+    if (rc == QKD_EINVAL) { qkapi::set_error("invalid dtype for this operator or aliased x/y"); return QKRYLOV_ERROR_INVALID_ARG; }
+    qkb::qkd_check(rc, "H.x rows");
+    return QKRYLOV_SUCCESS;
+  });
+}
+
 int qkrylov_hamiltonian_diagonal_device(qkrylov_hamiltonian_h h, int dtype, void* d, void* stream) {
   if (!h || !h->op || !d || !valid_dtype(dtype)) return QKRYLOV_ERROR_INVALID_ARG;
   return guarded([&] {
@@ -201,6 +230,80 @@ int qkrylov_hamiltonian_diagonal_device(qkrylov_hamiltonian_h h, int dtype, void
     const int rc = qkd_diagonal(h->op->plan(), qk_dtype(dtype), d, stream ? cudaStream_t(stream) : c.stream);
     if (rc == QKD_EINVAL) return QKRYLOV_ERROR_INVALID_ARG;
     qkb::qkd_check(rc, "diagonal");
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_spectral_function_batch(int device, int ncols, int ld, const double* alphas, const double* betas,
+                                         const int* lengths, const double* norm_phi0, size_t n_omega,
+                                         const double* omegas, double E0, double eta, double* out) {
+  if (device < 0 || ncols < 0 || ld < 0 || (ncols > 0 && n_omega > 0 && (!alphas || !betas || !omegas || !out)) ||
+      ncols > 65535)
+    return QKRYLOV_ERROR_INVALID_ARG;
+  if (lengths)
+    for (int c = 0; c < ncols; ++c)
+      if (lengths[c] < 0 || lengths[c] > ld) return QKRYLOV_ERROR_INVALID_ARG;
+  if (ncols == 0 || n_omega == 0) return QKRYLOV_SUCCESS;
+  return guarded([&] {
+    auto& c = qkb::Context::get(device);
+    c.activate();
+    const size_t nc = size_t(ncols) * size_t(ld);
+    const size_t bytes = (2 * nc + size_t(ncols) + n_omega + size_t(ncols) * n_omega) * sizeof(double) +
+                         size_t(ncols) * sizeof(int);
+    char* buf = static_cast<char*>(c.alloc(bytes));
+    double* da = reinterpret_cast<double*>(buf);
+    double* db = da + nc;
+    double* dn = db + nc;
+    double* dw = dn + ncols;
+    double* dout = dw + n_omega;
+    int* dl = reinterpret_cast<int*>(dout + size_t(ncols) * n_omega);
+    int rc = QKD_OK;
+    try {
+      auto h2d = [&](void* d, const void* h, size_t b) {
+        if (b) qkb::cuda_check(cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, c.stream), "H2D");
+      };
+      h2d(da, alphas, nc * sizeof(double));
+      h2d(db, betas, nc * sizeof(double));
+      if (norm_phi0) h2d(dn, norm_phi0, size_t(ncols) * sizeof(double));
+      if (lengths) h2d(dl, lengths, size_t(ncols) * sizeof(int));
+      h2d(dw, omegas, n_omega * sizeof(double));
+      rc = qkd_spectral_batch(da, db, lengths ? dl : nullptr, ncols, ld, norm_phi0 ? dn : nullptr, dw, n_omega, E0,
+                              eta, dout, c.stream);
+      if (rc == QKD_OK)
+        qkb::cuda_check(cudaMemcpyAsync(out, dout, size_t(ncols) * n_omega * sizeof(double), cudaMemcpyDeviceToHost,
+                                        c.stream), "D2H");
+      c.sync();
+    } catch (...) {
+      c.release(buf);
+      throw;
+    }
+    c.release(buf);
+    qkb::qkd_check(rc, "spectral function batch");
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_apply_operator(qkrylov_basis_h basis, qkrylov_site_h site, qkrylov_opsum_h opsum, int device,
+                                int dtype, const void* x, void* y, double* expectation) {
+  if (!basis || !basis->table || !site || !opsum || device < 0 || !valid_dtype(dtype) || !x || !y || x == y)
+    return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    qkb::Operator op(site->family, basis->table, opsum->terms, device);
+    const qk_dtype t = qk_dtype(dtype);
+    if (!qk_dtype_complex(t) && !op.all_real()) {
+      qkapi::set_error("apply_operator: a complex operator needs complex vectors");
+      return QKRYLOV_ERROR_INVALID_ARG;
+    }
+    auto& c = op.ctx();
+    if (expectation) {
+      op.apply_dot(t, x, y, c.dres(0));
+      const double* v = c.fetch(c.dres(0), 2);
+      expectation[0] = v[0];
+      expectation[1] = v[1];
+    } else {
+      op.apply(t, x, y);
+      c.sync();
+    }
     return QKRYLOV_SUCCESS;
   });
 }
@@ -579,6 +682,27 @@ int qkrylov_continued_fraction_coeffs_f64(qkrylov_hamiltonian_h h, const double*
   if (!h || !h->op || !phi0 || !alphas || !betas || !norm_phi0 || n_iter <= 0) return QKRYLOV_ERROR_INVALID_ARG;
   return guarded([&] {
     auto r = qkb::continued_fraction<double>(*h->op, reinterpret_cast<const std::complex<double>*>(phi0), n_iter);
+    *norm_phi0 = r.norm_phi0;
+    std::copy(r.alphas.begin(), r.alphas.end(), alphas);
+    std::copy(r.betas.begin(), r.betas.end(), betas);
+    if (na) *na = int(r.alphas.size());
+    if (nb) *nb = int(r.betas.size());
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_cf_checkpointed(qkrylov_hamiltonian_h h, const double* phi0, const char* resume_dir, int n_iter,
+                                 const char* save_dir, double* alphas, double* betas, double* norm_phi0, int* na,
+                                 int* nb) {
+  if (!h || !h->op || (!phi0 && !resume_dir) || !alphas || !betas || !norm_phi0 || n_iter <= 0)
+    return QKRYLOV_ERROR_INVALID_ARG;
+  return guarded([&] {
+    auto r = qkb::continued_fraction_checkpointed(*h->op, resume_dir ? nullptr : reinterpret_cast<const std::complex<double>*>(phi0),
+                                                  resume_dir ? resume_dir : "", n_iter, save_dir ? save_dir : "");
+    if (int(r.alphas.size()) > n_iter) {  // a checkpoint longer than the requested run
+      qkapi::set_error("cf_checkpointed: the checkpoint holds more steps than n_iter");
+      return QKRYLOV_ERROR_INVALID_ARG;
+    }
     *norm_phi0 = r.norm_phi0;
     std::copy(r.alphas.begin(), r.alphas.end(), alphas);
     std::copy(r.betas.begin(), r.betas.end(), betas);

@@ -143,4 +143,37 @@ uint64_t SectorTable::state(uint64_t i) const {
   return (h << L) | llist[key_off[block_need(h)] + r];
 }
 
+std::vector<uint64_t> SectorTable::shard_bounds(int nshards) const {
+  if (nshards < 1) throw std::invalid_argument("qkrylov_b200: shard count must be at least 1");
+  std::vector<uint64_t> starts;  // block starts in ascending row order
+  for (uint64_t h = 0; h < A.size(); ++h)
+    if (block_need(h) != kEmptyBlockKey && block_size(h) > 0) starts.push_back(block_offset(h));
+  starts.push_back(dim);
+  std::vector<uint64_t> b(size_t(nshards) + 1, 0);
+  b[nshards] = dim;
+  size_t j = 0;
+  for (int k = 1; k < nshards; ++k) {
+    const double want = double(dim) * k / nshards;
+    while (j + 1 < starts.size() && double(starts[j + 1]) <= want) ++j;
+    uint64_t pick = starts[j];
+    if (j + 1 < starts.size() && double(starts[j + 1]) - want < want - double(starts[j])) pick = starts[j + 1];
+    b[k] = std::max(pick, b[k - 1]);
+  }
+  return b;
+}
+
+bool SectorTable::is_block_start(uint64_t r) const {
+  if (r == dim || r == 0) return true;
+  // block offsets ascend with h: binary search over the high parts
+  uint64_t lo = 0, hi = A.size();
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) / 2;
+    if (block_offset(mid) < r) lo = mid + 1;
+    else hi = mid;
+  }
+  for (uint64_t h = lo; h < A.size() && block_offset(h) == r; ++h)
+    if (block_need(h) != kEmptyBlockKey && block_size(h) > 0) return true;
+  return false;
+}
+
 }  // namespace qkb

@@ -75,6 +75,12 @@ class SectorTable {
   uint64_t block_offset(uint64_t h) const { return A[h] & kOffsetMask; }
   uint32_t block_need(uint64_t h) const { return uint32_t(A[h] >> 56); }
   uint64_t block_size(uint64_t h) const;
+  // nshards + 1 row bounds at sector-block boundaries (0 and dim at the
+  // ends), each as close as a block boundary gets to k * dim / nshards:
+  // contiguous row ranges for a row-sharded H.x.
+  std::vector<uint64_t> shard_bounds(int nshards) const;
+  // true when row r starts a sector block (or is dim)
+  bool is_block_start(uint64_t r) const;
 };
 
 }  // namespace qkb

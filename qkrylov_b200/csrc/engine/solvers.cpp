@@ -1,6 +1,8 @@
 #include "solvers.hpp"
+#include "npy.hpp"
 
 #include <algorithm>
+#include <cstring>
 #include <chrono>
 #include <cmath>
 #include <numeric>
@@ -436,7 +438,12 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
 // vectors u = V y.  Corrections t = r / (diag - theta) (the reference's
 // clamped preconditioner) are orthogonalised against V twice (classical
 // Gram-Schmidt) and appended; when V would exceed max_subspace it restarts
-// from the lowest 2*block Ritz vectors (T becomes diagonal).
+// from the lowest 2*block Ritz vectors (T becomes diagonal) plus the block's
+// Ritz vectors of the previous iteration (GD+k, Stathopoulos & Saad 1998,
+// "Restarting techniques for the (Jacobi-)Davidson symmetric eigenvalue
+// methods"): the pair (current, previous) Ritz vector spans the direction of
+// the recurrence a plain thick restart discards, which keeps the upper pairs
+// converging at the rate they had before the restart.
 DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int block, int max_subspace, double tol,
                                 uint64_t seed, int maxiter, double* evecs_out) {
   if (t != QK_F32 && t != QK_F64) throw std::invalid_argument("qkrylov_b200: block Davidson needs real vectors");
@@ -453,7 +460,7 @@ DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int bl
   H.diagonal(t, diag.data());
   std::vector<DevVec> V;
   V.reserve(max_subspace);
-  std::vector<DevVec> U(2 * block), R(block);
+  std::vector<DevVec> U(2 * block), R(block), Uprev(block);
   DevVec w = d.vec(false);
   PtrArray P(size_t(max_subspace) + 4, dev);
   DevVec coef(size_t(2) * (max_subspace + 8), QK_F64, dev);
@@ -501,11 +508,13 @@ DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int bl
     }
     m_proj = m;
     jacobi_symmetric(T, m, theta, Y);
-    // Ritz vectors and residuals of the lowest nb pairs
+    // Ritz vectors and residuals of the lowest nb pairs; the previous
+    // iteration's Ritz vectors move to Uprev (kept for the restart)
     const int nb = std::min(block, m);
     std::vector<double> cz(2 * size_t(m));
     double worst = 0.0;
     out.residuals.assign(nb, 0.0);
+    for (int a = 0; a < nb; ++a) std::swap(U[a], Uprev[a]);
     for (int a = 0; a < nb; ++a) {
       for (int i = 0; i < m; ++i) { cz[2 * i] = Y[size_t(i) * m + a]; cz[2 * i + 1] = 0.0; }
       cuda_check(cudaMemcpyAsync(cd, cz.data(), sizeof(double) * 2 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
@@ -552,6 +561,15 @@ DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int bl
       T.assign(size_t(keep) * keep, 0.0);
       for (int a = 0; a < keep; ++a) T[size_t(a) * keep + a] = theta[a];
       ++out.restarts;
+      // GD+k: the previous iteration's Ritz vectors of the block, made
+      // orthogonal to the kept ones (dropped where they add no direction);
+      // their columns of T are formed at the top of the next iteration
+      for (int a = 0; a < nb && it > 0 && m + int(C.size()) < max_subspace; ++a) {
+        if (!Uprev[a].data()) break;
+        DevVec pv = d.vec(false);
+        qkd_check(qkd_copy(t, dim, Uprev[a].data(), pv.data(), d.c.stream), "copy");
+        append(std::move(pv));
+      }
     }
     int added = 0;
     for (auto& c : C)
@@ -575,6 +593,36 @@ DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int bl
   return out;
 }
 
+namespace {
+// The three-term recurrence of continued_fraction_coeffs
+// (src/solvers/dynamics.cpp:12-59) from step res.alphas.size() up to step
+// n_iter: v is the current normalised Lanczos vector, vp the previous one
+// (zero before the first step).  Returns true when it stopped on
+// beta < 1e-15 (breakdown).  A run split into several calls performs the
+// same device operations in the same order as one call.
+template <class Real>
+bool cf_steps(const Operator& H, Dev& d, DevVec& v, DevVec& vp, DevVec& w, CFOut<Real>& res, int n_iter) {
+  const qk_dtype T = d.t;
+  PtrArray P(1, H.device());
+  P.set(0, w.data(), d.c.stream);
+  double* r = d.c.dres(0);
+  for (int iter = int(res.alphas.size()); iter < n_iter; ++iter) {
+    H.apply_dot(T, v.data(), w.data(), r);
+    const Real alpha = Real(d.c.fetch(r, 1)[0]);
+    res.alphas.push_back(alpha);
+    const void* U[2] = {v.data(), vp.data()};
+    const double a[4] = {double(alpha), 0.0, iter > 0 ? double(res.betas.back()) : 0.0, 0.0};
+    d.update_mdot(iter > 0 ? 2 : 1, U, a, P, 1, w.data(), r);
+    const Real beta = Real(std::sqrt(Real(d.c.fetch(r, 1)[0])));
+    if (beta < Real(1e-15)) return true;
+    res.betas.push_back(beta);
+    d.scale_into(double(Real(1) / beta), w.data(), vp.data());
+    std::swap(v, vp);  // v <- w / beta, v_prev <- old v
+  }
+  return false;
+}
+}  // namespace
+
 template <class Real>
 CFOut<Real> continued_fraction(const Operator& H, const std::complex<Real>* phi0, int n_iter) {
   CFOut<Real> res;
@@ -588,21 +636,77 @@ CFOut<Real> continued_fraction(const Operator& H, const std::complex<Real>* phi0
   if (nphi < Real(1e-15)) return res;
   d.scal(double(Real(1) / nphi), v.data());
   res.norm_phi0 = nphi;
-  PtrArray P(1, H.device());
-  P.set(0, w.data(), d.c.stream);
-  double* r = d.c.dres(0);
-  for (int iter = 0; iter < n_iter; ++iter) {
-    H.apply_dot(T, v.data(), w.data(), r);
-    const Real alpha = Real(d.c.fetch(r, 1)[0]);
-    res.alphas.push_back(alpha);
-    const void* U[2] = {v.data(), vp.data()};
-    const double a[4] = {double(alpha), 0.0, iter > 0 ? double(res.betas.back()) : 0.0, 0.0};
-    d.update_mdot(iter > 0 ? 2 : 1, U, a, P, 1, w.data(), r);
-    const Real beta = Real(std::sqrt(Real(d.c.fetch(r, 1)[0])));
-    if (beta < Real(1e-15)) break;
-    res.betas.push_back(beta);
-    d.scale_into(double(Real(1) / beta), w.data(), vp.data());
-    std::swap(v, vp);  // v <- w / beta, v_prev <- old v
+  cf_steps<Real>(H, d, v, vp, w, res, n_iter);
+  return res;
+}
+
+// The continued fraction with a checkpoint of its state (the coefficients
+// so far, the norm of phi0, the current and previous Lanczos vectors) read
+// from resume_dir and/or written to save_dir as .npy files: alphas.npy,
+// betas.npy, norm_phi0.npy, state.npy ([steps, stopped]), v.npy, v_prev.npy
+// (complex128).  Resuming and running to n_iter steps gives the same
+// coefficients, bit for bit, as one uninterrupted run.
+CFOut<double> continued_fraction_checkpointed(const Operator& H, const std::complex<double>* phi0,
+                                              const std::string& resume_dir, int n_iter,
+                                              const std::string& save_dir) {
+  CFOut<double> res;
+  const uint64_t dim = H.dim();
+  if (dim == 0) return res;
+  const qk_dtype T = QK_C128;
+  Dev d(H, T);
+  DevVec v = d.vec(false), vp = d.vec(true), w = d.vec(false);
+  bool stopped = false;
+  std::vector<std::complex<double>> hv;
+  auto load_vec = [&](const std::string& name, DevVec& dst) {
+    std::string descr;
+    std::vector<uint64_t> shape;
+    std::vector<char> raw = npy_read(resume_dir + "/" + name, descr, shape);
+    if (descr != "<c16" || shape.size() != 1 || shape[0] != dim)
+      throw std::invalid_argument("qkrylov_b200: checkpoint " + name + " does not match this operator");
+    d.upload<double>(reinterpret_cast<const std::complex<double>*>(raw.data()), dst);
+  };
+  auto load_f8 = [&](const std::string& name) {
+    std::string descr;
+    std::vector<uint64_t> shape;
+    std::vector<char> raw = npy_read(resume_dir + "/" + name, descr, shape);
+    if (descr != "<f8") throw std::invalid_argument("qkrylov_b200: checkpoint " + name + " is not float64");
+    std::vector<double> out(raw.size() / 8);
+    std::memcpy(out.data(), raw.data(), raw.size());
+    return out;
+  };
+  if (!resume_dir.empty()) {
+    res.alphas = load_f8("alphas.npy");
+    res.betas = load_f8("betas.npy");
+    const std::vector<double> nrm = load_f8("norm_phi0.npy"), st = load_f8("state.npy");
+    if (nrm.size() != 1 || st.size() != 2 || st[0] != double(res.alphas.size()) ||
+        res.betas.size() + (st[1] != 0.0 ? 1 : 0) != res.alphas.size())
+      throw std::invalid_argument("qkrylov_b200: inconsistent continued-fraction checkpoint in " + resume_dir);
+    res.norm_phi0 = nrm[0];
+    stopped = st[1] != 0.0;
+    if (res.norm_phi0 < 1e-15) return res;
+    load_vec("v.npy", v);
+    load_vec("v_prev.npy", vp);
+  } else {
+    if (!phi0) throw std::invalid_argument("qkrylov_b200: continued fraction needs phi0 or a checkpoint");
+    d.upload<double>(phi0, v);
+    const double nphi = std::sqrt(d.dot(v.data(), v.data()).real());
+    res.norm_phi0 = nphi;
+    if (nphi >= 1e-15) d.scal(1.0 / nphi, v.data());
+    else stopped = true;
+  }
+  if (!stopped) stopped = cf_steps<double>(H, d, v, vp, w, res, n_iter);
+  if (!save_dir.empty()) {
+    npy_write(save_dir + "/alphas.npy", res.alphas.data(), "<f8", {res.alphas.size()});
+    npy_write(save_dir + "/betas.npy", res.betas.data(), "<f8", {res.betas.size()});
+    npy_write(save_dir + "/norm_phi0.npy", &res.norm_phi0, "<f8", {});
+    const double st[2] = {double(res.alphas.size()), stopped ? 1.0 : 0.0};
+    npy_write(save_dir + "/state.npy", st, "<f8", {2});
+    hv.resize(dim);
+    for (const auto& pr : {std::make_pair(&v, "v.npy"), std::make_pair(&vp, "v_prev.npy")}) {
+      cuda_check(cudaMemcpyAsync(hv.data(), pr.first->data(), dim * 16, cudaMemcpyDeviceToHost, d.c.stream), "D2H");
+      d.c.sync();
+      npy_write(save_dir + "/" + pr.second, hv.data(), "<c16", {dim});
+    }
   }
   return res;
 }

@@ -7,6 +7,7 @@
 #pragma once
 
 #include <complex>
+#include <string>
 #include <vector>
 
 #include "operator.hpp"
@@ -158,6 +159,12 @@ SweepOut lanczos_sweep(const Operator& H0, const Operator& H1, const std::vector
 // src/solvers/dynamics.cpp:12-59
 template <class Real>
 CFOut<Real> continued_fraction(const Operator& H, const std::complex<Real>* phi0, int n_iter);
+// continued_fraction on complex128 vectors with a checkpoint: resumed from
+// resume_dir (when not empty; phi0 is then ignored) and/or saved to
+// save_dir (when not empty) as .npy files; n_iter counts all steps.
+CFOut<double> continued_fraction_checkpointed(const Operator& H, const std::complex<double>* phi0,
+                                              const std::string& resume_dir, int n_iter,
+                                              const std::string& save_dir);
 
 // src/solvers/ftlm.cpp:122-170, for several inverse temperatures at once:
 // the R tridiagonals do not depend on beta (the generator is re-seeded on

@@ -55,13 +55,21 @@ int qkd_plan_all_real(const qk_plan* p);
 size_t qkd_plan_device_bytes(const qk_plan* p);
 
 /* 0: use specialised kernels where the operator qualifies (default);
- * 1: generic kernel only (for comparisons). */
+ * 1: generic kernel only; 2: as 0 without the per-die work queues of the
+ * row kernel (for comparisons). */
 int qkd_set_kernel_policy(int policy);
+/* Dies of the current device as measured by the row kernels' topology probe
+ * (2 or 1) and the SMs on each. */
+int qkd_die_count(int* sms_die0, int* sms_die1);
 /* 1 when applies of this plan run the specialised two-site spin kernel. */
 int qkd_plan_kernel(const qk_plan* p);
 
 /* y = H x (device pointers, n = dim elements of dtype t). */
 int qkd_apply(const qk_plan* p, qk_dtype t, const void* x, void* y, cudaStream_t s);
+/* Rows [row_lo, row_hi) of y = H x (x complete, other rows of y untouched);
+ * the bounds must be sector-block boundaries. */
+int qkd_apply_range(const qk_plan* p, qk_dtype t, const void* x, void* y, uint64_t row_lo, uint64_t row_hi,
+                    cudaStream_t s);
 /* y = H x and dot_out[0..1] = <x, y> (device memory) in the same pass. */
 int qkd_apply_dot(const qk_plan* p, qk_workspace* w, qk_dtype t, const void* x, void* y,
                   double* dot_out, cudaStream_t s);
@@ -189,6 +197,13 @@ int qkd_block_axpy_cols(qk_dtype t, size_t n, int R, const double* g, const void
                         double* partials, size_t partials_cap, double* dots, cudaStream_t s);
 /* Device scratch of the workspace: 2*kMaxK+16 doubles for small results. */
 double* qkd_workspace_results(qk_workspace* w);
+/* S(omega) of ncols continued fractions (column c: alphas/betas at c*ld,
+ * len[c] coefficients, NULL: ld; norm nrm[c], NULL: 1) at nw frequencies,
+ * the reference's evaluate_spectral_function per pair; out[c*nw + k].
+ * Device pointers. */
+int qkd_spectral_batch(const double* alphas, const double* betas, const int* len, int ncols, int ld,
+                       const double* nrm, const double* omega, size_t nw, double E0, double eta, double* out,
+                       cudaStream_t s);
 
 #ifdef __cplusplus
 }

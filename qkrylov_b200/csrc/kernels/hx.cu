@@ -24,6 +24,9 @@ int spin_plan_set_diag(SpinHandle* h, const double* diag);
 int spin_apply_block(const SpinHandle* h, qk_dtype t, int R, int lpr, const void* X, void* Y, double* dots,
                      cudaStream_t s, qk_workspace* w, const double* gacc = nullptr);
 void spin_plan_destroy(SpinHandle* h);
+void spin_set_die_queues(bool on);
+int spin_apply_range(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, uint64_t row_lo,
+                     uint64_t row_hi);
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
                double* dot_out);
 }  // namespace qkd
@@ -65,11 +68,12 @@ struct DevPlan {
   const qk_tile_t* __restrict__ tiles;
   uint32_t nterms, ngroups, ntiles;
   int has_diag;
+  uint64_t row_lo, row_hi;  // rows computed by k_hx: [row_lo, row_hi) (tiles never straddle a block)
 };
 
-DevPlan dev(const qk_plan* p) {
+DevPlan dev(const qk_plan* p, uint64_t row_lo = 0, uint64_t row_hi = ~0ull) {
   return DevPlan{p->L, p->lmask, p->diag_re, p->A, p->B, p->llist, p->terms, p->groups, p->tiles,
-                 p->nterms, p->ngroups, p->ntiles, p->has_diag};
+                 p->nterms, p->ngroups, p->ntiles, p->has_diag, row_lo, row_hi};
 }
 
 // Sum of the valid terms of one group on state s: returns false when none is valid.
@@ -179,6 +183,7 @@ k_hx(DevPlan p, const void* __restrict__ x, void* __restrict__ y, double* partia
   double dr = 0.0, di = 0.0;
   for (uint32_t ti = blockIdx.x; ti < p.ntiles; ti += gridDim.x) {
     const qk_tile_t tile = p.tiles[ti];
+    if (tile.row0 < p.row_lo || tile.row0 >= p.row_hi) continue;
     if (threadIdx.x < tile.count) {
       const uint64_t row = tile.row0 + threadIdx.x;
       const uint64_t s = (uint64_t(tile.h) << p.L) | __ldg(p.llist + tile.lstart + threadIdx.x);
@@ -353,8 +358,8 @@ unsigned hx_grid(const qk_plan* p, K kernel) {
 
 template <int DT, bool CC>
 int launch_apply(const qk_plan* p, const void* x, void* y, cudaStream_t s, qk_workspace* w,
-                 double* dot_out) {
-  const DevPlan d = dev(p);
+                 double* dot_out, uint64_t row_lo = 0, uint64_t row_hi = ~0ull) {
+  const DevPlan d = dev(p, row_lo, row_hi);
   if (dot_out) {
     auto k = k_hx<DT, CC, true>;
     if (set_smem(k, p->smem)) return QKD_EINVAL;
@@ -474,8 +479,9 @@ int qkd_plan_create(const qk_plan_desc* d, int device, qk_plan** out) {
 }
 
 int qkd_set_kernel_policy(int policy) {
-  if (policy < 0 || policy > 1) return QKD_EINVAL;
-  g_kernel_policy = policy;
+  if (policy < 0 || policy > 2) return QKD_EINVAL;
+  g_kernel_policy = policy == 1 ? 1 : 0;
+  qkd::spin_set_die_queues(policy != 2);
   return QKD_OK;
 }
 
@@ -505,6 +511,22 @@ int qkd_apply(const qk_plan* p, qk_dtype t, const void* x, void* y, cudaStream_t
   if (p->spin && g_kernel_policy == 0) return qkd::spin_apply(p->spin, t, x, y, s, nullptr, nullptr);
   if (p->all_real) { QKD_DISPATCH(t, return launch_apply<DT, false>(p, x, y, s, nullptr, nullptr)); }
   QKD_DISPATCH(t, return launch_apply<DT, true>(p, x, y, s, nullptr, nullptr));
+  return QKD_OK;
+}
+
+// Rows [row_lo, row_hi) of y = H x (x complete; the other rows of y are not
+// written).  The bounds must be sector-block boundaries (qkd_plan_shard).
+int qkd_apply_range(const qk_plan* p, qk_dtype t, const void* x, void* y, uint64_t row_lo, uint64_t row_hi,
+                    cudaStream_t s) {
+  if (!p || !x || !y || x == y || row_lo > row_hi || row_hi > p->dim) return QKD_EINVAL;
+  if (p->dim == 0 || p->ntiles == 0 || row_lo == row_hi) return QKD_OK;
+  if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
+  if (p->spin && g_kernel_policy == 0) {
+    const int rc = qkd::spin_apply_range(p->spin, t, x, y, s, row_lo, row_hi);
+    if (rc != QKD_EINVAL) return rc;
+  }
+  if (p->all_real) { QKD_DISPATCH(t, return launch_apply<DT, false>(p, x, y, s, nullptr, nullptr, row_lo, row_hi)); }
+  QKD_DISPATCH(t, return launch_apply<DT, true>(p, x, y, s, nullptr, nullptr, row_lo, row_hi));
   return QKD_OK;
 }
 

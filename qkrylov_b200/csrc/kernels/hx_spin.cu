@@ -82,6 +82,11 @@ struct SpinPlan {
   const uint4* btiles;      // block apply: (block record, first row, rows) runs of <= 256 rows
   uint32_t nbtiles;
   const uint32_t* border;   // order in which the row kernel visits the block records (null: record order)
+  // per-die work queues of the row kernel: the SMs of die 0 take the visiting
+  // positions [0, qsplit), those of die 1 [qsplit, nblocks); a CTA whose
+  // queue is empty takes from the other one
+  const uint8_t* sm_die;    // die of each SM id (null: one die)
+  uint32_t nsmid, qsplit;
 };
 
 namespace {
@@ -89,7 +94,7 @@ namespace {
 template <int DT, bool DOT>
 __global__ void __launch_bounds__(kSpinThreads)
 k_hx_spin(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y, double* partials,
-          unsigned* ticket, double* dot_out) {
+          unsigned* ticket, double* dot_out, uint64_t row_lo, uint64_t row_hi) {
   using T = VT<DT>;
   using R = typename T::R;
   extern __shared__ __align__(16) unsigned char sm[];
@@ -115,6 +120,7 @@ k_hx_spin(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __r
   double dr = 0.0, di = 0.0;
   for (uint32_t ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
     const qk_tile_t tile = p.tiles[ti];
+    if (tile.row0 < row_lo || tile.row0 >= row_hi) continue;
     const uint32_t h = tile.h;
     if (threadIdx.x < uint32_t(nbonds)) {  // per-tile data of the high bonds
       const SpinBond b = sbond[threadIdx.x];
@@ -237,10 +243,41 @@ __device__ __forceinline__ RowBlock load_block(const RowBlock* p) {
   return r;
 }
 
+// Next visiting position for this CTA from the per-die queues (wq[0], wq[1];
+// wq[2] counts CTAs that are done, the last one resets all three for the
+// next launch).  Returns nblocks when both queues are empty.
+__device__ __forceinline__ uint32_t wq_fetch(const SpinPlan& p, uint32_t* wq, int die) {
+  for (int k = 0; k < 2; ++k) {
+    const int q = die ^ k;
+    const uint32_t beg = q ? p.qsplit : 0u, n = q ? p.nblocks - p.qsplit : p.qsplit;
+    const uint32_t i = atomicAdd(wq + q, 1u);
+    if (i < n) return beg + i;
+  }
+  return p.nblocks;
+}
+
+__device__ __forceinline__ int sm_die_of(const SpinPlan& p) {
+  uint32_t s;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(s));
+  return (p.sm_die && s < p.nsmid) ? int(__ldg(p.sm_die + s)) : 0;
+}
+
+__device__ __forceinline__ void wq_done(uint32_t* wq) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(wq + 2, 1u) == gridDim.x - 1) {
+      atomicExch(wq, 0u);
+      atomicExch(wq + 1, 0u);
+      atomicExch(wq + 2, 0u);
+    }
+  }
+}
+
 template <int DT, bool DOT, bool GEN>
 __global__ void __launch_bounds__(kRowThreads, DT == QK_C128 ? kRowMinCtaC128 : 4)
 k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
-               double* partials, unsigned* ticket, double* dot_out) {
+               double* partials, unsigned* ticket, double* dot_out, uint32_t* wq, uint32_t row_lo,
+               uint32_t row_hi) {
   using T = VT<DT>;
   using R = typename T::R;
   using E = typename T::E;
@@ -260,12 +297,28 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
   double dr = 0.0, di = 0.0;
   RowBlock nxt;
   const uint32_t* __restrict__ bord = p.border;
-  if (blockIdx.x < nA) nxt = load_block(p.brec + (bord ? __ldg(bord + blockIdx.x) : blockIdx.x));
-  for (uint32_t h = blockIdx.x; h < nA; h += gridDim.x) {
+  // visiting positions: from the per-die queues (wq) or grid-stride
+  __shared__ uint32_t s_pos[2];
+  const int die = wq ? sm_die_of(p) : 0;
+  uint32_t pos = blockIdx.x;
+  if (wq) {
+    if (threadIdx.x == 0) s_pos[0] = wq_fetch(p, wq, die);
+    __syncthreads();
+    pos = s_pos[0];
+  }
+  if (pos < nA) nxt = load_block(p.brec + (bord ? __ldg(bord + pos) : pos));
+  for (uint32_t it = 1; pos < nA; ++it) {
     const RowBlock cur = nxt;
-    const uint32_t hn = h + gridDim.x;
-    if (hn < nA) nxt = load_block(p.brec + (bord ? __ldg(bord + hn) : hn));
-    if (cur.size == 0) continue;
+    uint32_t pn = pos + gridDim.x;
+    if (wq) {
+      // double-buffered: slot it & 1 was last read before the previous barrier
+      if (threadIdx.x == 0) s_pos[it & 1] = wq_fetch(p, wq, die);
+      __syncthreads();
+      pn = s_pos[it & 1];
+    }
+    if (pn < nA) nxt = load_block(p.brec + (bord ? __ldg(bord + pn) : pn));
+    pos = pn;
+    if (cur.size == 0 || cur.base < row_lo || cur.base >= row_hi) continue;
     const uint32_t base = cur.base, size = cur.size, nh = cur.nh;
     __syncthreads();  // the previous block is finished with the staging and the entry tables
     for (uint32_t r = threadIdx.x; r < size; r += kRowThreads) sx[r] = __ldg(xg + base + r);
@@ -480,6 +533,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       }
     }
   }
+  if (wq) wq_done(wq);
   if (DOT) {
     __shared__ double sbuf[2 * (kRowThreads / 32)];
     block_sum2(dr, di, sbuf);
@@ -656,14 +710,49 @@ struct SpinHandle {
   SpinPlan host;
   SpinPlan* dev = nullptr;
   void* bufs[20] = {};
-  bool lean = false;  // every bond conserves the charge: warp-tile kernel
+  uint32_t* wq = nullptr;  // per-die work queues of the row kernel (4 u32, zero between launches)
+  bool lean = false;       // every bond conserves the charge: row kernel
 };
 
 void spin_plan_destroy(SpinHandle* h) {
   if (!h) return;
   for (void* b : h->bufs) cudaFree(b);
+  cudaFree(h->wq);
   cudaFree(h->dev);
   delete h;
+}
+
+bool die_map(const uint8_t** dev_map, int* nsmid, int* n0, int* n1);
+
+// Per-die work queues (process-wide switch, for comparisons).
+static bool g_die_queues = true;
+
+// When the GPU has two dies: split the visiting sequence into a share per
+// die in proportion to its SMs (by rows), and allocate the queue counters.
+// Without them (one die, or no memory) the row kernel keeps its
+// grid-stride order.
+static void set_die_queues(SpinHandle* out, SpinPlan& h, const std::vector<RowBlock>& brec,
+                           const std::vector<uint32_t>& bord, size_t* dev_bytes) {
+  const uint8_t* map = nullptr;
+  int nsmid = 0, n0 = 0, n1 = 0;
+  if (!die_map(&map, &nsmid, &n0, &n1) || h.nblocks < 2) return;
+  uint64_t total = 0;
+  for (const RowBlock& b : brec) total += b.size;
+  const uint64_t want = total * uint64_t(n0) / uint64_t(n0 + n1);
+  uint64_t acc = 0;
+  uint32_t split = 0;
+  while (split < h.nblocks && acc < want) acc += brec[bord.empty() ? split : bord[split]].size, ++split;
+  if (cudaMalloc(&out->wq, 4 * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMemset(out->wq, 0, 4 * sizeof(uint32_t)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cudaFree(out->wq);
+    out->wq = nullptr;
+    return;
+  }
+  *dev_bytes += 4 * sizeof(uint32_t);
+  h.sm_die = map;
+  h.nsmid = uint32_t(nsmid);
+  h.qsplit = split;
 }
 
 // Visiting order of the 2^H sector blocks of a spin plan.  Blocks are
@@ -990,6 +1079,7 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.bent = static_cast<const uint2*>(out->bufs[16]);
     h.btiles = static_cast<const uint4*>(out->bufs[18]);
     h.nbtiles = uint32_t(btl.size());
+    if (h.rows_ok) set_die_queues(out, h, brec, bord, dev_bytes);
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1189,6 +1279,7 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.crk32 = static_cast<const uint32_t*>(out->bufs[17]);
     h.btiles = static_cast<const uint4*>(out->bufs[18]);
     h.nbtiles = uint32_t(tiles.size());
+    set_die_queues(out, h, brec, std::vector<uint32_t>(), dev_bytes);
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1203,11 +1294,14 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
 }
 
 int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s,
-                    qk_workspace* w, double* dot_out) {
+                    qk_workspace* w, double* dot_out, uint64_t row_lo = 0, uint64_t row_hi = ~0ull) {
   if (!h->host.rows_ok || (h->host.gen && !h->host.diag_full)) return QKD_EINVAL;
   const size_t es = (t == QK_C128) ? 16 : (t == QK_F32 ? 4 : 8);
   const size_t smem = es * (h->host.max_block + 1);  // staged block and the zero slot
   if (smem > 200 * 1024) return QKD_EINVAL;
+  uint32_t* const wq = g_die_queues ? h->wq : nullptr;
+  const uint32_t rlo = uint32_t(std::min<uint64_t>(row_lo, 0xFFFFFFFFull));
+  const uint32_t rhi = uint32_t(std::min<uint64_t>(row_hi, 0xFFFFFFFFull));
 #define QKD_ROWS_LAUNCH1(DT, G)                                                                           \
   {                                                                                                       \
     auto kd = k_hx_spin_rows<DT, true, G>;                                                                \
@@ -1217,8 +1311,9 @@ int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
       return QKD_EINVAL;                                                                                  \
     const unsigned cap = std::max(1u, h->host.nblocks);                                                   \
     if (dot_out) kd<<<resident_grid(kd, kRowThreads, smem, std::min<unsigned>(cap, kMaxG)), kRowThreads, smem, s>>>( \
-        h->dev, x, y, w->partials, w->ticket, dot_out);                                                   \
-    else kn<<<resident_grid(kn, kRowThreads, smem, cap), kRowThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr); \
+        h->dev, x, y, w->partials, w->ticket, dot_out, wq, rlo, rhi);                                     \
+    else kn<<<resident_grid(kn, kRowThreads, smem, cap), kRowThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, \
+                                                                                 nullptr, wq, rlo, rhi);  \
   }
 #define QKD_ROWS_LAUNCH(DT) { if (h->host.gen) QKD_ROWS_LAUNCH1(DT, true) else QKD_ROWS_LAUNCH1(DT, false) }
   switch (t) {
@@ -1275,11 +1370,11 @@ int spin_plan_set_diag(SpinHandle* h, const double* diag) {
   return cudaMemcpy(h->dev, &h->host, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess ? QKD_OK : QKD_ECUDA;
 }
 
-int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
-               double* dot_out) {
-  if (h->host.gen) return spin_apply_rows(h, t, x, y, s, w, dot_out);
+static int spin_apply_impl(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
+                           double* dot_out, uint64_t row_lo, uint64_t row_hi) {
+  if (h->host.gen) return spin_apply_rows(h, t, x, y, s, w, dot_out, row_lo, row_hi);
   if (h->lean) {  // the row kernel where its tables exist; otherwise the bond kernel below
-    const int rc = spin_apply_rows(h, t, x, y, s, w, dot_out);
+    const int rc = spin_apply_rows(h, t, x, y, s, w, dot_out, row_lo, row_hi);
     if (rc != QKD_EINVAL) return rc;
   }
   const size_t smem = h->host.smem;
@@ -1291,12 +1386,12 @@ int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStre
       if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) \
         return QKD_EINVAL;                                                                              \
       k<<<std::min<unsigned>(grid, kMaxG), kSpinThreads, smem, s>>>(h->dev, x, y, w->partials, w->ticket, \
-                                                                     dot_out);                          \
+                                                                     dot_out, row_lo, row_hi);          \
     } else {                                                                                            \
       auto k = k_hx_spin<DT, false>;                                                                    \
       if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) \
         return QKD_EINVAL;                                                                              \
-      k<<<grid, kSpinThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr);                      \
+      k<<<grid, kSpinThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, nullptr, row_lo, row_hi);      \
     }                                                                                                   \
   }
   switch (t) {
@@ -1310,6 +1405,19 @@ int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStre
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
+
+int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
+               double* dot_out) {
+  return spin_apply_impl(h, t, x, y, s, w, dot_out, 0, ~0ull);
+}
+
+// Rows [row_lo, row_hi) only (block-aligned bounds); no fused dot.
+int spin_apply_range(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, uint64_t row_lo,
+                     uint64_t row_hi) {
+  return spin_apply_impl(h, t, x, y, s, nullptr, nullptr, row_lo, row_hi);
+}
+
+void spin_set_die_queues(bool on) { g_die_queues = on; }
 
 }  // namespace qkd
 

@@ -44,7 +44,8 @@ def test_structure_factor_n24_matches_reference():
     del ref
     c = qk.continued_fraction_coeffs(H, phi, 300)
     assert len(c.alphas) == len(c_ref["alphas"]) == 300
-    assert abs(c.norm_phi0 - c_ref["norm_phi0"]) <= 1e-14 * c_ref["norm_phi0"]
+    # a sum over 2.7 M elements in a different order: rounding-level agreement
+    assert abs(c.norm_phi0 - c_ref["norm_phi0"]) <= 1e-12 * c_ref["norm_phi0"]
     # the leading coefficients fix the low moments of the spectral measure
     a, b = np.asarray(c.alphas), np.asarray(c.betas)
     ar, br = np.asarray(c_ref["alphas"]), np.asarray(c_ref["betas"])
