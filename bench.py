@@ -639,6 +639,55 @@ def dynamics_all_momenta(qk, N=24, steps=300):
     return out
 
 
+def profile_case(qk, name):
+    """Small, self-contained launches of one kernel family for ncu captures
+    (each runs a few launches on a few GB at most):
+      tj20-hx          t-J N=20 (2 holes) two-part row kernel, float64, 4 applies
+      tj20-ftlm-block  batched FTLM on the same chain, R=64 FP32 vectors, 4 steps
+                       without graph capture (after one tuning run)
+      mdot             the reorthogonalisation multi-dot / multi-update of the
+                       solvers on 32 float64 vectors of 16 M elements (the
+                       kernels of the Davidson projection and the Lanczos
+                       reorthogonalisation, at C3's vector length / 10)
+      sweep-n20        the batched coupling sweep on the J1-J2 chain N=20 (its
+                       column multi-dot / multi-update kernels)"""
+    import torch
+    out = {}
+    if name in ("tj20-hx", "tj20-ftlm-block"):
+        N = 20
+        B = qk.TJBasis(N, conserve_nup=True, nup=9, conserve_ndn=True, ndn=9)
+        H = qk.MatrixFreeHamiltonian(B, qk.TJSite(), tj_opsum(qk, N, 1.0, 0.4), dtype=np.float64)
+        out["dim"] = H.dimension
+        if name == "tj20-hx":
+            x = torch.randn(H.dimension, dtype=torch.float64, device="cuda")
+            y = torch.empty_like(x)
+            for _ in range(4):
+                H.apply_device(x.data_ptr(), y.data_ptr(), qk.DTYPE_F64)
+            torch.cuda.synchronize()
+        else:
+            T = [0.5, 1.0]
+            qk.ftlm_block(H, T, n_random=64, n_steps=4, seed=5, precision=32, graph=False)
+            r = qk.ftlm_block(H, T, n_random=64, n_steps=4, seed=5, precision=32, graph=False)
+            out["lanes_per_row"] = r.lanes_per_row
+    elif name == "mdot":
+        n, k = 16 * 1024 * 1024, 32
+        V = [torch.randn(n, dtype=torch.float64, device="cuda") for _ in range(k)]
+        x = torch.randn(n, dtype=torch.float64, device="cuda")
+        L = qk.lib()
+        import ctypes
+        ptrs = (ctypes.c_void_p * k)(*[v.data_ptr() for v in V])
+        o = np.zeros(2 * k)
+        for _ in range(3):
+            L.qkrylov_b200_multi_dot(torch.cuda.current_device(), qk.DTYPE_F64, n, k, ptrs,
+                                     ctypes.c_void_p(x.data_ptr()), o.ctypes.data)
+        out.update(n=n, k=k)
+    elif name == "sweep-n20":
+        out.update(coupling_sweep(qk, N=20, sequential=False))
+    else:
+        raise ValueError(f"unknown profile case {name}")
+    return out
+
+
 def run_reference(args):
     """The reference arm: the reference's own CPU H.x (oracle/_ref, its
     unchanged sources, OpenMP on all host threads) on the headline workload
@@ -713,6 +762,12 @@ def run_b200(args):
         return ms, launches
 
     peak, peak_kind = peaks()
+    if args.profile_case:
+        if rank == 0:
+            print(json.dumps({"profile_case": args.profile_case, **profile_case(qk, args.profile_case)}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.hubbard:
         if rank == 0:
             print(json.dumps({"hubbard_only": True, **hubbard_c3(qk)}), flush=True)
@@ -875,6 +930,8 @@ def main():
     ap.add_argument("--policy", default="auto", help="H.x kernel policy of --kernel-only (qkrylov_b200.set_kernel_policy)")
     ap.add_argument("--hubbard", action="store_true",
                     help="only the Hubbard 4x4 (8 up, 8 down) H.x, mixed-precision Lanczos and block Davidson")
+    ap.add_argument("--profile-case", default=None,
+                    help="run one small kernel case for an ncu capture (see profile_case) and exit")
     ap.add_argument("--sweep-only", action="store_true",
                     help="only the batched coupling sweep on the J1-J2 chain of --n sites (no one-at-a-time runs)")
     args = ap.parse_args()

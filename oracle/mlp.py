@@ -2,7 +2,7 @@
 
 FP64 numpy restatement of the GPU definitions in qkrylov_b200's warm-start
 kernels: inputs (spins as +-1, bit set = +1, then J2), two hidden layers of
-128 with exact GELU, outputs (log-amplitude o0, sign logit o1); weights
+128 with the tanh form of GELU, outputs (log-amplitude o0, sign logit o1); weights
 rounded to BF16 (round to nearest even) as the GPU products see them,
 biases in FP32; per-sample loss w [(o0 - a)^2 + c_sign softplus(-y o1)]
 averaged over the samples, and its gradient by backpropagation (the
@@ -40,12 +40,22 @@ def bf16(x):
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+GELU_C, GELU_K = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """tanh form of GELU (Hendrycks & Gimpel 2016), the network's activation."""
+    return 0.5 * z * (1.0 + np.tanh(GELU_C * (z + GELU_K * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_C * (z + GELU_K * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_K * z * z)
+
+
+def gelu_exact(z):
+    """GELU with the Gaussian CDF (for the approximation bound test)."""
+    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
 
 
 def inputs(states, j2, nsites):

@@ -77,7 +77,7 @@ struct SpinPlan {
   // two-part operators (any factorisable group, e.g. Hubbard and t-J hops)
   bool gen;
   uint32_t nblocks;       // block records (all 2^H, or only the non-empty ones)
-  const uint32_t* crk32;  // [pos][ncross]: rank | lv0 << 24 | ls0 << 25 | lv1 << 26 | ls1 << 27
+  const uint32_t* crk32;  // [ncross][pos] (coalesced over rows): rank | lv0 << 24 | ls0 << 25 | lv1 << 26 | ls1 << 27
   const double* diag_full;  // two-part operators: the diagonal per row, summed in term order
   const uint4* btiles;      // block apply: (block record, first row, rows) runs of <= 256 rows
   uint32_t nbtiles;
@@ -306,9 +306,14 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
     __syncthreads();
     pos = s_pos[0];
   }
-  if (pos < nA) nxt = load_block(p.brec + (bord ? __ldg(bord + pos) : pos));
+  // DOT: one partial per block record, so the sum does not depend on which
+  // CTA took which block
+  __shared__ double s_dot[2 * (kRowThreads / 32)];
+  uint32_t nrec = pos < nA ? (bord ? __ldg(bord + pos) : pos) : 0u;
+  if (pos < nA) nxt = load_block(p.brec + nrec);
   for (uint32_t it = 1; pos < nA; ++it) {
     const RowBlock cur = nxt;
+    const uint32_t rec = nrec;
     uint32_t pn = pos + gridDim.x;
     if (wq) {
       // double-buffered: slot it & 1 was last read before the previous barrier
@@ -316,9 +321,15 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       __syncthreads();
       pn = s_pos[it & 1];
     }
-    if (pn < nA) nxt = load_block(p.brec + (bord ? __ldg(bord + pn) : pn));
+    if (pn < nA) {
+      nrec = bord ? __ldg(bord + pn) : pn;
+      nxt = load_block(p.brec + nrec);
+    }
     pos = pn;
-    if (cur.size == 0 || cur.base < row_lo || cur.base >= row_hi) continue;
+    if (cur.size == 0 || cur.base < row_lo || cur.base >= row_hi) {
+      if (DOT && threadIdx.x == 0) { partials[2 * rec] = 0.0; partials[2 * rec + 1] = 0.0; }
+      continue;
+    }
     const uint32_t base = cur.base, size = cur.size, nh = cur.nh;
     __syncthreads();  // the previous block is finished with the staging and the entry tables
     for (uint32_t r = threadIdx.x; r < size; r += kRowThreads) sx[r] = __ldg(xg + base + r);
@@ -471,8 +482,9 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
           // low condition (row table) and high condition (block entry) hold,
           // with the sign of both parts' Jordan-Wigner / Sz parities
           for (int q = 0; q < ncross; ++q) {
-            const uint32_t ent = __ldg(p.crk32 + pos[k] * uint32_t(ncross) + q);
             const uint32_t bf = s_ebit[q];
+            if (!(((bf >> 16) | (bf >> 18)) & 1u)) continue;  // no term valid in this block (block-uniform)
+            const uint32_t ent = __ldg(p.crk32 + size_t(q) * nll + pos[k]);
             R c = R(0);
             if ((ent >> 24) & (bf >> 16) & 1u) {
               const R w = s_coef[bf & 0xFFu];
@@ -532,14 +544,15 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
         }
       }
     }
+    if (DOT) {
+      block_sum2(dr, di, s_dot);
+      if (threadIdx.x == 0) { partials[2 * rec] = dr; partials[2 * rec + 1] = di; }
+      dr = 0.0;
+      di = 0.0;
+    }
   }
   if (wq) wq_done(wq);
-  if (DOT) {
-    __shared__ double sbuf[2 * (kRowThreads / 32)];
-    block_sum2(dr, di, sbuf);
-    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = dr; partials[2 * blockIdx.x + 1] = di; }
-    grid_finish(partials, ticket, 1, dot_out);
-  }
+  if (DOT) grid_finish_items(partials, ticket, nA, dot_out);
 }
 
 // Block form of the row kernel for R vectors stored row-interleaved
@@ -554,7 +567,8 @@ struct alignas(sizeof(E) * VPL) BlkPack { E v[VPL]; };
 template <int DT, bool GEN, int LPR, int VPL>
 __global__ void __launch_bounds__(256)
 k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, void* __restrict__ Y,
-                double* partials, unsigned* ticket, double* dots, const double* __restrict__ gacc) {
+                double* partials, unsigned* ticket, double* dots, const double* __restrict__ gacc,
+                uint32_t* wq, uint32_t tpc, uint32_t nchunks, uint32_t qsplit) {
   using T = VT<DT>;
   using R = typename T::R;
   using E = typename T::E;
@@ -586,8 +600,37 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
   };
   // Tiles of <= 256 rows in block order: the CTAs running at the same time
   // work on a few neighbouring blocks, whose rows (the low-bond targets)
-  // then stay in L2 while they are gathered.
-  for (uint32_t ti = blockIdx.x; ti < p.nbtiles; ti += gridDim.x) {
+  // then stay in L2 while they are gathered.  The tiles are handed out in
+  // chunks of tpc consecutive tiles, from a queue per die of the GPU (wq) or
+  // grid-stride; the column dots are summed per chunk and the chunk sums in
+  // chunk order, so the dots do not depend on which CTA took which chunk.
+  __shared__ uint32_t s_chunk[2];
+  __shared__ double red[2 * 256];
+  int die = 0;
+  if (wq) {
+    uint32_t sid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(sid));
+    die = (p.sm_die && sid < p.nsmid) ? int(__ldg(p.sm_die + sid)) : 0;
+  }
+  auto fetch = [&](uint32_t prev) -> uint32_t {
+    if (!wq) return prev + gridDim.x;
+    for (int k = 0; k < 2; ++k) {
+      const int q = die ^ k;
+      const uint32_t beg = q ? qsplit : 0u, n = q ? nchunks - qsplit : qsplit;
+      const uint32_t i = atomicAdd(wq + q, 1u);
+      if (i < n) return beg + i;
+    }
+    return nchunks;
+  };
+  uint32_t chunk = blockIdx.x;
+  if (wq) {
+    if (threadIdx.x == 0) s_chunk[0] = fetch(0);
+    __syncthreads();
+    chunk = s_chunk[0];
+  }
+  for (uint32_t it = 1; chunk < nchunks; ++it) {
+   const uint32_t t_end = min(p.nbtiles, (chunk + 1) * tpc);
+   for (uint32_t ti = chunk * tpc; ti < t_end; ++ti) {
     const uint4 tile = __ldg(p.btiles + ti);
     const RowBlock cur = load_block(p.brec + tile.x);
     const uint32_t base = cur.base, size = tile.y + tile.z, nh = cur.nh;
@@ -644,8 +687,9 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
         R c = R(0);
         uint32_t rank = 0;
         if constexpr (GEN) {
-          const uint32_t ent = __ldg(p.crk32 + size_t(pos) * uint32_t(ncross) + q);
           const uint32_t bf = s_ebit[q];
+          if (!(((bf >> 16) | (bf >> 18)) & 1u)) continue;  // no term valid in this block (block-uniform)
+          const uint32_t ent = __ldg(p.crk32 + size_t(q) * p.nllist + pos);
           if ((ent >> 24) & (bf >> 16) & 1u) {
             const R w = s_coef[bf & 0xFFu];
             c += (((ent >> 25) ^ (bf >> 17)) & 1u) ? -w : w;
@@ -686,22 +730,33 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
       }
       *reinterpret_cast<Pack*>(Ye + size_t(row) * RV + l * VPL) = yv;
     }
-  }
-  __shared__ double red[2 * 256];
-  for (int v = 0; v < VPL; ++v) {
-    __syncthreads();
-    red[2 * threadIdx.x] = dr[v];
-    red[2 * threadIdx.x + 1] = di[v];
-    __syncthreads();
-    if (threadIdx.x < LPR) {
-      double sr = 0.0, si = 0.0;
-      for (int t = threadIdx.x; t < 256; t += LPR) { sr += red[2 * t]; si += red[2 * t + 1]; }
-      const int c = threadIdx.x * VPL + v;
-      partials[(size_t(c) * gridDim.x + blockIdx.x) * 2] = sr;
-      partials[(size_t(c) * gridDim.x + blockIdx.x) * 2 + 1] = si;
+   }
+    // this chunk's column dots, in thread order, then the next chunk
+    for (int v = 0; v < VPL; ++v) {
+      __syncthreads();
+      red[2 * threadIdx.x] = dr[v];
+      red[2 * threadIdx.x + 1] = di[v];
+      __syncthreads();
+      if (threadIdx.x < LPR) {
+        double sr = 0.0, si = 0.0;
+        for (int t = threadIdx.x; t < 256; t += LPR) { sr += red[2 * t]; si += red[2 * t + 1]; }
+        const int c = threadIdx.x * VPL + v;
+        partials[(size_t(c) * nchunks + chunk) * 2] = sr;
+        partials[(size_t(c) * nchunks + chunk) * 2 + 1] = si;
+      }
+      dr[v] = 0.0;
+      di[v] = 0.0;
     }
+    uint32_t cn = chunk + gridDim.x;
+    if (wq) {
+      if (threadIdx.x == 0) s_chunk[it & 1] = fetch(chunk);
+      __syncthreads();
+      cn = s_chunk[it & 1];
+    }
+    chunk = cn;
   }
-  grid_finish(partials, ticket, RV, dots);
+  if (wq) wq_done(wq);
+  grid_finish_n(partials, ticket, RV, dots, nchunks);
 }
 
 }  // namespace
@@ -710,7 +765,8 @@ struct SpinHandle {
   SpinPlan host;
   SpinPlan* dev = nullptr;
   void* bufs[20] = {};
-  uint32_t* wq = nullptr;  // per-die work queues of the row kernel (4 u32, zero between launches)
+  uint32_t* wq = nullptr;  // per-die work queues (8 u32: row kernel, block kernel; zero between launches)
+  int n0 = 0, n1 = 0;      // SMs of each die
   bool lean = false;       // every bond conserves the charge: row kernel
 };
 
@@ -742,14 +798,16 @@ static void set_die_queues(SpinHandle* out, SpinPlan& h, const std::vector<RowBl
   uint64_t acc = 0;
   uint32_t split = 0;
   while (split < h.nblocks && acc < want) acc += brec[bord.empty() ? split : bord[split]].size, ++split;
-  if (cudaMalloc(&out->wq, 4 * sizeof(uint32_t)) != cudaSuccess ||
-      cudaMemset(out->wq, 0, 4 * sizeof(uint32_t)) != cudaSuccess) {
+  if (cudaMalloc(&out->wq, 8 * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMemset(out->wq, 0, 8 * sizeof(uint32_t)) != cudaSuccess) {
     (void)cudaGetLastError();
     cudaFree(out->wq);
     out->wq = nullptr;
     return;
   }
-  *dev_bytes += 4 * sizeof(uint32_t);
+  *dev_bytes += 8 * sizeof(uint32_t);
+  out->n0 = n0;
+  out->n1 = n1;
   h.sm_die = map;
   h.nsmid = uint32_t(nsmid);
   h.qsplit = split;
@@ -1203,7 +1261,7 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
         const uint32_t lv = (l & lo(t.cmask)) == lo(t.cval), ls = par(l & lo(t.smask));
         e |= (lv << (24 + 2 * k)) | (ls << (25 + 2 * k));
       }
-      crk32[pos * crossg.size() + q] = e;
+      crk32[q * nll + pos] = e;
     }
   }
   if (lgrp.empty()) lgrp.push_back(make_uint2(0, 0));
@@ -1300,6 +1358,7 @@ int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
   const size_t smem = es * (h->host.max_block + 1);  // staged block and the zero slot
   if (smem > 200 * 1024) return QKD_EINVAL;
   uint32_t* const wq = g_die_queues ? h->wq : nullptr;
+  if (dot_out && size_t(h->host.nblocks) > size_t(kMaxK) * kMaxG) return QKD_EINVAL;  // one partial per block
   const uint32_t rlo = uint32_t(std::min<uint64_t>(row_lo, 0xFFFFFFFFull));
   const uint32_t rhi = uint32_t(std::min<uint64_t>(row_hi, 0xFFFFFFFFull));
 #define QKD_ROWS_LAUNCH1(DT, G)                                                                           \
@@ -1333,8 +1392,23 @@ template <int DT, bool GEN, int LPR, int VPL>
 int launch_rows_block(const SpinHandle* h, qk_workspace* w, const void* X, void* Y, double* dots, cudaStream_t s,
                       const double* gacc) {
   auto k = k_hx_rows_block<DT, GEN, LPR, VPL>;
-  const unsigned g = resident_grid(k, 256, 0, std::min<unsigned>(std::max(1u, h->host.nbtiles), kMaxG));
-  k<<<g, 256, 0, s>>>(h->dev, X, Y, w->partials, w->ticket, dots ? dots : qkd_workspace_results(w), gacc);
+  constexpr uint32_t RV = uint32_t(LPR * VPL);
+  const uint32_t nt = std::max(1u, h->host.nbtiles);
+  const unsigned g = resident_grid(k, 256, 0, std::min<unsigned>(nt, kMaxG));
+  // chunks of consecutive tiles: about 8 per CTA, at most what the
+  // workspace holds for RV column partials each
+  const uint32_t cap = uint32_t(size_t(kMaxK) * kMaxG / RV);
+  const uint32_t want = std::min<uint32_t>(cap, std::max<uint32_t>(1u, 8u * g));
+  const uint32_t tpc = (nt + want - 1) / want;
+  const uint32_t nchunks = (nt + tpc - 1) / tpc;
+  uint32_t* wq = nullptr;
+  uint32_t qsplit = nchunks;
+  if (g_die_queues && h->wq && h->host.sm_die) {
+    wq = h->wq + 4;
+    qsplit = uint32_t(uint64_t(nchunks) * h->n0 / std::max(1, h->n0 + h->n1));
+  }
+  k<<<g, 256, 0, s>>>(h->dev, X, Y, w->partials, w->ticket, dots ? dots : qkd_workspace_results(w), gacc, wq, tpc,
+                      nchunks, qsplit);
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }

@@ -24,9 +24,18 @@ template <class T> __device__ __forceinline__ float tof(T v);
 template <> __device__ __forceinline__ float tof<float>(float v) { return v; }
 template <> __device__ __forceinline__ float tof<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
+// The network's activation: the tanh form of GELU (Hendrycks & Gimpel,
+// "Gaussian Error Linear Units", 2016), 0.5 z (1 + tanh(c (z + k z^3)))
+// with c = sqrt(2/pi), k = 0.044715, and its derivative.  Training uses the
+// accurate tanhf; the tensor-core inference kernel uses the hardware
+// approximation, whose error is below the BF16 rounding of its activations.
+constexpr float kGeluC = 0.79788456080286536f, kGeluK = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+  return 0.5f * z * (1.f + tanhf(kGeluC * z * fmaf(kGeluK * z, z, 1.f)));
+}
 __device__ __forceinline__ float gelu_d(float z) {
-  return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  const float t = tanhf(kGeluC * z * fmaf(kGeluK * z, z, 1.f));
+  return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * kGeluC * fmaf(3.f * kGeluK * z, z, 1.f);
 }
 
 // C[M][N] = sum_k A[m][k] * B'(k, n) (+ bias[n]); B'(k, n) = B[n*ldb + k]

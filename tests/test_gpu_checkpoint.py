@@ -44,11 +44,13 @@ def test_cf_resume_is_bit_identical(tmp_path):
 
 
 def test_cf_checkpoint_of_a_finished_run_resumes_as_stopped(tmp_path):
-    # dim 20 (N=6, Sz=0): the recurrence exhausts the Krylov space and stops
-    H = ham("spin", 6, dict(use_sz=1, sz2=0), O.heisenberg_chain(6))
-    phi = np.random.default_rng(1).standard_normal(H.dimension) + 0j
+    # |up up> is an eigenstate of the two-site Heisenberg model: the
+    # recurrence stops after one step (beta = 0)
+    H = ham("spin", 2, {}, O.heisenberg_chain(2, periodic=False))
+    phi = np.zeros(H.dimension, complex)
+    phi[3] = 1.0
     full = qk.continued_fraction_coeffs(H, phi, 40)
-    assert len(full.alphas) < 40
+    assert len(full.alphas) == 1 and len(full.betas) == 0
     d = str(tmp_path / "s")
     qk.continued_fraction_coeffs(H, phi, 40, save=d)
     again = qk.continued_fraction_coeffs(H, None, 40, resume=d)

@@ -55,3 +55,20 @@ def test_argument_checks():
         qk.davidson_block(H, n_eig=4, block=2)        # block < n_eig
     with pytest.raises(RuntimeError):
         qk.davidson_block(H, n_eig=2, block=4, max_subspace=8)
+
+
+def test_restarts_keep_the_previous_ritz_vectors():
+    """Hubbard 4x2 (4 up, 4 down; dim 4900) with a small basis: many
+    restarts, each keeping 2*block Ritz vectors plus the previous
+    iteration's; the 4 lowest eigenvalues converge to the sparse
+    eigensolver's values."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as sla
+    model = ("hubbard", 8, dict(use_nup=1, nup=4, use_ndn=1, ndn=4), O.hubbard_square(4, 2, 1.0, 4.0))
+    H = ham(*model)
+    r, c, v = O.port().hamiltonian(*model).coo()
+    A = sp.csr_matrix((v.real, (r, c)), shape=(H.dimension, H.dimension))
+    ev = np.sort(sla.eigsh(A, k=6, which="SA", tol=1e-12)[0])[:4]
+    d = qk.davidson_block(H, n_eig=4, block=6, max_subspace=24, tol=1e-8, seed=2, maxiter=300)
+    assert d.converged and d.restarts > 2
+    assert np.allclose(d.eigenvalues, ev, rtol=0, atol=1e-9), (d.eigenvalues, ev)

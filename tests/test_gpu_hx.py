@@ -234,3 +234,14 @@ def test_per_die_work_queues_give_identical_results():
             finally:
                 qk.set_kernel_policy("auto")
             assert torch.equal(ys[0], ys[1]) and torch.equal(ys[0], ys[2]), (kind, code)
+    # the block kernel (batched FTLM): its column dots are summed per chunk
+    # of tiles, so queue order does not change them either
+    H = ham("tj", 12, dict(use_nup=1, nup=5, use_ndn=1, ndn=5), O.tj_chain(12, 1.0, 0.4))
+    rs = []
+    try:
+        for pol in ("auto", "auto", "no-die-queues"):
+            qk.set_kernel_policy(pol)
+            rs.append(qk.ftlm_block(H, [0.5, 2.0], n_random=32, n_steps=20, seed=3, precision=64, graph=False))
+    finally:
+        qk.set_kernel_policy("auto")
+    assert np.array_equal(rs[0].U, rs[1].U) and np.array_equal(rs[0].U, rs[2].U)

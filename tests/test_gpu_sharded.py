@@ -47,10 +47,14 @@ def test_shards_reassemble_the_full_apply(kind, N, sec, terms, basis):
 
 def test_range_bounds_must_be_block_boundaries():
     H = ham("spin", 12, dict(use_sz=1, sz2=0), O.heisenberg_chain(12))
+    st = qk.SpinHalfBasis(12, sz=0).states()
+    # a row inside a sector block: its state shares every bit above bit 1
+    # with the previous row's, so no split of the 12 bits separates them
+    r = int(next(i for i in range(1, len(st)) if (int(st[i]) >> 2) == (int(st[i - 1]) >> 2)))
     x = torch.zeros(H.dimension, dtype=torch.float64, device="cuda")
     y = torch.zeros_like(x)
     rc = qk.lib().qkrylov_hamiltonian_apply_range_device(H._h, qk.DTYPE_F64, ctypes.c_void_p(x.data_ptr()),
-                                                         ctypes.c_void_p(y.data_ptr()), 1, H.dimension, None)
+                                                         ctypes.c_void_p(y.data_ptr()), r, H.dimension, None)
     assert rc == -1 and b"block" in qk.lib().qkrylov_b200_last_error()
 
 

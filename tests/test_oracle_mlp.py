@@ -57,3 +57,12 @@ def test_bf16_rounding_is_nearest_even():
     assert r[1] == 1.0             # exactly halfway: rounds to the even neighbour
     assert r[2] == 1.0078125
     assert abs(r[3] + 3.140625) < 1e-12
+
+
+def test_tanh_gelu_stays_close_to_the_gaussian_one():
+    # Hendrycks & Gimpel's tanh form: max |error| about 4.7e-4 (near |z| = 2.7)
+    z = np.linspace(-12.0, 12.0, 480001)
+    assert np.abs(mlp.gelu(z) - mlp.gelu_exact(z)).max() < 5e-4
+    h = 1e-6
+    d = (mlp.gelu(z + h) - mlp.gelu(z - h)) / (2 * h)
+    assert np.abs(d - mlp.gelu_d(z)).max() < 1e-7
