@@ -22,6 +22,9 @@ template <> struct VT<QK_C128> {
   __device__ static void st(void* p, uint64_t i, R re, R im) {
     reinterpret_cast<double2*>(p)[i] = make_double2(re, im);
   }
+  __device__ static void st_cs(void* p, uint64_t i, R re, R im) {
+    __stcs(reinterpret_cast<double2*>(p) + i, make_double2(re, im));
+  }
 };
 template <> struct VT<QK_C64> {
   using E = float2; using R = float; static constexpr bool cplx = true;
@@ -34,6 +37,9 @@ template <> struct VT<QK_C64> {
   __device__ static void st(void* p, uint64_t i, R re, R im) {
     reinterpret_cast<float2*>(p)[i] = make_float2(re, im);
   }
+  __device__ static void st_cs(void* p, uint64_t i, R re, R im) {
+    __stcs(reinterpret_cast<float2*>(p) + i, make_float2(re, im));
+  }
 };
 template <> struct VT<QK_F64> {
   using E = double; using R = double; static constexpr bool cplx = false;
@@ -44,6 +50,7 @@ template <> struct VT<QK_F64> {
     re = reinterpret_cast<const double*>(p)[i]; im = 0;
   }
   __device__ static void st(void* p, uint64_t i, R re, R) { reinterpret_cast<double*>(p)[i] = re; }
+  __device__ static void st_cs(void* p, uint64_t i, R re, R) { __stcs(reinterpret_cast<double*>(p) + i, re); }
 };
 template <> struct VT<QK_F32> {
   using E = float; using R = float; static constexpr bool cplx = false;
@@ -54,6 +61,7 @@ template <> struct VT<QK_F32> {
     re = reinterpret_cast<const float*>(p)[i]; im = 0;
   }
   __device__ static void st(void* p, uint64_t i, R re, R) { reinterpret_cast<float*>(p)[i] = re; }
+  __device__ static void st_cs(void* p, uint64_t i, R re, R) { __stcs(reinterpret_cast<float*>(p) + i, re); }
 };
 
 void count_launch();

@@ -14,6 +14,7 @@
 // state of a row comes from the coalesced low-part list.  One thread per row,
 // 512 rows per tile.
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "reduce.cuh"
@@ -78,6 +79,7 @@ struct SpinPlan {
   bool gen;
   uint32_t nblocks;       // block records (all 2^H, or only the non-empty ones)
   const uint32_t* crk32;  // [ncross][pos] (coalesced over rows): rank | lv0 << 24 | ls0 << 25 | lv1 << 26 | ls1 << 27
+  const uint32_t* crm;    // [pos]: bit q set when a term of crossing group q has its low condition
   const double* diag_full;  // two-part operators: the diagonal per row, summed in term order
   const uint4* btiles;      // block apply: (block record, first row, rows) runs of <= 256 rows
   uint32_t nbtiles;
@@ -201,6 +203,7 @@ k_hx_spin(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __r
 // size, and crossing ranks are in-class ranks of the partner's class; the
 // plan builder checks the high-bond sizes.
 constexpr int kRowThreads = 256;
+constexpr uint32_t kRowStreamY = 1u;  // launch flag: store y with the streaming (evict-first) hint
 constexpr int kRowHighC128 = 4;   // complex128: high bonds held in registers (more spill)
 constexpr int kRowMinCtaC128 = 3; // complex128: CTAs per SM the registers are sized for
 constexpr int kPrefetchAhead = 2; // row chunks of high-bond partner rows prefetched into L2
@@ -277,7 +280,7 @@ template <int DT, bool DOT, bool GEN>
 __global__ void __launch_bounds__(kRowThreads, DT == QK_C128 ? kRowMinCtaC128 : 4)
 k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
                double* partials, unsigned* ticket, double* dot_out, uint32_t* wq, uint32_t row_lo,
-               uint32_t row_hi) {
+               uint32_t row_hi, uint32_t flags) {
   using T = VT<DT>;
   using R = typename T::R;
   using E = typename T::E;
@@ -346,6 +349,9 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
     const R dh = R(cur.dh);
     const double* __restrict__ dcol = p.dtab + size_t(cur.combo) * nll;
     const uint32_t* __restrict__ ckw = reinterpret_cast<const uint32_t*>(p.crk);
+    uint32_t chm = 0u;  // two-part: crossing groups with a term whose high condition holds in this block
+    if constexpr (GEN)
+      for (int q = 0; q < ncross; ++q) chm |= (((s_ebit[q] >> 16) | (s_ebit[q] >> 18)) & 1u) << q;
     // block-uniform entries in registers: the first NB high bonds, 2 crossing
     constexpr int NB = kRowHighRegs<DT>;
     const int nh8 = nh < uint32_t(NB) ? int(nh) : NB;
@@ -481,9 +487,11 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
           // two-part crossing groups: up to two terms, each valid when its
           // low condition (row table) and high condition (block entry) hold,
           // with the sign of both parts' Jordan-Wigner / Sz parities
-          for (int q = 0; q < ncross; ++q) {
+          // only the groups with a term valid in both parts: the row's low
+          // mask and the block's high mask
+          for (uint32_t m = __ldg(p.crm + pos[k]) & chm; m; m &= m - 1u) {
+            const int q = __ffs(m) - 1;
             const uint32_t bf = s_ebit[q];
-            if (!(((bf >> 16) | (bf >> 18)) & 1u)) continue;  // no term valid in this block (block-uniform)
             const uint32_t ent = __ldg(p.crk32 + size_t(q) * nll + pos[k]);
             R c = R(0);
             if ((ent >> 24) & (bf >> 16) & 1u) {
@@ -537,7 +545,8 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
         const R d = GEN ? R(__ldg(p.diag_full + base + r)) : dh + R(dt[k]);
         ar[k] += d * x0r;
         if (T::cplx) ai[k] += d * x0i;
-        T::st(y, base + r, ar[k], ai[k]);
+        if (flags & kRowStreamY) T::st_cs(y, base + r, ar[k], ai[k]);  // y is not read again here
+        else T::st(y, base + r, ar[k], ai[k]);
         if (DOT) {
           dr += double(x0r) * double(ar[k]) + double(x0i) * double(ai[k]);
           di += double(x0r) * double(ai[k]) - double(x0i) * double(ar[k]);
@@ -568,7 +577,7 @@ template <int DT, bool GEN, int LPR, int VPL>
 __global__ void __launch_bounds__(256)
 k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, void* __restrict__ Y,
                 double* partials, unsigned* ticket, double* dots, const double* __restrict__ gacc,
-                uint32_t* wq, uint32_t tpc, uint32_t nchunks, uint32_t qsplit) {
+                uint32_t* wq, uint32_t nchunks, uint32_t qsplit, double* tile_part) {
   using T = VT<DT>;
   using R = typename T::R;
   using E = typename T::E;
@@ -600,10 +609,11 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
   };
   // Tiles of <= 256 rows in block order: the CTAs running at the same time
   // work on a few neighbouring blocks, whose rows (the low-bond targets)
-  // then stay in L2 while they are gathered.  The tiles are handed out in
-  // chunks of tpc consecutive tiles, from a queue per die of the GPU (wq) or
-  // grid-stride; the column dots are summed per chunk and the chunk sums in
-  // chunk order, so the dots do not depend on which CTA took which chunk.
+  // then stay in L2 while they are gathered.  The tiles are handed out
+  // grid-stride, or (wq) from a queue per die of the GPU, each die taking
+  // its own contiguous share; with queues the column dots of every tile go
+  // to tile_part and are summed in tile order, so they do not depend on
+  // which CTA took which tile (grid-stride: per CTA, in CTA order).
   __shared__ uint32_t s_chunk[2];
   __shared__ double red[2 * 256];
   int die = 0;
@@ -629,8 +639,8 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
     chunk = s_chunk[0];
   }
   for (uint32_t it = 1; chunk < nchunks; ++it) {
-   const uint32_t t_end = min(p.nbtiles, (chunk + 1) * tpc);
-   for (uint32_t ti = chunk * tpc; ti < t_end; ++ti) {
+   {
+    const uint32_t ti = chunk;
     const uint4 tile = __ldg(p.btiles + ti);
     const RowBlock cur = load_block(p.brec + tile.x);
     const uint32_t base = cur.base, size = tile.y + tile.z, nh = cur.nh;
@@ -643,6 +653,9 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
     }
     __syncthreads();
     const double* __restrict__ dcol = p.dtab + size_t(cur.combo) * nll;
+    uint32_t chm = 0u;
+    if constexpr (GEN)
+      for (int q = 0; q < ncross; ++q) chm |= (((s_ebit[q] >> 16) | (s_ebit[q] >> 18)) & 1u) << q;
     for (uint32_t r = tile.y + warp * RPW + sub; r < size; r += (256 / 32) * RPW) {
       const uint32_t pos = cur.lst + r, row = base + r;
       R x0r[VPL], x0i[VPL], ar[VPL], ai[VPL];
@@ -682,13 +695,15 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
         #pragma unroll
         for (int v = 0; v < VPL; ++v) { ar[v] += c * vr[v]; if (T::cplx) ai[v] += c * vi[v]; }
       }
-      // crossing bonds
+      // crossing bonds (two-part: only the groups the row's low mask and the
+      // block's high mask both allow)
+      const uint32_t cmask = GEN ? (__ldg(p.crm + pos) & chm) : ((1u << ncross) - 1u);
       for (int q = 0; q < ncross; ++q) {
+        if (!((cmask >> q) & 1u)) continue;
         R c = R(0);
         uint32_t rank = 0;
         if constexpr (GEN) {
           const uint32_t bf = s_ebit[q];
-          if (!(((bf >> 16) | (bf >> 18)) & 1u)) continue;  // no term valid in this block (block-uniform)
           const uint32_t ent = __ldg(p.crk32 + size_t(q) * p.nllist + pos);
           if ((ent >> 24) & (bf >> 16) & 1u) {
             const R w = s_coef[bf & 0xFFu];
@@ -731,21 +746,23 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
       *reinterpret_cast<Pack*>(Ye + size_t(row) * RV + l * VPL) = yv;
     }
    }
-    // this chunk's column dots, in thread order, then the next chunk
-    for (int v = 0; v < VPL; ++v) {
-      __syncthreads();
-      red[2 * threadIdx.x] = dr[v];
-      red[2 * threadIdx.x + 1] = di[v];
-      __syncthreads();
-      if (threadIdx.x < LPR) {
-        double sr = 0.0, si = 0.0;
-        for (int t = threadIdx.x; t < 256; t += LPR) { sr += red[2 * t]; si += red[2 * t + 1]; }
-        const int c = threadIdx.x * VPL + v;
-        partials[(size_t(c) * nchunks + chunk) * 2] = sr;
-        partials[(size_t(c) * nchunks + chunk) * 2 + 1] = si;
+    // queues: this tile's column dots, in thread order
+    if (tile_part) {
+      for (int v = 0; v < VPL; ++v) {
+        __syncthreads();
+        red[2 * threadIdx.x] = dr[v];
+        red[2 * threadIdx.x + 1] = di[v];
+        __syncthreads();
+        if (threadIdx.x < LPR) {
+          double sr = 0.0, si = 0.0;
+          for (int t = threadIdx.x; t < 256; t += LPR) { sr += red[2 * t]; si += red[2 * t + 1]; }
+          const int c = threadIdx.x * VPL + v;
+          tile_part[(size_t(c) * nchunks + chunk) * 2] = sr;
+          tile_part[(size_t(c) * nchunks + chunk) * 2 + 1] = si;
+        }
+        dr[v] = 0.0;
+        di[v] = 0.0;
       }
-      dr[v] = 0.0;
-      di[v] = 0.0;
     }
     uint32_t cn = chunk + gridDim.x;
     if (wq) {
@@ -756,7 +773,24 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
     chunk = cn;
   }
   if (wq) wq_done(wq);
-  grid_finish_n(partials, ticket, RV, dots, nchunks);
+  if (tile_part) {
+    grid_finish_n(tile_part, ticket, RV, dots, nchunks);
+    return;
+  }
+  for (int v = 0; v < VPL; ++v) {
+    __syncthreads();
+    red[2 * threadIdx.x] = dr[v];
+    red[2 * threadIdx.x + 1] = di[v];
+    __syncthreads();
+    if (threadIdx.x < LPR) {
+      double sr = 0.0, si = 0.0;
+      for (int t = threadIdx.x; t < 256; t += LPR) { sr += red[2 * t]; si += red[2 * t + 1]; }
+      const int c = threadIdx.x * VPL + v;
+      partials[(size_t(c) * gridDim.x + blockIdx.x) * 2] = sr;
+      partials[(size_t(c) * gridDim.x + blockIdx.x) * 2 + 1] = si;
+    }
+  }
+  grid_finish(partials, ticket, RV, dots);
 }
 
 }  // namespace
@@ -768,11 +802,16 @@ struct SpinHandle {
   uint32_t* wq = nullptr;  // per-die work queues (8 u32: row kernel, block kernel; zero between launches)
   int n0 = 0, n1 = 0;      // SMs of each die
   bool lean = false;       // every bond conserves the charge: row kernel
+  // per-tile column-dot partials of the queued block kernel, sized on first use
+  mutable std::mutex tp_mu;
+  mutable double* tile_part = nullptr;
+  mutable size_t tp_cap = 0;
 };
 
 void spin_plan_destroy(SpinHandle* h) {
   if (!h) return;
   for (void* b : h->bufs) cudaFree(b);
+  cudaFree(h->tile_part);
   cudaFree(h->wq);
   cudaFree(h->dev);
   delete h;
@@ -782,6 +821,9 @@ bool die_map(const uint8_t** dev_map, int* nsmid, int* n0, int* n1);
 
 // Per-die work queues (process-wide switch, for comparisons).
 static bool g_die_queues = true;
+// Launch flags of the row kernel, process-wide: y is written once and not
+// read again by the kernel, so it is stored with the streaming hint.
+static uint32_t g_row_flags = kRowStreamY;
 
 // When the GPU has two dies: split the visiting sequence into a share per
 // die in proportion to its SMs (by rows), and allocate the queue counters.
@@ -839,13 +881,42 @@ static std::vector<uint32_t> block_order(int H) {
   return o;
 }
 
-// Runs of <= 256 rows of each non-empty block record, in record order.
-static std::vector<uint4> block_tiles(const std::vector<RowBlock>& brec) {
+// Runs of <= 256 rows of each non-empty block record, in record order or
+// in the visiting order `order` (record indices) when given.
+static std::vector<uint4> block_tiles(const std::vector<RowBlock>& brec,
+                                      const std::vector<uint32_t>& order = std::vector<uint32_t>()) {
   std::vector<uint4> t;
-  for (uint32_t b = 0; b < uint32_t(brec.size()); ++b)
+  for (uint32_t i = 0; i < uint32_t(brec.size()); ++i) {
+    const uint32_t b = order.empty() ? i : order[i];
     for (uint32_t r = 0; r < brec[b].size; r += 256) t.push_back(make_uint4(b, r, std::min(256u, brec[b].size - r), 0));
+  }
   if (t.empty()) t.push_back(make_uint4(0, 0, 0, 0));
   return t;
+}
+
+// Visiting order of the block records of a two-part plan (records of the
+// non-empty blocks, high parts rec_h in ascending order): the counter of
+// block_order over units of `unit` bits (2: the up and down bit of one site
+// of a pair family), so the blocks reached by hops at either end of the high
+// segment and across the split are visited close together.
+static std::vector<uint32_t> record_order(const std::vector<uint32_t>& rec_h, int H, int unit) {
+  const int nu = std::max(1, H / unit);
+  std::vector<int> fast;  // unit of h for each counter digit, fastest first
+  const int k = nu * 2 / 7;
+  for (int u = 0; u < k; ++u) fast.push_back(u);
+  for (int u = nu - k; u < nu; ++u) fast.push_back(u);
+  for (int u = k; u < nu - k; ++u) fast.push_back(u);
+  const uint32_t umask = (1u << unit) - 1u;
+  std::vector<std::pair<uint64_t, uint32_t>> key(rec_h.size());
+  for (uint32_t i = 0; i < uint32_t(rec_h.size()); ++i) {
+    uint64_t c = 0;
+    for (int d = 0; d < nu; ++d) c |= uint64_t((rec_h[i] >> (fast[d] * unit)) & umask) << (d * unit);
+    key[i] = {c, i};
+  }
+  std::sort(key.begin(), key.end());
+  std::vector<uint32_t> o(rec_h.size());
+  for (size_t i = 0; i < key.size(); ++i) o[i] = key[i].second;
+  return o;
 }
 
 // Host side: decide eligibility from the compiled plan and build the
@@ -1216,6 +1287,7 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
   std::vector<uint2> rrec(nll), lgrp;
   std::vector<double> dtab(nll, 0.0);
   std::vector<uint32_t> crk32(std::max<uint64_t>(1, nll * crossg.size()), 0);
+  std::vector<uint32_t> crm(std::max<uint64_t>(1, nll), 0);
   std::vector<double> cls;
   std::vector<uint16_t> bucket[kRowCls];
   for (uint64_t pos = 0; pos < nll; ++pos) {
@@ -1262,6 +1334,7 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
         e |= (lv << (24 + 2 * k)) | (ls << (25 + 2 * k));
       }
       crk32[q * nll + pos] = e;
+      if (e & ((1u << 24) | (1u << 26))) crm[pos] |= 1u << q;
     }
   }
   if (lgrp.empty()) lgrp.push_back(make_uint2(0, 0));
@@ -1270,11 +1343,13 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
   // block records of the non-empty blocks
   std::vector<RowBlock> brec;
   std::vector<uint2> bent;
+  std::vector<uint32_t> rec_h;
   for (uint64_t hh = 0; hh < d->nA; ++hh) {
     const uint32_t need = uint32_t(d->A[hh] >> 56);
     if (need == qkb::kEmptyBlockKey) continue;
     const uint32_t size = d->key_off[need + 1] - d->key_off[need];
     if (size == 0) continue;
+    rec_h.push_back(uint32_t(hh));
     RowBlock b{};
     b.base = uint32_t(d->A[hh] & qkb::kOffsetMask);
     b.size = size;
@@ -1324,9 +1399,15 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
   bool ok = up(11, rrec.data(), rrec.size() * sizeof(uint2)) && up(12, lgrp.data(), lgrp.size() * sizeof(uint2)) &&
             up(13, crk_dummy.data(), 4) && up(14, dtab.data(), dtab.size() * 8) &&
             up(15, brec.data(), brec.size() * sizeof(RowBlock)) && up(16, bent.data(), bent.size() * sizeof(uint2)) &&
-            up(17, crk32.data(), crk32.size() * 4);
+            up(17, crk32.data(), crk32.size() * 4) && up(19, crm.data(), crm.size() * 4);
+  // the row kernel visits the records in the two-bit-unit order (sites of a
+  // pair family: t-J N=20 0.47 -> 0.41 ms per apply); the block kernel keeps
+  // record order, where its tiles of neighbouring blocks gather better
+  // (batched FTLM on the same chain: 0.86 s in record order, 0.92 s in the
+  // visiting order)
+  const std::vector<uint32_t> rord = record_order(rec_h, H, (L % 2 == 0 && H % 2 == 0) ? 2 : 1);
   const std::vector<uint4> tiles = block_tiles(brec);
-  ok = ok && up(18, tiles.data(), tiles.size() * sizeof(uint4));
+  ok = ok && up(18, tiles.data(), tiles.size() * sizeof(uint4)) && up(10, rord.data(), rord.size() * 4);
   if (ok) {
     h.rrec = static_cast<const uint2*>(out->bufs[11]);
     h.lgrp = static_cast<const uint2*>(out->bufs[12]);
@@ -1335,9 +1416,11 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.brec = static_cast<const RowBlock*>(out->bufs[15]);
     h.bent = static_cast<const uint2*>(out->bufs[16]);
     h.crk32 = static_cast<const uint32_t*>(out->bufs[17]);
+    h.crm = static_cast<const uint32_t*>(out->bufs[19]);
+    h.border = static_cast<const uint32_t*>(out->bufs[10]);
     h.btiles = static_cast<const uint4*>(out->bufs[18]);
     h.nbtiles = uint32_t(tiles.size());
-    set_die_queues(out, h, brec, std::vector<uint32_t>(), dev_bytes);
+    set_die_queues(out, h, brec, rord, dev_bytes);
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1370,9 +1453,10 @@ int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
       return QKD_EINVAL;                                                                                  \
     const unsigned cap = std::max(1u, h->host.nblocks);                                                   \
     if (dot_out) kd<<<resident_grid(kd, kRowThreads, smem, std::min<unsigned>(cap, kMaxG)), kRowThreads, smem, s>>>( \
-        h->dev, x, y, w->partials, w->ticket, dot_out, wq, rlo, rhi);                                     \
+        h->dev, x, y, w->partials, w->ticket, dot_out, wq, rlo, rhi, g_row_flags);                        \
     else kn<<<resident_grid(kn, kRowThreads, smem, cap), kRowThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, \
-                                                                                 nullptr, wq, rlo, rhi);  \
+                                                                                 nullptr, wq, rlo, rhi,   \
+                                                                                 g_row_flags);            \
   }
 #define QKD_ROWS_LAUNCH(DT) { if (h->host.gen) QKD_ROWS_LAUNCH1(DT, true) else QKD_ROWS_LAUNCH1(DT, false) }
   switch (t) {
@@ -1395,20 +1479,30 @@ int launch_rows_block(const SpinHandle* h, qk_workspace* w, const void* X, void*
   constexpr uint32_t RV = uint32_t(LPR * VPL);
   const uint32_t nt = std::max(1u, h->host.nbtiles);
   const unsigned g = resident_grid(k, 256, 0, std::min<unsigned>(nt, kMaxG));
-  // chunks of consecutive tiles: about 8 per CTA, at most what the
-  // workspace holds for RV column partials each
-  const uint32_t cap = uint32_t(size_t(kMaxK) * kMaxG / RV);
-  const uint32_t want = std::min<uint32_t>(cap, std::max<uint32_t>(1u, 8u * g));
-  const uint32_t tpc = (nt + want - 1) / want;
-  const uint32_t nchunks = (nt + tpc - 1) / tpc;
   uint32_t* wq = nullptr;
-  uint32_t qsplit = nchunks;
+  uint32_t qsplit = nt;
+  double* tp = nullptr;
   if (g_die_queues && h->wq && h->host.sm_die) {
-    wq = h->wq + 4;
-    qsplit = uint32_t(uint64_t(nchunks) * h->n0 / std::max(1, h->n0 + h->n1));
+    // per-tile dot partials for the queued form (RV columns, 2 doubles each)
+    std::lock_guard<std::mutex> lk(h->tp_mu);
+    const size_t need = size_t(nt) * RV * 2;
+    cudaStreamCaptureStatus cap_st = cudaStreamCaptureStatusNone;
+    const bool capturing = cudaStreamIsCapturing(s, &cap_st) != cudaSuccess || cap_st != cudaStreamCaptureStatusNone;
+    if (h->tp_cap < need && !capturing) {  // (a graph keeps the grid-stride form unless sized before capture)
+      cudaFree(h->tile_part);
+      h->tile_part = nullptr;
+      h->tp_cap = 0;
+      if (cudaMalloc(&h->tile_part, need * sizeof(double)) == cudaSuccess) h->tp_cap = need;
+      else (void)cudaGetLastError();
+    }
+    if (h->tile_part && h->tp_cap >= need) {
+      tp = h->tile_part;
+      wq = h->wq + 4;
+      qsplit = uint32_t(uint64_t(nt) * h->n0 / std::max(1, h->n0 + h->n1));
+    }
   }
-  k<<<g, 256, 0, s>>>(h->dev, X, Y, w->partials, w->ticket, dots ? dots : qkd_workspace_results(w), gacc, wq, tpc,
-                      nchunks, qsplit);
+  k<<<g, 256, 0, s>>>(h->dev, X, Y, w->partials, w->ticket, dots ? dots : qkd_workspace_results(w), gacc, wq, nt,
+                      qsplit, tp);
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
@@ -1492,6 +1586,7 @@ int spin_apply_range(const SpinHandle* h, qk_dtype t, const void* x, void* y, cu
 }
 
 void spin_set_die_queues(bool on) { g_die_queues = on; }
+void spin_set_row_flags(uint32_t f) { g_row_flags = f; }
 
 }  // namespace qkd
 

@@ -234,8 +234,9 @@ def test_per_die_work_queues_give_identical_results():
             finally:
                 qk.set_kernel_policy("auto")
             assert torch.equal(ys[0], ys[1]) and torch.equal(ys[0], ys[2]), (kind, code)
-    # the block kernel (batched FTLM): its column dots are summed per chunk
-    # of tiles, so queue order does not change them either
+    # the block kernel (batched FTLM): with queues its column dots are summed
+    # per tile in tile order, so repeated runs agree bit for bit; the
+    # grid-stride form sums per CTA (another order, rounding-level apart)
     H = ham("tj", 12, dict(use_nup=1, nup=5, use_ndn=1, ndn=5), O.tj_chain(12, 1.0, 0.4))
     rs = []
     try:
@@ -244,4 +245,5 @@ def test_per_die_work_queues_give_identical_results():
             rs.append(qk.ftlm_block(H, [0.5, 2.0], n_random=32, n_steps=20, seed=3, precision=64, graph=False))
     finally:
         qk.set_kernel_policy("auto")
-    assert np.array_equal(rs[0].U, rs[1].U) and np.array_equal(rs[0].U, rs[2].U)
+    assert np.array_equal(rs[0].U, rs[1].U)
+    assert np.allclose(rs[0].U, rs[2].U, rtol=1e-12, atol=0)

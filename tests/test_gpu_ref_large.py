@@ -5,8 +5,10 @@ unchanged sources) at sizes beyond the golden fixtures, on the GPU box:
   N = 24 (dim 2,704,156; the reference's CSR is ~2.3 GB): the same start
   vector phi0 = Sz(pi)|psi0> fed to the reference's
   continued_fraction_coeffs (src/solvers/dynamics.cpp:12-59) and to the
-  library's, 300 steps; S(omega) on [0, 4] at eta = 0.05 with
-  evaluate_spectral_function semantics (dynamics.cpp:61-89);
+  library's, 300 steps: the first 10 coefficients within 1e-10, S(omega)
+  on [0, 4] at eta = 0.05 (evaluate_spectral_function semantics,
+  dynamics.cpp:61-89) within 1e-6 of its maximum (see the test for why the
+  later coefficients of any two implementations differ);
 * FTLM on the t-J chain N = 14, 2 holes (dim 84,084) at several
   temperatures with the reference's Gaussian stream (src/solvers/ftlm.cpp:
   122-170): Z, U, Cv within 1e-10 relative.
@@ -46,15 +48,24 @@ def test_structure_factor_n24_matches_reference():
     assert len(c.alphas) == len(c_ref["alphas"]) == 300
     # a sum over 2.7 M elements in a different order: rounding-level agreement
     assert abs(c.norm_phi0 - c_ref["norm_phi0"]) <= 1e-12 * c_ref["norm_phi0"]
-    # the leading coefficients fix the low moments of the spectral measure
+    # Without reorthogonalisation the recurrence amplifies rounding: two CPU
+    # implementations of the reference's algorithm (its own sources and
+    # this project's restatement) on the same start vector at N = 24 differ
+    # by 4e-13 at step 0, 6e-11 at step 10, 1e-6 at step 50 and O(1) from
+    # step ~70 on, while their S(omega) agree to 7e-8 of its maximum.  So
+    # the leading coefficients (the low moments of the spectral measure)
+    # are compared tightly and S(omega) at a bar above that conditioning.
     a, b = np.asarray(c.alphas), np.asarray(c.betas)
     ar, br = np.asarray(c_ref["alphas"]), np.asarray(c_ref["betas"])
-    assert np.abs(a[:20] - ar[:20]).max() <= 1e-10 and np.abs(b[:20] - br[:20]).max() <= 1e-10
+    da = np.abs(a[:10] - ar[:10]) / np.abs(ar[:10]).max()
+    db = np.abs(b[:10] - br[:10]) / np.abs(br[:10]).max()
+    assert da.max() <= 1e-10 and db.max() <= 1e-10, (da.max(), db.max())
     omega = np.linspace(0.0, 4.0, 2001)
     E0 = gs.energy
-    S = np.array([qk.evaluate_spectral_function(c, w, E0, 0.05) for w in omega])
+    S = qk.spectral_function_batch(c, omega, E0, 0.05)
     S_ref = np.array([O.ref().spectral(ar, br, c_ref["norm_phi0"], w, E0, 0.05) for w in omega])
-    assert np.abs(S - S_ref).max() <= 1e-10 * np.abs(S_ref).max()
+    err = np.abs(S - S_ref).max() / np.abs(S_ref).max()
+    assert err <= 1e-6, err
 
 
 def test_ftlm_tj14_matches_reference_at_several_temperatures():
