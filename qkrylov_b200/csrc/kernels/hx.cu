@@ -22,7 +22,7 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes);
 bool spin_plan_is_gen(const SpinHandle* h);
 int spin_plan_set_diag(SpinHandle* h, const double* diag);
 int spin_apply_block(const SpinHandle* h, qk_dtype t, int R, int lpr, const void* X, void* Y, double* dots,
-                     cudaStream_t s, qk_workspace* w, const double* gacc = nullptr);
+                     cudaStream_t s, qk_workspace* w, const double* gacc = nullptr, int tilec = 0);
 void spin_plan_destroy(SpinHandle* h);
 void spin_set_die_queues(bool on);
 void spin_set_row_flags(uint32_t f);
@@ -48,7 +48,8 @@ struct qk_plan {
   uint32_t nterms, ngroups, ntiles;
   int has_diag, all_real;
   size_t bytes, smem;
-  int rows_lpr[4][3];  // autotuned lanes per row of the block apply, by dtype and R = 32, 64, 128
+  int rows_lpr[4][3];   // autotuned lanes per row of the block apply, by dtype and R = 32, 64, 128
+  int rows_tile[4][3];  // autotuned tile shape of the block apply (row kernels: 256 / 128 / 512 rows)
   double* diag_re;     // real diagonal (generic-kernel operators with a real diagonal), else null
 };
 
@@ -554,14 +555,17 @@ int qkd_apply_block(const qk_plan* p, qk_dtype t, int nvec, const void* X, size_
   return QKD_OK;
 }
 
-int qkd_apply_rows(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lanes_per_row, const void* X,
-                   void* Y, const void* diag, double* dots, cudaStream_t s) {
+static int apply_rows_shape(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lpr, int tilec, const void* X,
+                            void* Y, const void* diag, const double* g, double* dots, cudaStream_t s) {
   if (!p || !w || !X || !Y || X == Y || r_index(R) < 0) return QKD_EINVAL;
   if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
   if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
-  const int lpr = lanes_per_row ? lanes_per_row : (p->rows_lpr[t][r_index(R)] ? p->rows_lpr[t][r_index(R)] : 32);
+  if (g) {
+    if (!p->spin || g_kernel_policy != 0) return QKD_EINVAL;  // row-kernel tables only
+    return qkd::spin_apply_block(p->spin, t, R, lpr, X, Y, dots, s, w, g, tilec);
+  }
   if (p->spin && g_kernel_policy == 0) {  // the row-kernel tables where the operator has them
-    const int rc = qkd::spin_apply_block(p->spin, t, R, lpr, X, Y, dots, s, w);
+    const int rc = qkd::spin_apply_block(p->spin, t, R, lpr, X, Y, dots, s, w, nullptr, tilec);
     if (rc != QKD_EINVAL) return rc;
   }
   if (p->all_real) { QKD_DISPATCH(t, return launch_block_shape<DT, false>(p, w, R, lpr, X, Y, diag, dots, s)); }
@@ -570,14 +574,20 @@ int qkd_apply_rows(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lan
   return QKD_EINVAL;
 }
 
+int qkd_apply_rows(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lanes_per_row, const void* X,
+                   void* Y, const void* diag, double* dots, cudaStream_t s) {
+  if (!p || r_index(R) < 0 || t < QK_C128 || t > QK_F32) return QKD_EINVAL;
+  const int lpr = lanes_per_row ? lanes_per_row : (p->rows_lpr[t][r_index(R)] ? p->rows_lpr[t][r_index(R)] : 32);
+  const int tilec = lanes_per_row ? 0 : p->rows_tile[t][r_index(R)];
+  return apply_rows_shape(p, w, t, R, lpr, tilec, X, Y, diag, nullptr, dots, s);
+}
+
 int qkd_apply_rows_acc(const qk_plan* p, qk_workspace* w, qk_dtype t, int R, int lanes_per_row, const void* X,
                        void* Y, const double* g, double* dots, cudaStream_t s) {
-  if (!p || !w || !X || !Y || !g || X == Y || r_index(R) < 0) return QKD_EINVAL;
-  if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
-  if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
-  if (!p->spin || g_kernel_policy != 0) return QKD_EINVAL;  // row-kernel tables only
+  if (!p || !g || r_index(R) < 0 || t < QK_C128 || t > QK_F32) return QKD_EINVAL;
   const int lpr = lanes_per_row ? lanes_per_row : (p->rows_lpr[t][r_index(R)] ? p->rows_lpr[t][r_index(R)] : 32);
-  return qkd::spin_apply_block(p->spin, t, R, lpr, X, Y, dots, s, w, g);
+  const int tilec = lanes_per_row ? 0 : p->rows_tile[t][r_index(R)];
+  return apply_rows_shape(p, w, t, R, lpr, tilec, X, Y, nullptr, g, dots, s);
 }
 
 int qkd_rows_shape(const qk_plan* p, qk_dtype t, int R) {
@@ -585,44 +595,48 @@ int qkd_rows_shape(const qk_plan* p, qk_dtype t, int R) {
   return p->rows_lpr[t][r_index(R)];
 }
 
-// Times every valid lanes-per-row shape launch by launch, in two
-// interleaved rounds of three launches; the fastest single launch decides
-// (robust to clock drift and to a slow first round).  g != NULL tunes the
-// accumulating form Y += diag(g) H X.
+// The block apply's shape: lanes per row (so vectors per lane R / lanes)
+// times tile rows (the rows a CTA takes per fetch: 256, 128 or 512; row
+// kernels only), each timed launch by launch in two interleaved rounds of
+// three launches after a warm-up; the fastest single launch decides (robust
+// to clock drift and to a slow first round) and is kept in the plan per
+// dtype and R.  g != NULL tunes the accumulating form Y += diag(g) H X.
 static int tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, const void* diag,
                      const double* g, cudaStream_t s, int* chosen) {
   if (!p || !w || r_index(R) < 0 || t < QK_C128 || t > QK_F32) return QKD_EINVAL;
-  auto launch = [&](int lpr) {
-    return g ? qkd_apply_rows_acc(p, w, t, R, lpr, X, Y, g, nullptr, s)
-             : qkd_apply_rows(p, w, t, R, lpr, X, Y, diag, nullptr, s);
-  };
+  const int lprs[3] = {32, 16, 8};
+  const int ntile = (p->spin && g_kernel_policy == 0) ? 3 : 1;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return QKD_ECUDA;
-  const int shapes[3] = {32, 16, 8};
-  float fastest[3] = {1e30f, 1e30f, 1e30f};
+  float fastest[3][3];
+  for (auto& r : fastest) for (float& v : r) v = 1e30f;
   for (int round = 0; round < 2; ++round)
-    for (int q = 0; q < 3; ++q) {
-      const int lpr = shapes[q];
-      if (R / lpr > 8) continue;
-      if (round == 0 && launch(lpr) != QKD_OK) continue;  // warm-up
-      for (int i = 0; i < 3; ++i) {
-        cudaEventRecord(e0, s);
-        if (launch(lpr) != QKD_OK) break;
-        cudaEventRecord(e1, s);
-        float ms = 0.f;
-        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) break;
-        fastest[q] = std::min(fastest[q], ms);
+    for (int q = 0; q < 3; ++q)
+      for (int tc = 0; tc < ntile; ++tc) {
+        const int lpr = lprs[q];
+        if (R / lpr > 8) continue;
+        auto launch = [&]() { return apply_rows_shape(p, w, t, R, lpr, tc, X, Y, diag, g, nullptr, s); };
+        if (round == 0 && launch() != QKD_OK) continue;  // warm-up
+        for (int i = 0; i < 3; ++i) {
+          cudaEventRecord(e0, s);
+          if (launch() != QKD_OK) break;
+          cudaEventRecord(e1, s);
+          float ms = 0.f;
+          if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) break;
+          fastest[q][tc] = std::min(fastest[q][tc], ms);
+        }
       }
-    }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   (void)cudaGetLastError();
   float best = 1e30f;
-  int pick = 0;
+  int pick = 0, pick_tc = 0;
   for (int q = 0; q < 3; ++q)
-    if (fastest[q] < best) { best = fastest[q]; pick = shapes[q]; }
+    for (int tc = 0; tc < ntile; ++tc)
+      if (fastest[q][tc] < best) { best = fastest[q][tc]; pick = lprs[q]; pick_tc = tc; }
   if (!pick) return QKD_ECUDA;
   p->rows_lpr[t][r_index(R)] = pick;
+  p->rows_tile[t][r_index(R)] = pick_tc;
   if (chosen) *chosen = pick;
   return QKD_OK;
 }

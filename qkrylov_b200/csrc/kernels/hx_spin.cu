@@ -573,11 +573,15 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
 template <class E, int VPL>
 struct alignas(sizeof(E) * VPL) BlkPack { E v[VPL]; };
 
+// Float32 shapes with up to 4 vectors per lane are held to three CTAs per
+// SM (85 registers; the batched FTLM's form): the kernel is latency-bound,
+// and these shapes fit with at most a few spilled words, where the wider
+// types would spill whole rows of accumulators.  The tuner times them all.
 template <int DT, bool GEN, int LPR, int VPL>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, (DT == QK_F32 && VPL <= 4) ? 3 : 1)
 k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, void* __restrict__ Y,
                 double* partials, unsigned* ticket, double* dots, const double* __restrict__ gacc,
-                uint32_t* wq, uint32_t nchunks, uint32_t qsplit, double* tile_part) {
+                uint32_t* wq, uint32_t nchunks, uint32_t qsplit, double* tile_part, const uint4* __restrict__ tiles) {
   using T = VT<DT>;
   using R = typename T::R;
   using E = typename T::E;
@@ -641,7 +645,7 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
   for (uint32_t it = 1; chunk < nchunks; ++it) {
    {
     const uint32_t ti = chunk;
-    const uint4 tile = __ldg(p.btiles + ti);
+    const uint4 tile = __ldg(tiles + ti);
     const RowBlock cur = load_block(p.brec + tile.x);
     const uint32_t base = cur.base, size = tile.y + tile.z, nh = cur.nh;
     __syncthreads();
@@ -795,10 +799,14 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
 
 }  // namespace
 
+constexpr uint32_t kTileRows[3] = {256, 128, 512};  // tile shapes of the block kernel, by tile code
+
 struct SpinHandle {
   SpinPlan host;
   SpinPlan* dev = nullptr;
   void* bufs[20] = {};
+  const uint4* bt[3] = {};  // block-kernel tiles of kTileRows[i] rows
+  uint32_t nbt[3] = {};
   uint32_t* wq = nullptr;  // per-die work queues (8 u32: row kernel, block kernel; zero between launches)
   int n0 = 0, n1 = 0;      // SMs of each die
   bool lean = false;       // every bond conserves the charge: row kernel
@@ -881,14 +889,16 @@ static std::vector<uint32_t> block_order(int H) {
   return o;
 }
 
-// Runs of <= 256 rows of each non-empty block record, in record order or
-// in the visiting order `order` (record indices) when given.
+// Runs of <= `rows` rows of each non-empty block record, in record order or
+// in the visiting order `order` (record indices) when given.  The block
+// kernel has three tile tables (kTileRows) for its shape tuner.
 static std::vector<uint4> block_tiles(const std::vector<RowBlock>& brec,
-                                      const std::vector<uint32_t>& order = std::vector<uint32_t>()) {
+                                      const std::vector<uint32_t>& order = std::vector<uint32_t>(),
+                                      uint32_t rows = 256) {
   std::vector<uint4> t;
   for (uint32_t i = 0; i < uint32_t(brec.size()); ++i) {
     const uint32_t b = order.empty() ? i : order[i];
-    for (uint32_t r = 0; r < brec[b].size; r += 256) t.push_back(make_uint4(b, r, std::min(256u, brec[b].size - r), 0));
+    for (uint32_t r = 0; r < brec[b].size; r += rows) t.push_back(make_uint4(b, r, std::min(rows, brec[b].size - r), 0));
   }
   if (t.empty()) t.push_back(make_uint4(0, 0, 0, 0));
   return t;
@@ -1192,6 +1202,12 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
                             up(16, bent.data(), bent.size() * sizeof(uint2))));
   const std::vector<uint4> btl = h.rows_ok ? block_tiles(brec) : std::vector<uint4>();
   ok = ok && (!h.rows_ok || up(18, btl.data(), btl.size() * sizeof(uint4)));
+  std::vector<uint4> bt1, bt2;
+  if (h.rows_ok) {
+    bt1 = block_tiles(brec, std::vector<uint32_t>(), kTileRows[1]);
+    bt2 = block_tiles(brec, std::vector<uint32_t>(), kTileRows[2]);
+    ok = ok && up(6, bt1.data(), bt1.size() * sizeof(uint4)) && up(7, bt2.data(), bt2.size() * sizeof(uint4));
+  }
   const std::vector<uint32_t> bord = h.rows_ok ? block_order(H) : std::vector<uint32_t>();
   ok = ok && (bord.empty() || up(19, bord.data(), bord.size() * 4));
   if (ok) {
@@ -1208,7 +1224,12 @@ SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.bent = static_cast<const uint2*>(out->bufs[16]);
     h.btiles = static_cast<const uint4*>(out->bufs[18]);
     h.nbtiles = uint32_t(btl.size());
-    if (h.rows_ok) set_die_queues(out, h, brec, bord, dev_bytes);
+    if (h.rows_ok) {
+      out->bt[0] = h.btiles; out->nbt[0] = h.nbtiles;
+      out->bt[1] = static_cast<const uint4*>(out->bufs[6]); out->nbt[1] = uint32_t(bt1.size());
+      out->bt[2] = static_cast<const uint4*>(out->bufs[7]); out->nbt[2] = uint32_t(bt2.size());
+      set_die_queues(out, h, brec, bord, dev_bytes);
+    }
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
          cudaMemcpy(out->dev, &h, sizeof(SpinPlan), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1407,7 +1428,10 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
   // visiting order)
   const std::vector<uint32_t> rord = record_order(rec_h, H, (L % 2 == 0 && H % 2 == 0) ? 2 : 1);
   const std::vector<uint4> tiles = block_tiles(brec);
-  ok = ok && up(18, tiles.data(), tiles.size() * sizeof(uint4)) && up(10, rord.data(), rord.size() * 4);
+  const std::vector<uint4> t1 = block_tiles(brec, std::vector<uint32_t>(), kTileRows[1]);
+  const std::vector<uint4> t2 = block_tiles(brec, std::vector<uint32_t>(), kTileRows[2]);
+  ok = ok && up(18, tiles.data(), tiles.size() * sizeof(uint4)) && up(10, rord.data(), rord.size() * 4) &&
+       up(6, t1.data(), t1.size() * sizeof(uint4)) && up(7, t2.data(), t2.size() * sizeof(uint4));
   if (ok) {
     h.rrec = static_cast<const uint2*>(out->bufs[11]);
     h.lgrp = static_cast<const uint2*>(out->bufs[12]);
@@ -1420,6 +1444,9 @@ SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes) {
     h.border = static_cast<const uint32_t*>(out->bufs[10]);
     h.btiles = static_cast<const uint4*>(out->bufs[18]);
     h.nbtiles = uint32_t(tiles.size());
+    out->bt[0] = h.btiles; out->nbt[0] = h.nbtiles;
+    out->bt[1] = static_cast<const uint4*>(out->bufs[6]); out->nbt[1] = uint32_t(t1.size());
+    out->bt[2] = static_cast<const uint4*>(out->bufs[7]); out->nbt[2] = uint32_t(t2.size());
     set_die_queues(out, h, brec, rord, dev_bytes);
     out->host = h;
     ok = cudaMalloc(reinterpret_cast<void**>(&out->dev), sizeof(SpinPlan)) == cudaSuccess &&
@@ -1474,10 +1501,12 @@ int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
 
 template <int DT, bool GEN, int LPR, int VPL>
 int launch_rows_block(const SpinHandle* h, qk_workspace* w, const void* X, void* Y, double* dots, cudaStream_t s,
-                      const double* gacc) {
+                      const double* gacc, int tilec) {
   auto k = k_hx_rows_block<DT, GEN, LPR, VPL>;
   constexpr uint32_t RV = uint32_t(LPR * VPL);
-  const uint32_t nt = std::max(1u, h->host.nbtiles);
+  if (tilec < 0 || tilec > 2 || !h->bt[tilec]) tilec = 0;
+  const uint4* tiles = h->bt[tilec] ? h->bt[tilec] : h->host.btiles;
+  const uint32_t nt = std::max(1u, h->bt[tilec] ? h->nbt[tilec] : h->host.nbtiles);
   const unsigned g = resident_grid(k, 256, 0, std::min<unsigned>(nt, kMaxG));
   uint32_t* wq = nullptr;
   uint32_t qsplit = nt;
@@ -1502,15 +1531,15 @@ int launch_rows_block(const SpinHandle* h, qk_workspace* w, const void* X, void*
     }
   }
   k<<<g, 256, 0, s>>>(h->dev, X, Y, w->partials, w->ticket, dots ? dots : qkd_workspace_results(w), gacc, wq, nt,
-                      qsplit, tp);
+                      qsplit, tp, tiles);
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
 
 template <int DT, bool GEN>
 int rows_block_shape(const SpinHandle* h, qk_workspace* w, int R, int lpr, const void* X, void* Y, double* dots,
-                     cudaStream_t s, const double* gacc) {
-#define QKD_RB(RR, L, V) if (R == RR && lpr == L) return launch_rows_block<DT, GEN, L, V>(h, w, X, Y, dots, s, gacc);
+                     cudaStream_t s, const double* gacc, int tilec) {
+#define QKD_RB(RR, L, V) if (R == RR && lpr == L) return launch_rows_block<DT, GEN, L, V>(h, w, X, Y, dots, s, gacc, tilec);
   QKD_RB(32, 32, 1) QKD_RB(32, 16, 2) QKD_RB(32, 8, 4)
   QKD_RB(64, 32, 2) QKD_RB(64, 16, 4) QKD_RB(64, 8, 8)
   QKD_RB(128, 32, 4) QKD_RB(128, 16, 8)
@@ -1521,10 +1550,10 @@ int rows_block_shape(const SpinHandle* h, qk_workspace* w, int R, int lpr, const
 // Block apply with the row-kernel tables; QKD_EINVAL when this plan has none.
 // gacc != NULL (R device doubles): Y += diag(gacc) (H X) instead of Y = H X.
 int spin_apply_block(const SpinHandle* h, qk_dtype t, int R, int lpr, const void* X, void* Y, double* dots,
-                     cudaStream_t s, qk_workspace* w, const double* gacc) {
+                     cudaStream_t s, qk_workspace* w, const double* gacc, int tilec) {
   if (!h || !h->host.rows_ok || !h->host.btiles || (h->host.gen && !h->host.diag_full)) return QKD_EINVAL;
-  if (h->host.gen) { QKD_DISPATCH(t, return rows_block_shape<DT, true>(h, w, R, lpr, X, Y, dots, s, gacc)); }
-  QKD_DISPATCH(t, return rows_block_shape<DT, false>(h, w, R, lpr, X, Y, dots, s, gacc));
+  if (h->host.gen) { QKD_DISPATCH(t, return rows_block_shape<DT, true>(h, w, R, lpr, X, Y, dots, s, gacc, tilec)); }
+  QKD_DISPATCH(t, return rows_block_shape<DT, false>(h, w, R, lpr, X, Y, dots, s, gacc, tilec));
   return QKD_EINVAL;
 }
 

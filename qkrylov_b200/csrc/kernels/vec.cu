@@ -143,6 +143,10 @@ __device__ __forceinline__ bool al16(const void* p) { return (reinterpret_cast<u
 // the last whole pack are done by one warp with scalar loads.  If any
 // pointer is not 16-byte aligned the same scheme runs on single elements.
 template <int DT> struct MdotShape { static constexpr int E = 4, J = 4; };
+// 4-byte elements: four per 16-byte pack, so two packs per lane keep the
+// 64 loaded values of four vectors within the registers of three CTAs per SM
+template <> struct MdotShape<QK_F32> { static constexpr int E = 2, J = 4; };
+template <> struct MdotShape<QK_C64> { static constexpr int E = 2, J = 4; };
 
 template <int DT, int W, class LD, class ST>
 __device__ __forceinline__ void mdot_tiles(size_t nq, int M, const UPack& U, int k, const void* const* sV,
@@ -221,8 +225,11 @@ __device__ __forceinline__ void mdot_tiles(size_t nq, int M, const UPack& U, int
   }
 }
 
+// Three CTAs per SM (at most 85 registers): 24 warps keep the streams of
+// vector loads in flight (two CTAs, 102 registers: 4.6 TB/s at 32 float64
+// vectors of 16 M elements, long-scoreboard bound).
 template <int DT>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 3)
 k_update_mdot(size_t n, int M, UPack U, int k,
               const void* const* __restrict__ V, void* x, double* partials, unsigned* ticket,
               double* out) {
@@ -474,13 +481,16 @@ int qkd_update_mdot(qk_workspace* w, qk_dtype t, size_t n, int M, const void* co
   if (k == 0 && M == 0) return QKD_OK;
   UPack up{};
   for (int m = 0; m < M; ++m) { up.u[m] = U[m]; up.ar[m] = a[2 * m]; up.ai[m] = a[2 * m + 1]; }
-  const unsigned G = std::min<unsigned>(reduce_grid(n), kMaxG);
   const size_t smem = size_t(kThreads / 32) * std::max(k, 1) * 2 * sizeof(double) + size_t(k) * sizeof(void*);
   if (smem > 48 * 1024) {
     QKD_DISPATCH(t, cudaFuncSetAttribute(k_update_mdot<DT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   }
-  QKD_DISPATCH(t, k_update_mdot<DT><<<G, kThreads, smem, s>>>(n, M, up, k, V, x, w->partials,
-                                                              w->ticket, out));
+  // one wave: no more CTAs than are resident at once (a second partial
+  // wave would leave most SMs idle at the end)
+  QKD_DISPATCH(t, {
+    const unsigned G = std::min<unsigned>(reduce_grid(n), resident_grid(k_update_mdot<DT>, kThreads, smem, kMaxG));
+    k_update_mdot<DT><<<std::max(1u, G), kThreads, smem, s>>>(n, M, up, k, V, x, w->partials, w->ticket, out);
+  });
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
@@ -504,13 +514,19 @@ int qkd_dot(qk_workspace* w, qk_dtype t, size_t n, const void* x, const void* y,
 int qkd_mupdate(qk_workspace* w, qk_dtype t, size_t n, int k, const void* const* V,
                 const double* c, void* x, double* nrm2, cudaStream_t s) {
   if (!w || !x || k < 0 || k > kMaxK || (k > 0 && (!V || !c))) return QKD_EINVAL;
-  const unsigned G = std::min<unsigned>(reduce_grid(n), kMaxG);
   const size_t smem = (2 * size_t(k) + 16) * sizeof(double) + size_t(k) * sizeof(void*);
+  const unsigned G0 = std::min<unsigned>(reduce_grid(n), kMaxG);
   if (nrm2) {
-    QKD_DISPATCH(t, k_mupdate<DT, true><<<G, kThreads, smem, s>>>(n, k, V, c, x, w->partials, w->ticket, nrm2));
+    QKD_DISPATCH(t, {
+      const unsigned G = std::max(1u, std::min(G0, resident_grid(k_mupdate<DT, true>, kThreads, smem, kMaxG)));
+      k_mupdate<DT, true><<<G, kThreads, smem, s>>>(n, k, V, c, x, w->partials, w->ticket, nrm2);
+    });
   } else {
     if (k == 0) return QKD_OK;
-    QKD_DISPATCH(t, k_mupdate<DT, false><<<G, kThreads, smem, s>>>(n, k, V, c, x, w->partials, w->ticket, nrm2));
+    QKD_DISPATCH(t, {
+      const unsigned G = std::max(1u, std::min(G0, resident_grid(k_mupdate<DT, false>, kThreads, smem, kMaxG)));
+      k_mupdate<DT, false><<<G, kThreads, smem, s>>>(n, k, V, c, x, w->partials, w->ticket, nrm2);
+    });
   }
   QKD_LAUNCH_CHECK();
   return QKD_OK;
