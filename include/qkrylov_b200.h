@@ -113,6 +113,25 @@ int qkrylov_b200_basis_shard_bounds(qkrylov_basis_h basis, int nshards, uint64_t
 int qkrylov_hamiltonian_apply_range_device(qkrylov_hamiltonian_h h, int dtype, const void* x, void* y,
                                            uint64_t row_lo, uint64_t row_hi, void* stream);
 
+/* The block apply's autotuner (no counterpart in the reference; it replaces
+ * the one-vector loop of ftlm.cpp:140-157): the fastest timed launch in ms
+ * for each shape it tried on this operator, dtype and block size R (32, 64
+ * or 128), ms9[3*i + j] for lanes per row 32, 16, 8 (i) and tile code j
+ * (CTA tiles of 256, 128, 512 rows); 0 where a shape was not timed or the
+ * tuner has not run (it runs on the first batched FTLM or sweep). */
+int qkrylov_b200_block_shape_timings(qkrylov_hamiltonian_h h, int dtype, int R, double* ms9);
+/* Block H.X on R vectors stored row-interleaved (element (i, r) at
+ * X[i*R + r]; R = 32, 64 or 128; device memory, 16-byte aligned, X != Y):
+ * Y = H X in one pass that reads each row's terms and target ranks once for
+ * all R vectors (the reference applies one vector at a time,
+ * matrix_free_hamiltonian.cpp:140-168).  lanes_per_row 8, 16 or 32
+ * (R / lanes <= 8) forces a shape, 0 the autotuned one (the first call with
+ * 0 tunes on X and Y).  dots_out: NULL, or a host array of 2R doubles that
+ * receives <X_r, Y_r> (the call then waits for the stream).  stream: NULL
+ * for the library stream. */
+int qkrylov_b200_apply_block_device(qkrylov_hamiltonian_h h, int dtype, int R, int lanes_per_row, const void* X,
+                                    void* Y, double* dots_out, void* stream);
+
 /* ------------------------------------------------------ device vector ops
  * Multi-vector dot out[2j..2j+1] = <V_j, x> = sum_i conj(V_j[i]) x[i] for
  * j < k (the reorthogonalisation coefficients of vector_ops.hpp:14-30

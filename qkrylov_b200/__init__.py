@@ -420,6 +420,27 @@ class MatrixFreeHamiltonian:
                                                       ctypes.c_void_p(y_ptr), ctypes.c_void_p(stream or None)),
                "apply_device")
 
+    def apply_block_device(self, X_ptr: int, Y_ptr: int, dtype: int, R: int, lanes_per_row: int = 0,
+                           dots: bool = False, stream: int = 0):
+        """Y = H X for R row-interleaved vectors (element (i, r) at X[i*R + r])
+        on device pointers; returns the 2R column dots <X_r, Y_r> (re, im
+        interleaved) when dots, else None (no sync)."""
+        out = np.zeros(2 * R) if dots else None
+        _check(lib().qkrylov_b200_apply_block_device(self._h, dtype, int(R), int(lanes_per_row), ctypes.c_void_p(X_ptr),
+                                                     ctypes.c_void_p(Y_ptr), out.ctypes.data if dots else None,
+                                                     ctypes.c_void_p(stream or None)), "apply_block_device")
+        return out
+
+    def block_shape_timings(self, precision: int = 64, R: int = 64) -> np.ndarray:
+        """The block apply's autotuner table for this operator: fastest timed
+        launch in ms, rows = lanes per row 32, 16, 8, columns = CTA tiles of
+        256, 128, 512 rows; 0 where not timed (the tuner runs on the first
+        batched FTLM or sweep with this precision and block size)."""
+        dt = {64: DTYPE_F64, 32: DTYPE_F32}[precision]
+        out = np.zeros(9)
+        _check(lib().qkrylov_b200_block_shape_timings(self._h, dt, int(R), out.ctypes.data), "block_shape_timings")
+        return out.reshape(3, 3)
+
     @property
     def kernel(self) -> str:
         """The H.x kernel this operator uses: 'spin-exchange' (two-site

@@ -101,6 +101,8 @@ PROTOTYPES = {
     "qkrylov_b200_cf_checkpointed": (_i, [_vp, _vp, _cp, _i, _cp, _vp, _vp, _vp, _vp, _vp]),
     "qkrylov_b200_basis_shard_bounds": (_i, [_vp, _i, _vp]),
     "qkrylov_hamiltonian_apply_range_device": (_i, [_vp, _i, _vp, _vp, _u64, _u64, _vp]),
+    "qkrylov_b200_block_shape_timings": (_i, [_vp, _i, _i, _vp]),
+    "qkrylov_b200_apply_block_device": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp]),
     "qkrylov_ftlm_sweep_f64": (_i, [_vp, _i, _vp, _i, _i, _vp, _vp, _vp]),
     "qkrylov_b200_lanczos_mixed": (_i, [_vp, _u64, _vp, _i, _i, _d, _vp, _vp, _i, _vp, _vp, _vp]),
     "qkrylov_b200_lanczos_fp64": (_i, [_vp, _u64, _vp, _i, _i, _d, _vp, _vp, _i, _vp, _vp, _vp]),

@@ -223,6 +223,49 @@ int qkrylov_hamiltonian_apply_range_device(qkrylov_hamiltonian_h h, int dtype, c
   });
 }
 
+int qkrylov_b200_apply_block_device(qkrylov_hamiltonian_h h, int dtype, int R, int lanes_per_row, const void* X,
+                                    void* Y, double* dots_out, void* stream) {
+  if (!h || !h->op || !X || !Y || X == Y || !valid_dtype(dtype) || (R != 32 && R != 64 && R != 128) ||
+      (lanes_per_row != 0 && lanes_per_row != 8 && lanes_per_row != 16 && lanes_per_row != 32) ||
+      (lanes_per_row != 0 && R / lanes_per_row > 8))
+    return QKRYLOV_ERROR_INVALID_ARG;
+  if ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) & 15u) {
+    qkapi::set_error("apply_block: X and Y must be 16-byte aligned");
+    return QKRYLOV_ERROR_INVALID_ARG;
+  }
+  return guarded([&] {
+    auto& c = h->op->ctx();
+    c.activate();
+    const cudaStream_t s = stream ? cudaStream_t(stream) : c.stream;
+    qk_plan* plan = const_cast<qk_plan*>(h->op->plan());
+    const qk_dtype t = qk_dtype(dtype);
+    if (lanes_per_row == 0 && !qkd_rows_shape(plan, t, R)) {  // first call: tune the shape on these blocks
+      int chosen = 0;
+      const int rc = qkd_tune_rows(plan, c.ws, t, R, X, Y, nullptr, s, &chosen);
+      if (rc == QKD_EINVAL) { qkapi::set_error("apply_block: invalid dtype for this operator"); return QKRYLOV_ERROR_INVALID_ARG; }
+      qkb::qkd_check(rc, "block shape tuning");
+    }
+    double* dd = dots_out ? c.dres(0) : nullptr;
+    const int rc = qkd_apply_rows(plan, c.ws, t, R, lanes_per_row, X, Y, nullptr, dd, s);
+    if (rc == QKD_EINVAL) { qkapi::set_error("apply_block: invalid dtype for this operator"); return QKRYLOV_ERROR_INVALID_ARG; }
+    qkb::qkd_check(rc, "block H.X");
+    if (dots_out) {
+      if (s != c.stream) qkb::cuda_check(cudaStreamSynchronize(s), "block H.X");
+      const double* v = c.fetch(dd, 2 * R);
+      for (int i = 0; i < 2 * R; ++i) dots_out[i] = v[i];
+    }
+    return QKRYLOV_SUCCESS;
+  });
+}
+
+int qkrylov_b200_block_shape_timings(qkrylov_hamiltonian_h h, int dtype, int R, double* ms9) {
+  if (!h || !h->op || !ms9 || !valid_dtype(dtype)) return QKRYLOV_ERROR_INVALID_ARG;
+  float f[9];
+  if (qkd_rows_timings(h->op->plan(), qk_dtype(dtype), R, f) != QKD_OK) return QKRYLOV_ERROR_INVALID_ARG;
+  for (int i = 0; i < 9; ++i) ms9[i] = f[i];
+  return QKRYLOV_SUCCESS;
+}
+
 int qkrylov_hamiltonian_diagonal_device(qkrylov_hamiltonian_h h, int dtype, void* d, void* stream) {
   if (!h || !h->op || !d || !valid_dtype(dtype)) return QKRYLOV_ERROR_INVALID_ARG;
   return guarded([&] {

@@ -99,6 +99,9 @@ int qkd_tune_rows_acc(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void
                       cudaStream_t s, int* chosen);
 /* The tuned lanes per row for (t, R), 0 before tuning. */
 int qkd_rows_shape(const qk_plan* p, qk_dtype t, int R);
+/* The tuner's fastest launch (ms) for lanes per row 32, 16, 8 (rows) x tile
+ * code 0, 1, 2 (columns), row-major; 0 where a shape was not timed. */
+int qkd_rows_timings(const qk_plan* p, qk_dtype t, int R, float* ms9);
 /* diag[i] = <i|H|i> as dtype t. */
 int qkd_diagonal(const qk_plan* p, qk_dtype t, void* diag, cudaStream_t s);
 /* Number of kernel launches issued by this library since load (for the

@@ -50,6 +50,7 @@ struct qk_plan {
   size_t bytes, smem;
   int rows_lpr[4][3];   // autotuned lanes per row of the block apply, by dtype and R = 32, 64, 128
   int rows_tile[4][3];  // autotuned tile shape of the block apply (row kernels: 256 / 128 / 512 rows)
+  float rows_ms[4][3][9];  // the tuner's fastest launch (ms) per lanes per row (32/16/8) x tile code; 0: untimed
   double* diag_re;     // real diagonal (generic-kernel operators with a real diagonal), else null
 };
 
@@ -595,6 +596,12 @@ int qkd_rows_shape(const qk_plan* p, qk_dtype t, int R) {
   return p->rows_lpr[t][r_index(R)];
 }
 
+int qkd_rows_timings(const qk_plan* p, qk_dtype t, int R, float* ms9) {
+  if (!p || !ms9 || r_index(R) < 0 || t < QK_C128 || t > QK_F32) return QKD_EINVAL;
+  for (int i = 0; i < 9; ++i) ms9[i] = p->rows_ms[t][r_index(R)][i];
+  return QKD_OK;
+}
+
 // The block apply's shape: lanes per row (so vectors per lane R / lanes)
 // times tile rows (the rows a CTA takes per fetch: 256, 128 or 512; row
 // kernels only), each timed launch by launch in two interleaved rounds of
@@ -635,6 +642,9 @@ static int tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void*
     for (int tc = 0; tc < ntile; ++tc)
       if (fastest[q][tc] < best) { best = fastest[q][tc]; pick = lprs[q]; pick_tc = tc; }
   if (!pick) return QKD_ECUDA;
+  for (int q = 0; q < 3; ++q)
+    for (int tc = 0; tc < 3; ++tc)
+      p->rows_ms[t][r_index(R)][q * 3 + tc] = (tc < ntile && fastest[q][tc] < 1e29f) ? fastest[q][tc] : 0.f;
   p->rows_lpr[t][r_index(R)] = pick;
   p->rows_tile[t][r_index(R)] = pick_tc;
   if (chosen) *chosen = pick;

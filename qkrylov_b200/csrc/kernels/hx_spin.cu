@@ -211,6 +211,9 @@ constexpr int kRowCoef = 32, kRowEnt = 48, kRowCross = 16, kRowCls = 4;
 template <int DT> constexpr int kRowBatch = DT == QK_C128 ? 1 : 4;  // rows per thread and pass
 template <int DT> constexpr int kRowHighRegs = DT == QK_C128 ? kRowHighC128 : 8;  // high bonds held in registers
 template <int DT> constexpr bool kRowPipe = DT == QK_C128;  // rows pipelined one ahead (one row per thread)
+// two-part crossing groups whose loads are issued together (fewer where a
+// thread holds several rows, to stay within its registers)
+template <int DT> constexpr int kCrossBatch = kRowBatch<DT> == 1 ? 4 : 2;
 
 __device__ __forceinline__ void sld(const double2* s, uint32_t k, double& re, double& im) {
   const double2 v = s[k]; re = v.x; im = v.y;
@@ -234,6 +237,24 @@ __device__ __forceinline__ void l2_prefetch(const void* base, uint32_t es, uint3
   const uintptr_t hi = (b + uintptr_t(first + count) * es) & ~uintptr_t(15);
   if (hi > lo)
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"(uint32_t(hi - lo)) : "memory");
+}
+
+// Coefficient of a two-part crossing group in a row: up to two terms, each
+// valid when its low condition (row table word `ent`) and its high
+// condition (block entry flags `bf`) hold, signed by the parities of both
+// parts.  Terms are added in order (first, then second).
+template <class R>
+__device__ __forceinline__ R cross_coef(uint32_t ent, uint32_t bf, const R* s_coef) {
+  R c = R(0);
+  if ((ent >> 24) & (bf >> 16) & 1u) {
+    const R w = s_coef[bf & 0xFFu];
+    c += (((ent >> 25) ^ (bf >> 17)) & 1u) ? -w : w;
+  }
+  if ((ent >> 26) & (bf >> 18) & 1u) {
+    const R w = s_coef[(bf >> 8) & 0xFFu];
+    c += (((ent >> 27) ^ (bf >> 19)) & 1u) ? -w : w;
+  }
+  return c;
 }
 
 __device__ __forceinline__ RowBlock load_block(const RowBlock* p) {
@@ -488,26 +509,33 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
           // low condition (row table) and high condition (block entry) hold,
           // with the sign of both parts' Jordan-Wigner / Sz parities
           // only the groups with a term valid in both parts: the row's low
-          // mask and the block's high mask
-          for (uint32_t m = __ldg(p.crm + pos[k]) & chm; m; m &= m - 1u) {
-            const int q = __ffs(m) - 1;
-            const uint32_t bf = s_ebit[q];
-            const uint32_t ent = __ldg(p.crk32 + size_t(q) * nll + pos[k]);
-            R c = R(0);
-            if ((ent >> 24) & (bf >> 16) & 1u) {
-              const R w = s_coef[bf & 0xFFu];
-              c += (((ent >> 25) ^ (bf >> 17)) & 1u) ? -w : w;
+          // mask and the block's high mask.  Four groups at a time: their
+          // table words, then their partner values, are in flight together
+          // (sums still in ascending group order).
+          for (uint32_t m = __ldg(p.crm + pos[k]) & chm; m;) {
+            constexpr int CBAT = kCrossBatch<DT>;
+            int qq[CBAT];
+            uint32_t ent[CBAT];
+            #pragma unroll
+            for (int u = 0; u < CBAT; ++u) {
+              qq[u] = m ? __ffs(m) - 1 : -1;
+              m &= m - 1u;
+              ent[u] = qq[u] >= 0 ? __ldg(p.crk32 + size_t(qq[u]) * nll + pos[k]) : 0u;
             }
-            if ((ent >> 26) & (bf >> 18) & 1u) {
-              const R w = s_coef[(bf >> 8) & 0xFFu];
-              c += (((ent >> 27) ^ (bf >> 19)) & 1u) ? -w : w;
+            R cq[CBAT], vr[CBAT], vi[CBAT];
+            #pragma unroll
+            for (int u = 0; u < CBAT; ++u) {
+              cq[u] = qq[u] >= 0 ? cross_coef<R>(ent[u], s_ebit[qq[u]], s_coef) : R(0);
+              vr[u] = R(0);
+              vi[u] = R(0);
+              if (cq[u] != R(0)) T::ld(x, s_eb[nh + qq[u]] + (ent[u] & 0xFFFFFFu), vr[u], vi[u]);
             }
-            if (c != R(0)) {
-              R vr, vi;
-              T::ld(x, s_eb[nh + q] + (ent & 0xFFFFFFu), vr, vi);
-              ar[k] += c * vr;
-              if (T::cplx) ai[k] += c * vi;
-            }
+            #pragma unroll
+            for (int u = 0; u < CBAT; ++u)
+              if (cq[u] != R(0)) {
+                ar[k] += cq[u] * vr[u];
+                if (T::cplx) ai[k] += cq[u] * vi[u];
+              }
           }
         }
         for (int q = 2; q < ncr; q += 2) {
@@ -587,6 +615,7 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
   using E = typename T::E;
   using Pack = BlkPack<E, VPL>;
   constexpr int RV = LPR * VPL, RPW = 32 / LPR;
+  constexpr int NBAT = VPL * sizeof(E) <= 16 ? 4 : 2;  // partner rows in flight per batch
   const SpinPlan& p = *pp;
   __shared__ R s_coef[kRowCoef], s_lc[kRowCls], s_ec[kRowEnt];
   __shared__ uint32_t s_eb[kRowEnt], s_ebit[kRowCross];
@@ -691,44 +720,62 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
         #pragma unroll
         for (int v = 0; v < VPL; ++v) { ar[v] += s_lc[c] * sr[v]; if (T::cplx) ai[v] += s_lc[c] * si[v]; }
       }
-      // high bonds: the same row of a partner block
-      for (uint32_t e = 0; e < nh; ++e) {
-        R vr[VPL], vi[VPL];
-        ldrow(s_eb[e] + r, vr, vi);
-        const R c = s_ec[e];
+      // high bonds: the same row of a partner block, NBAT partner rows in
+      // flight at a time
+      for (uint32_t e0 = 0; e0 < nh; e0 += NBAT) {
+        R vr[NBAT][VPL], vi[NBAT][VPL];
         #pragma unroll
-        for (int v = 0; v < VPL; ++v) { ar[v] += c * vr[v]; if (T::cplx) ai[v] += c * vi[v]; }
+        for (int u = 0; u < NBAT; ++u) {
+          #pragma unroll
+          for (int v = 0; v < VPL; ++v) { vr[u][v] = R(0); vi[u][v] = R(0); }
+          if (e0 + u < nh) ldrow(s_eb[e0 + u] + r, vr[u], vi[u]);
+        }
+        #pragma unroll
+        for (int u = 0; u < NBAT; ++u)
+          if (e0 + u < nh) {
+            const R c = s_ec[e0 + u];
+            #pragma unroll
+            for (int v = 0; v < VPL; ++v) { ar[v] += c * vr[u][v]; if (T::cplx) ai[v] += c * vi[u][v]; }
+          }
       }
       // crossing bonds (two-part: only the groups the row's low mask and the
-      // block's high mask both allow)
-      const uint32_t cmask = GEN ? (__ldg(p.crm + pos) & chm) : ((1u << ncross) - 1u);
-      for (int q = 0; q < ncross; ++q) {
-        if (!((cmask >> q) & 1u)) continue;
-        R c = R(0);
-        uint32_t rank = 0;
-        if constexpr (GEN) {
-          const uint32_t bf = s_ebit[q];
-          const uint32_t ent = __ldg(p.crk32 + size_t(q) * p.nllist + pos);
-          if ((ent >> 24) & (bf >> 16) & 1u) {
-            const R w = s_coef[bf & 0xFFu];
-            c += (((ent >> 25) ^ (bf >> 17)) & 1u) ? -w : w;
-          }
-          if ((ent >> 26) & (bf >> 18) & 1u) {
-            const R w = s_coef[(bf >> 8) & 0xFFu];
-            c += (((ent >> 27) ^ (bf >> 19)) & 1u) ? -w : w;
-          }
-          rank = ent & 0xFFFFFFu;
-        } else {
-          const uint32_t ent = __ldg(p.crk + size_t(pos) * cpad + q);
-          if ((ent >> 15) != s_ebit[q]) c = s_ec[nh + q];
-          rank = ent & 0x7FFFu;
+      // block's high mask both allow), NBAT groups at a time: their table
+      // words, then their partner rows, in flight together
+      for (uint32_t m = GEN ? (__ldg(p.crm + pos) & chm) : ((1u << ncross) - 1u); m;) {
+        int qq[NBAT];
+        uint32_t ent[NBAT];
+        #pragma unroll
+        for (int u = 0; u < NBAT; ++u) {
+          qq[u] = m ? __ffs(m) - 1 : -1;
+          m &= m - 1u;
+          ent[u] = qq[u] < 0 ? 0u
+                   : GEN ? __ldg(p.crk32 + size_t(qq[u]) * p.nllist + pos)
+                         : uint32_t(__ldg(p.crk + size_t(pos) * cpad + qq[u]));
         }
-        if (c != R(0)) {
-          R vr[VPL], vi[VPL];
-          ldrow(s_eb[nh + q] + rank, vr, vi);
+        R cq[NBAT], vr[NBAT][VPL], vi[NBAT][VPL];
+        #pragma unroll
+        for (int u = 0; u < NBAT; ++u) {
+          uint32_t rank = 0;
+          cq[u] = R(0);
+          if (qq[u] >= 0) {
+            if constexpr (GEN) {
+              cq[u] = cross_coef<R>(ent[u], s_ebit[qq[u]], s_coef);
+              rank = ent[u] & 0xFFFFFFu;
+            } else {
+              if ((ent[u] >> 15) != s_ebit[qq[u]]) cq[u] = s_ec[nh + qq[u]];
+              rank = ent[u] & 0x7FFFu;
+            }
+          }
           #pragma unroll
-          for (int v = 0; v < VPL; ++v) { ar[v] += c * vr[v]; if (T::cplx) ai[v] += c * vi[v]; }
+          for (int v = 0; v < VPL; ++v) { vr[u][v] = R(0); vi[u][v] = R(0); }
+          if (cq[u] != R(0)) ldrow(s_eb[nh + qq[u]] + rank, vr[u], vi[u]);
         }
+        #pragma unroll
+        for (int u = 0; u < NBAT; ++u)
+          if (cq[u] != R(0)) {
+            #pragma unroll
+            for (int v = 0; v < VPL; ++v) { ar[v] += cq[u] * vr[u][v]; if (T::cplx) ai[v] += cq[u] * vi[u][v]; }
+          }
       }
       Pack yv;
       if (gacc) {
