@@ -650,7 +650,9 @@ def profile_case(qk, name):
                        kernels of the Davidson projection and the Lanczos
                        reorthogonalisation, at C3's vector length / 10)
       sweep-n20        the batched coupling sweep on the J1-J2 chain N=20 (its
-                       column multi-dot / multi-update kernels)"""
+                       column multi-dot / multi-update kernels)
+      hub44-hx         Hubbard 4x4, U=4, 8 up 8 down (dim 165,636,900) two-part
+                       row kernel, float64, 3 applies (2.6 GB of vectors)"""
     import torch
     out = {}
     if name in ("tj20-hx", "tj20-ftlm-block"):
@@ -661,6 +663,7 @@ def profile_case(qk, name):
         if name == "tj20-hx":
             x = torch.randn(H.dimension, dtype=torch.float64, device="cuda")
             y = torch.empty_like(x)
+            torch.cuda.synchronize()  # x comes from torch's stream, the applies run on the library's
             for _ in range(4):
                 H.apply_device(x.data_ptr(), y.data_ptr(), qk.DTYPE_F64)
             torch.cuda.synchronize()
@@ -681,6 +684,16 @@ def profile_case(qk, name):
             L.qkrylov_b200_multi_dot(torch.cuda.current_device(), qk.DTYPE_F64, n, k, ptrs,
                                      ctypes.c_void_p(x.data_ptr()), o.ctypes.data)
         out.update(n=n, k=k)
+    elif name == "hub44-hx":
+        H = qk.MatrixFreeHamiltonian(qk.HubbardBasis(16, nup=8, ndn=8), qk.HubbardSite(),
+                                     hubbard_opsum(qk, 4, 4, 1.0, 4.0), dtype=np.float64)
+        out["dim"] = H.dimension
+        x = torch.randn(H.dimension, dtype=torch.float64, device="cuda")
+        y = torch.empty_like(x)
+        torch.cuda.synchronize()
+        for _ in range(3):
+            H.apply_device(x.data_ptr(), y.data_ptr(), qk.DTYPE_F64)
+        torch.cuda.synchronize()
     elif name == "sweep-n20":
         out.update(coupling_sweep(qk, N=20, sequential=False))
     else:

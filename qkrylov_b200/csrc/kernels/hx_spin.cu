@@ -601,12 +601,16 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
 template <class E, int VPL>
 struct alignas(sizeof(E) * VPL) BlkPack { E v[VPL]; };
 
-// Float32 shapes with up to 4 vectors per lane are held to three CTAs per
-// SM (85 registers; the batched FTLM's form): the kernel is latency-bound,
-// and these shapes fit with at most a few spilled words, where the wider
-// types would spill whole rows of accumulators.  The tuner times them all.
+// Registers are sized by the bytes a lane loads per target row: up to 16
+// bytes four CTAs per SM (64 registers), up to 32 bytes two, wider one.  The
+// kernel is latency-bound, so resident warps count more than the few words
+// the narrow shapes spill (t-J N=20, 64 float64 vectors: 12.7 -> 9.5 ms per
+// apply against one CTA per SM for every shape).  The tuner times them all.
+template <int DT, int VPL>
+constexpr int kBlockMinCta = VPL * int(sizeof(typename VT<DT>::E)) <= 16 ? 4
+                             : VPL * int(sizeof(typename VT<DT>::E)) <= 32 ? 2 : 1;
 template <int DT, bool GEN, int LPR, int VPL>
-__global__ void __launch_bounds__(256, (DT == QK_F32 && VPL <= 4) ? 3 : 1)
+__global__ void __launch_bounds__(256, kBlockMinCta<DT, VPL>)
 k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, void* __restrict__ Y,
                 double* partials, unsigned* ticket, double* dots, const double* __restrict__ gacc,
                 uint32_t* wq, uint32_t nchunks, uint32_t qsplit, double* tile_part, const uint4* __restrict__ tiles) {
