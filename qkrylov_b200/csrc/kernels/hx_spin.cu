@@ -205,12 +205,14 @@ k_hx_spin(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __r
 constexpr int kRowThreads = 256;
 constexpr uint32_t kRowStreamY = 1u;  // launch flag: store y with the streaming (evict-first) hint
 constexpr int kRowHighC128 = 4;   // complex128: high bonds held in registers (more spill)
-constexpr int kRowMinCtaC128 = 3; // complex128: CTAs per SM the registers are sized for
+constexpr int kRowMinCtaC128 = 2; // complex128: CTAs per SM the registers are sized for
+constexpr int kRowThreadsC128 = 512;  // complex128: threads per CTA (one staged block shared by 16 warps)
 constexpr int kPrefetchAhead = 2; // row chunks of high-bond partner rows prefetched into L2
 constexpr int kRowCoef = 32, kRowEnt = 48, kRowCross = 16, kRowCls = 4;
 template <int DT> constexpr int kRowBatch = DT == QK_C128 ? 1 : 4;  // rows per thread and pass
 template <int DT> constexpr int kRowHighRegs = DT == QK_C128 ? kRowHighC128 : 8;  // high bonds held in registers
 template <int DT> constexpr bool kRowPipe = DT == QK_C128;  // rows pipelined one ahead (one row per thread)
+template <int DT> constexpr int kRowNT = DT == QK_C128 ? kRowThreadsC128 : kRowThreads;  // threads per CTA
 // two-part crossing groups whose loads are issued together (fewer where a
 // thread holds several rows, to stay within its registers)
 template <int DT> constexpr int kCrossBatch = kRowBatch<DT> == 1 ? 4 : 2;
@@ -298,7 +300,7 @@ __device__ __forceinline__ void wq_done(uint32_t* wq) {
 }
 
 template <int DT, bool DOT, bool GEN>
-__global__ void __launch_bounds__(kRowThreads, DT == QK_C128 ? kRowMinCtaC128 : 4)
+__global__ void __launch_bounds__(kRowNT<DT>, DT == QK_C128 ? kRowMinCtaC128 : 4)
 k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
                double* partials, unsigned* ticket, double* dot_out, uint32_t* wq, uint32_t row_lo,
                uint32_t row_hi, uint32_t flags) {
@@ -332,7 +334,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
   }
   // DOT: one partial per block record, so the sum does not depend on which
   // CTA took which block
-  __shared__ double s_dot[2 * (kRowThreads / 32)];
+  __shared__ double s_dot[2 * (kRowNT<DT> / 32)];
   uint32_t nrec = pos < nA ? (bord ? __ldg(bord + pos) : pos) : 0u;
   if (pos < nA) nxt = load_block(p.brec + nrec);
   for (uint32_t it = 1; pos < nA; ++it) {
@@ -356,7 +358,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
     }
     const uint32_t base = cur.base, size = cur.size, nh = cur.nh;
     __syncthreads();  // the previous block is finished with the staging and the entry tables
-    for (uint32_t r = threadIdx.x; r < size; r += kRowThreads) sx[r] = __ldg(xg + base + r);
+    for (uint32_t r = threadIdx.x; r < size; r += kRowNT<DT>) sx[r] = __ldg(xg + base + r);
     if (threadIdx.x < nh + uint32_t(ncross)) {
       const uint2 e = __ldg(p.bent + cur.ebeg + threadIdx.x);
       s_eb[threadIdx.x] = e.x;
@@ -364,7 +366,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       s_ec[threadIdx.x] = (GEN && threadIdx.x >= nh) ? R(0) : s_coef[e.y & 0xFFFFu];
       if (threadIdx.x >= nh) s_ebit[threadIdx.x - nh] = GEN ? e.y : e.y >> 16;
       else  // high partner rows of the first row chunks into L2
-        l2_prefetch(x, sizeof(E), e.x, min(size, uint32_t(kPrefetchAhead) * kRowBatch<DT> * kRowThreads));
+        l2_prefetch(x, sizeof(E), e.x, min(size, uint32_t(kPrefetchAhead) * kRowBatch<DT> * kRowNT<DT>));
     }
     __syncthreads();
     const R dh = R(cur.dh);
@@ -410,12 +412,12 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       ndt = __ldg(dcol + pz);
       ntwo = ncr ? __ldg(ckw + pz * cw) : 0u;
     }
-    for (uint32_t r0 = threadIdx.x; r0 < size; r0 += K * kRowThreads) {
+    for (uint32_t r0 = threadIdx.x; r0 < size; r0 += K * kRowNT<DT>) {
       // the high partner rows two chunks ahead go to L2 while this chunk runs
       {
-        const uint32_t ahead = r0 - threadIdx.x + uint32_t(kPrefetchAhead) * K * kRowThreads;
+        const uint32_t ahead = r0 - threadIdx.x + uint32_t(kPrefetchAhead) * K * kRowNT<DT>;
         if (threadIdx.x < nh && ahead < size)
-          l2_prefetch(x, sizeof(E), s_eb[threadIdx.x] + ahead, min(size - ahead, uint32_t(K * kRowThreads)));
+          l2_prefetch(x, sizeof(E), s_eb[threadIdx.x] + ahead, min(size - ahead, uint32_t(K * kRowNT<DT>)));
       }
       // K rows r0 + k * 256 per thread.  Loads that do not depend on each
       // other are issued together: row records, diagonals, crossing pairs,
@@ -427,7 +429,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       uint32_t two[K];
       #pragma unroll
       for (int k = 0; k < K; ++k) {
-        rk[k] = r0 + k * kRowThreads;
+        rk[k] = r0 + k * kRowNT<DT>;
         ok[k] = rk[k] < size;
         pos[k] = cur.lst + (ok[k] ? rk[k] : 0u);
         if constexpr (PIPE) {
@@ -439,7 +441,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
         }
       }
       if constexpr (PIPE) {
-        const uint32_t rn = r0 + kRowThreads;
+        const uint32_t rn = r0 + kRowNT<DT>;
         if (rn < size) {
           const uint32_t pz = cur.lst + rn;
           nrec = __ldg(p.rrec + pz);
@@ -1530,9 +1532,9 @@ int spin_apply_rows(const SpinHandle* h, qk_dtype t, const void* x, void* y, cud
         cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)    \
       return QKD_EINVAL;                                                                                  \
     const unsigned cap = std::max(1u, h->host.nblocks);                                                   \
-    if (dot_out) kd<<<resident_grid(kd, kRowThreads, smem, std::min<unsigned>(cap, kMaxG)), kRowThreads, smem, s>>>( \
+    if (dot_out) kd<<<resident_grid(kd, kRowNT<DT>, smem, std::min<unsigned>(cap, kMaxG)), kRowNT<DT>, smem, s>>>( \
         h->dev, x, y, w->partials, w->ticket, dot_out, wq, rlo, rhi, g_row_flags);                        \
-    else kn<<<resident_grid(kn, kRowThreads, smem, cap), kRowThreads, smem, s>>>(h->dev, x, y, nullptr, nullptr, \
+    else kn<<<resident_grid(kn, kRowNT<DT>, smem, cap), kRowNT<DT>, smem, s>>>(h->dev, x, y, nullptr, nullptr, \
                                                                                  nullptr, wq, rlo, rhi,   \
                                                                                  g_row_flags);            \
   }
