@@ -209,13 +209,23 @@ constexpr int kRowMinCtaC128 = 2; // complex128: CTAs per SM the registers are s
 constexpr int kRowThreadsC128 = 512;  // complex128: threads per CTA (one staged block shared by 16 warps)
 constexpr int kPrefetchAhead = 2; // row chunks of high-bond partner rows prefetched into L2
 constexpr int kRowCoef = 32, kRowEnt = 48, kRowCross = 16, kRowCls = 4;
-template <int DT> constexpr int kRowBatch = DT == QK_C128 ? 1 : 4;  // rows per thread and pass
+// Rows per thread and pass (K) and CTAs per SM the registers are sized for,
+// by vector type and table form.  The kernel is latency-bound, so resident
+// warps count for more than the words they spill; measured on Heisenberg
+// N=28 (exchange tables), t-J N=20 and Hubbard 4x4 (two-part tables)
+// against K = 4 at 4 CTAs: float32 0.576 -> 0.441 ms (K = 1, 8 CTAs),
+// float64 0.803 -> 0.580 ms (K = 2, 6 CTAs), complex64 0.620 -> 0.587 ms
+// (K = 2, 6 CTAs); two-part float64 t-J 0.414 -> 0.347 ms and Hubbard
+// 16.0 -> 13.0 ms (K = 1, 6 CTAs), float32 Hubbard 13.6 -> 8.8 ms (K = 1,
+// 8 CTAs).  complex128: one row per thread, 512-thread CTAs, 2 per SM.
+template <int DT, bool GEN> constexpr int kRowBatchG = DT == QK_C128 ? 1 : DT == QK_F32 ? 1 : GEN && DT == QK_F64 ? 1 : 2;
+template <int DT, bool GEN> constexpr int kRowMinCta = DT == QK_C128 ? kRowMinCtaC128 : DT == QK_F32 ? 8 : 6;
 template <int DT> constexpr int kRowHighRegs = DT == QK_C128 ? kRowHighC128 : 8;  // high bonds held in registers
 template <int DT> constexpr bool kRowPipe = DT == QK_C128;  // rows pipelined one ahead (one row per thread)
 template <int DT> constexpr int kRowNT = DT == QK_C128 ? kRowThreadsC128 : kRowThreads;  // threads per CTA
 // two-part crossing groups whose loads are issued together (fewer where a
 // thread holds several rows, to stay within its registers)
-template <int DT> constexpr int kCrossBatch = kRowBatch<DT> == 1 ? 4 : 2;
+template <int DT, bool GEN> constexpr int kCrossBatch = kRowBatchG<DT, GEN> == 1 ? 4 : 2;
 
 __device__ __forceinline__ void sld(const double2* s, uint32_t k, double& re, double& im) {
   const double2 v = s[k]; re = v.x; im = v.y;
@@ -300,7 +310,7 @@ __device__ __forceinline__ void wq_done(uint32_t* wq) {
 }
 
 template <int DT, bool DOT, bool GEN>
-__global__ void __launch_bounds__(kRowNT<DT>, DT == QK_C128 ? kRowMinCtaC128 : 4)
+__global__ void __launch_bounds__(kRowNT<DT>, kRowMinCta<DT, GEN>)
 k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __restrict__ y,
                double* partials, unsigned* ticket, double* dot_out, uint32_t* wq, uint32_t row_lo,
                uint32_t row_hi, uint32_t flags) {
@@ -366,7 +376,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       s_ec[threadIdx.x] = (GEN && threadIdx.x >= nh) ? R(0) : s_coef[e.y & 0xFFFFu];
       if (threadIdx.x >= nh) s_ebit[threadIdx.x - nh] = GEN ? e.y : e.y >> 16;
       else  // high partner rows of the first row chunks into L2
-        l2_prefetch(x, sizeof(E), e.x, min(size, uint32_t(kPrefetchAhead) * kRowBatch<DT> * kRowNT<DT>));
+        l2_prefetch(x, sizeof(E), e.x, min(size, uint32_t(kPrefetchAhead) * kRowBatchG<DT, GEN> * kRowNT<DT>));
     }
     __syncthreads();
     const R dh = R(cur.dh);
@@ -394,7 +404,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
       cbit[u] = u < ncr ? s_ebit[u] : 2u;  // 2: never equal to a low bit, never valid
       cc[u] = u < ncr ? s_ec[nh + u] : R(0);
     }
-    constexpr int K = kRowBatch<DT>;
+    constexpr int K = kRowBatchG<DT, GEN>;
     // complex128 exchange tables: the row tables (record, diagonal,
     // crossing ranks) of a thread's next row are loaded while the current row
     // runs, so the loads that depend on them (low groups, crossing partners)
@@ -515,7 +525,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
           // table words, then their partner values, are in flight together
           // (sums still in ascending group order).
           for (uint32_t m = __ldg(p.crm + pos[k]) & chm; m;) {
-            constexpr int CBAT = kCrossBatch<DT>;
+            constexpr int CBAT = kCrossBatch<DT, GEN>;
             int qq[CBAT];
             uint32_t ent[CBAT];
             #pragma unroll
