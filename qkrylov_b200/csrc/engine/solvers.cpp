@@ -465,12 +465,46 @@ DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int bl
   PtrArray P(size_t(max_subspace) + 4, dev);
   DevVec coef(size_t(2) * (max_subspace + 8), QK_F64, dev);
   double* cd = static_cast<double*>(coef.data());
+  // many-against-many passes: up to kX vectors X_a against the basis in one
+  // pass over it (projections <V_i, X_a>, combinations sum_i c_ia V_i)
+  constexpr int kX = 8;
+  PtrArray PX(kX, dev), PN(size_t(block), dev);
+  const int mrows = (max_subspace + 7) / 8 * 8;
+  DevVec cm(size_t(max_subspace) * kX, QK_F64, dev), dm(size_t(16) * mrows, QK_F64, dev);
+  std::vector<double> dmh(size_t(16) * mrows);
+  // D[i*nx + a] = <V_i, X_a> for i < mm
+  auto multi_dot = [&](int mm, const std::vector<void*>& xs) {
+    const int nx = int(xs.size());
+    for (int a = 0; a < nx; ++a) PX.set(a, xs[a], d.c.stream);
+    qkd_check(qkd_multi_dot(d.c.ws, t, dim, mm, P.at(0), nx, PX.data(), static_cast<double*>(dm.data()), d.c.stream),
+              "multi-dot");
+    const size_t rows = size_t(mm + 7) / 8 * 8;
+    cuda_check(cudaMemcpyAsync(dmh.data(), dm.data(), sizeof(double) * 16 * rows, cudaMemcpyDeviceToHost, d.c.stream),
+               "D2H");
+    d.c.sync();
+    std::vector<double> D(size_t(mm) * nx);
+    for (int i = 0; i < mm; ++i)
+      for (int a = 0; a < nx; ++a) D[size_t(i) * nx + a] = dmh[2 * (size_t(i) * kX + a)];
+    return D;
+  };
+  // X_a = sum_i c[i*nx + a] V_i (acc false) or X_a -= ... (acc true), i < mm
+  auto multi_update = [&](int mm, const std::vector<double>& c, const std::vector<void*>& xs, bool acc) {
+    const int nx = int(xs.size());
+    for (int a = 0; a < nx; ++a) PX.set(a, xs[a], d.c.stream);
+    cuda_check(cudaMemcpyAsync(cm.data(), c.data(), sizeof(double) * size_t(mm) * nx, cudaMemcpyHostToDevice,
+                               d.c.stream), "H2D");
+    qkd_check(qkd_multi_update(t, dim, mm, P.at(0), static_cast<const double*>(cm.data()), nx,
+                               const_cast<void* const*>(reinterpret_cast<const void* const*>(PX.data())), acc ? 1 : 0,
+                               d.c.stream), "multi-update");
+    d.c.sync();  // c is host memory reused by the caller
+  };
   std::vector<double> T;  // m x m, row major
   int m = 0, m_proj = 0;  // basis size; columns of T filled
   // Orthonormalise x against V[0..m) (two passes) and append it; false if
-  // it vanished (linearly dependent).
-  auto append = [&](DevVec&& x) -> bool {
-    double before = d.dot(x.data(), x.data()).real();
+  // it vanished (linearly dependent).  `before`: |x|^2 before any
+  // orthogonalisation (< 0: take it now).
+  auto append = [&](DevVec&& x, double before = -1.0) -> bool {
+    if (before < 0.0) before = d.dot(x.data(), x.data()).real();
     for (int pass = 0; pass < 2 && m > 0; ++pass) {
       d.update_mdot(0, nullptr, nullptr, P, m, x.data(), cd);
       d.mupdate(P, m, cd, x.data(), cd + 2 * (m + 1));
@@ -488,39 +522,60 @@ DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int bl
     qkd_check(qkd_random(t, dim, seed * 7919ull + uint64_t(a) + 1, 0, x.data(), d.c.stream), "random");
     append(std::move(x));
   }
+  for (auto& r : R) r = d.vec(false);
   std::vector<double> theta, Y;
   for (int it = 0; it < maxiter; ++it) {
     out.iterations = it + 1;
-    // new columns of T: T[i][j] = <v_i, H v_j> for the vectors added since
-    for (int j = m_proj; j < m; ++j) {
-      H.apply(t, V[j].data(), w.data());
-      ++out.applies;
-      d.update_mdot(0, nullptr, nullptr, P, j + 1, w.data(), cd);
-      const double* dots = d.c.fetch(cd, 2 * (j + 1));
-      std::vector<double> Tn(size_t(j + 1) * (j + 1), 0.0);
-      for (int r = 0; r < j; ++r)
-        for (int c = 0; c < j; ++c) Tn[size_t(r) * (j + 1) + c] = T[size_t(r) * j + c];
-      for (int i = 0; i <= j; ++i) {
-        Tn[size_t(i) * (j + 1) + j] = dots[2 * i];
-        Tn[size_t(j) * (j + 1) + i] = dots[2 * i];
+    // new columns of T: T[i][j] = <v_i, H v_j> for the vectors added since,
+    // H v_j formed into the residual buffers (free at this point) and
+    // projected onto the basis up to kX columns per pass
+    for (int j0 = m_proj; j0 < m;) {
+      const int cnt = std::min({kX, block, m - j0});
+      std::vector<void*> xs;
+      for (int b = 0; b < cnt; ++b) {
+        H.apply(t, V[j0 + b].data(), R[b].data());
+        ++out.applies;
+        xs.push_back(R[b].data());
+      }
+      const std::vector<double> D = multi_dot(j0 + cnt, xs);
+      const int mn = j0 + cnt;
+      std::vector<double> Tn(size_t(mn) * mn, 0.0);
+      for (int r = 0; r < j0; ++r)
+        for (int c = 0; c < j0; ++c) Tn[size_t(r) * mn + c] = T[size_t(r) * j0 + c];
+      for (int b = 0; b < cnt; ++b) {
+        const int j = j0 + b;
+        for (int i = 0; i <= j; ++i) {
+          Tn[size_t(i) * mn + j] = D[size_t(i) * cnt + b];
+          Tn[size_t(j) * mn + i] = D[size_t(i) * cnt + b];
+        }
       }
       T.swap(Tn);
+      j0 += cnt;
     }
     m_proj = m;
     jacobi_symmetric(T, m, theta, Y);
-    // Ritz vectors and residuals of the lowest nb pairs; the previous
-    // iteration's Ritz vectors move to Uprev (kept for the restart)
+    // Ritz vectors of the lowest nb pairs in one pass over the basis (kX at
+    // a time), then their residuals; the previous iteration's Ritz vectors
+    // move to Uprev (kept for the restart)
     const int nb = std::min(block, m);
-    std::vector<double> cz(2 * size_t(m));
     double worst = 0.0;
     out.residuals.assign(nb, 0.0);
     for (int a = 0; a < nb; ++a) std::swap(U[a], Uprev[a]);
+    auto ritz = [&](int a0, int a1) {  // U[a] = V y_a for a in [a0, a1)
+      for (int c0 = a0; c0 < a1; c0 += kX) {
+        const int cnt = std::min(kX, a1 - c0);
+        std::vector<double> c(size_t(m) * cnt);
+        std::vector<void*> xs;
+        for (int b = 0; b < cnt; ++b) {
+          if (!U[c0 + b].data()) U[c0 + b] = d.vec(false);
+          xs.push_back(U[c0 + b].data());
+          for (int i = 0; i < m; ++i) c[size_t(i) * cnt + b] = Y[size_t(i) * m + c0 + b];
+        }
+        multi_update(m, c, xs, false);
+      }
+    };
+    ritz(0, nb);
     for (int a = 0; a < nb; ++a) {
-      for (int i = 0; i < m; ++i) { cz[2 * i] = Y[size_t(i) * m + a]; cz[2 * i + 1] = 0.0; }
-      cuda_check(cudaMemcpyAsync(cd, cz.data(), sizeof(double) * 2 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
-      if (!U[a].data()) U[a] = d.vec(false);
-      if (!R[a].data()) R[a] = d.vec(false);
-      qkd_check(qkd_combine(t, dim, m, P.at(0), cd, t, U[a].data(), d.c.stream), "combine");
       H.apply(t, U[a].data(), R[a].data());
       ++out.applies;
       d.axpy({-theta[a], 0.0}, U[a].data(), R[a].data());
@@ -541,12 +596,7 @@ DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int bl
     }
     if (m + int(C.size()) > max_subspace) {  // restart from the lowest 2*block Ritz vectors
       const int keep = std::min(2 * block, m);
-      for (int a = nb; a < keep; ++a) {
-        for (int i = 0; i < m; ++i) { cz[2 * i] = Y[size_t(i) * m + a]; cz[2 * i + 1] = 0.0; }
-        cuda_check(cudaMemcpyAsync(cd, cz.data(), sizeof(double) * 2 * m, cudaMemcpyHostToDevice, d.c.stream), "H2D");
-        if (!U[a].data()) U[a] = d.vec(false);
-        qkd_check(qkd_combine(t, dim, m, P.at(0), cd, t, U[a].data(), d.c.stream), "combine");
-      }
+      ritz(nb, keep);
       std::vector<DevVec> NV;
       for (int a = 0; a < keep; ++a) { NV.push_back(std::move(U[a])); U[a] = DevVec(); }
       for (int a = 0; a < keep; ++a) { U[a] = std::move(V[a]); }  // recycle storage
@@ -571,9 +621,40 @@ DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int bl
         append(std::move(pv));
       }
     }
+    // the corrections against the basis as one block (classical Gram-Schmidt,
+    // twice: a projection pass and an update pass over the basis per kX
+    // corrections), then one by one against the corrections already taken
     int added = 0;
-    for (auto& c : C)
-      if (m < max_subspace && append(std::move(c))) ++added;
+    const int m_old = m;
+    for (size_t c0 = 0; c0 < C.size(); c0 += kX) {
+      const int cnt = int(std::min<size_t>(kX, C.size() - c0));
+      std::vector<void*> xs;
+      std::vector<double> before(cnt);
+      for (int b = 0; b < cnt; ++b) {
+        xs.push_back(C[c0 + b].data());
+        before[b] = d.dot(C[c0 + b].data(), C[c0 + b].data()).real();
+      }
+      for (int pass = 0; pass < 2; ++pass) {
+        const std::vector<double> D = multi_dot(m_old, xs);
+        multi_update(m_old, D, xs, true);
+      }
+      for (int b = 0; b < cnt; ++b) {
+        if (m >= max_subspace) break;
+        DevVec x = std::move(C[c0 + b]);
+        for (int pass = 0; pass < 2 && added > 0; ++pass) {  // against the corrections taken so far
+          d.update_mdot(0, nullptr, nullptr, PN, added, x.data(), cd);
+          d.mupdate(PN, added, cd, x.data(), cd + 2 * (added + 1));
+        }
+        const double nn = d.dot(x.data(), x.data()).real();
+        if (!(nn > 1e-20 * std::max(before[b], 1e-300)) || nn == 0.0) continue;
+        d.scal(1.0 / std::sqrt(nn), x.data());
+        P.set(m, x.data(), d.c.stream);
+        PN.set(added, x.data(), d.c.stream);
+        V.push_back(std::move(x));
+        ++m;
+        ++added;
+      }
+    }
     if (added == 0) break;  // no new direction: stagnated
   }
   if (evecs_out) {

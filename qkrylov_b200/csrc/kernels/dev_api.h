@@ -98,6 +98,16 @@ int qkd_tune_rows(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X,
 int qkd_tune_rows_acc(qk_plan* p, qk_workspace* w, qk_dtype t, int R, const void* X, void* Y, const double* g,
                       cudaStream_t s, int* chosen);
 /* The tuned lanes per row for (t, R), 0 before tuning. */
+/* Block Davidson forms (t = QK_F64 or QK_F32; V, X: device arrays of device
+ * pointers; nx <= 8).  qkd_multi_dot: out[2*(i*8 + a)] = <V_i, X_a> for
+ * i < m, a < nx (out: 16 * (m rounded up to 8) device doubles; FP64,
+ * deterministic).
+ * qkd_multi_update: X_a = sum_i c[i*nx + a] V_i (accumulate = 0) or
+ * X_a -= sum_i c[i*nx + a] V_i (accumulate = 1); c: m*nx device doubles. */
+int qkd_multi_dot(qk_workspace* w, qk_dtype t, size_t n, int m, const void* const* V, int nx, const void* const* X,
+                  double* out, cudaStream_t s);
+int qkd_multi_update(qk_dtype t, size_t n, int m, const void* const* V, const double* c, int nx, void* const* X,
+                     int accumulate, cudaStream_t s);
 int qkd_rows_shape(const qk_plan* p, qk_dtype t, int R);
 /* The tuner's fastest launch (ms) for lanes per row 32, 16, 8 (rows) x tile
  * code 0, 1, 2 (columns), row-major; 0 where a shape was not timed. */

@@ -381,12 +381,201 @@ k_mupdate(size_t n, int k, const void* const* __restrict__ V, const double* __re
   }
 }
 
+// Many-against-many forms for the block Davidson (real vectors): the
+// projections of nx <= 8 vectors X_a onto a tile of up to 8 basis vectors
+// V_i in one pass (64 FP64 accumulators per thread), and X_a = (or -=) the
+// combinations sum_i c[i][a] V_i of m basis vectors in one pass.  Elements
+// are read in pairs (8- or 16-byte loads); a pointer that is not aligned to
+// a pair sends the launch through the single-element loop.
+constexpr int kMX = 8;  // X vectors per launch
+constexpr int kMV = 8;  // V vectors per multi-dot launch
+
+template <int DT> struct Pair;
+template <> struct Pair<QK_F64> {
+  using V = double2;
+  __device__ static void un(const V& v, double& a, double& b) { a = v.x; b = v.y; }
+  __device__ static V pk(double a, double b) { return make_double2(a, b); }
+};
+template <> struct Pair<QK_F32> {
+  using V = float2;
+  __device__ static void un(const V& v, double& a, double& b) { a = v.x; b = v.y; }
+  __device__ static V pk(double a, double b) { return make_float2(float(a), float(b)); }
+};
+
+template <int DT>
+__global__ void __launch_bounds__(kThreads, 1)
+k_multi_dot(size_t n, int mv, const void* const* __restrict__ V, int nx, const void* const* __restrict__ X,
+            double* partials, unsigned* ticket, double* out) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  using P = Pair<DT>;
+  __shared__ const void* sV[kMV];
+  __shared__ const void* sX[kMX];
+  __shared__ double red[kThreads / 32][kMV * kMX];
+  // tiles shorter than kMV repeat their last vector, and fewer than kMX
+  // X vectors repeat the last one: the extra outputs are computed and not used
+  bool ok = true;
+  if (threadIdx.x < kMV) {
+    sV[threadIdx.x] = V[threadIdx.x < mv ? threadIdx.x : mv - 1];
+    ok = (reinterpret_cast<uintptr_t>(sV[threadIdx.x]) % sizeof(typename P::V)) == 0;
+  } else if (threadIdx.x >= 32 && threadIdx.x < 32 + kMX) {
+    const int a = threadIdx.x - 32;
+    sX[a] = X[a < nx ? a : nx - 1];
+    ok = (reinterpret_cast<uintptr_t>(sX[a]) % sizeof(typename P::V)) == 0;
+  }
+  ok = __syncthreads_and(ok) != 0;
+  double acc[kMV][kMX];
+  #pragma unroll
+  for (int i = 0; i < kMV; ++i)
+    #pragma unroll
+    for (int a = 0; a < kMX; ++a) acc[i][a] = 0.0;
+  const size_t np = ok ? n / 2 : 0;  // whole pairs
+  for (size_t q = blockIdx.x * size_t(kThreads) + threadIdx.x; q < np; q += size_t(gridDim.x) * kThreads) {
+    double x0[kMX], x1[kMX];
+    #pragma unroll
+    for (int a = 0; a < kMX; ++a) P::un(__ldg(reinterpret_cast<const typename P::V*>(sX[a]) + q), x0[a], x1[a]);
+    #pragma unroll
+    for (int i = 0; i < kMV; ++i) {
+      double v0, v1;
+      P::un(__ldg(reinterpret_cast<const typename P::V*>(sV[i]) + q), v0, v1);
+      #pragma unroll
+      for (int a = 0; a < kMX; ++a) acc[i][a] += v0 * x0[a] + v1 * x1[a];
+    }
+  }
+  for (size_t e = 2 * np + blockIdx.x * size_t(kThreads) + threadIdx.x; e < n; e += size_t(gridDim.x) * kThreads) {
+    double xe[kMX];
+    #pragma unroll
+    for (int a = 0; a < kMX; ++a) { R r, m; T::ld(sX[a], e, r, m); xe[a] = double(r); }
+    #pragma unroll
+    for (int i = 0; i < kMV; ++i) {
+      R r, m;
+      T::ld(sV[i], e, r, m);
+      #pragma unroll
+      for (int a = 0; a < kMX; ++a) acc[i][a] += double(r) * xe[a];
+    }
+  }
+  // block sums in a fixed order: warps, then warps' partials in warp order
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  #pragma unroll
+  for (int i = 0; i < kMV; ++i)
+    #pragma unroll
+    for (int a = 0; a < kMX; ++a) {
+      const double v = warp_sum(acc[i][a]);
+      if (lane == 0) red[warp][i * kMX + a] = v;
+    }
+  __syncthreads();
+  const int G = gridDim.x;
+  for (int j = threadIdx.x; j < kMV * kMX; j += kThreads) {
+    double sum = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) sum += red[w][j];
+    partials[(size_t(j) * G + blockIdx.x) * 2] = sum;
+    partials[(size_t(j) * G + blockIdx.x) * 2 + 1] = 0.0;
+  }
+  grid_finish(partials, ticket, kMV * kMX, out);
+}
+
+// X_a = sum_i c[i*nx + a] V_i (acc = 0) or X_a -= sum_i c[i*nx + a] V_i
+// (acc = 1), a < nx, i < m; FP64 accumulation.
+template <int DT>
+__global__ void __launch_bounds__(kThreads)
+k_multi_update(size_t n, int m, const void* const* __restrict__ V, const double* __restrict__ c, int nx,
+               void* const* __restrict__ X, int acc) {
+  using T = VT<DT>;
+  using R = typename T::R;
+  using P = Pair<DT>;
+  extern __shared__ double sm[];  // m*nx coefficients, then m + nx pointers
+  double* sc = sm;
+  const void** sV = reinterpret_cast<const void**>(sc + size_t(m) * nx);
+  void** sX = reinterpret_cast<void**>(sc + size_t(m) * nx + m);
+  bool ok = true;
+  for (int j = threadIdx.x; j < m * nx; j += kThreads) sc[j] = c[j];
+  for (int j = threadIdx.x; j < m; j += kThreads) {
+    sV[j] = V[j];
+    ok = ok && (reinterpret_cast<uintptr_t>(sV[j]) % sizeof(typename P::V)) == 0;
+  }
+  for (int a = threadIdx.x; a < kMX; a += kThreads) {
+    sX[a] = X[a < nx ? a : nx - 1];
+    ok = ok && (reinterpret_cast<uintptr_t>(sX[a]) % sizeof(typename P::V)) == 0;
+  }
+  ok = __syncthreads_and(ok) != 0;
+  const size_t np = ok ? n / 2 : 0;
+  for (size_t q = blockIdx.x * size_t(kThreads) + threadIdx.x; q < np; q += size_t(gridDim.x) * kThreads) {
+    double x0[kMX], x1[kMX];
+    #pragma unroll
+    for (int a = 0; a < kMX; ++a) {
+      x0[a] = 0.0; x1[a] = 0.0;
+      if (acc && a < nx) P::un(reinterpret_cast<const typename P::V*>(sX[a])[q], x0[a], x1[a]);
+    }
+    #pragma unroll 4
+    for (int i = 0; i < m; ++i) {
+      double v0, v1;
+      P::un(__ldg(reinterpret_cast<const typename P::V*>(sV[i]) + q), v0, v1);
+      const double* ci = sc + size_t(i) * nx;
+      #pragma unroll
+      for (int a = 0; a < kMX; ++a)
+        if (a < nx) {
+          const double w = acc ? -ci[a] : ci[a];
+          x0[a] += w * v0;
+          x1[a] += w * v1;
+        }
+    }
+    #pragma unroll
+    for (int a = 0; a < kMX; ++a)
+      if (a < nx) reinterpret_cast<typename P::V*>(sX[a])[q] = P::pk(x0[a], x1[a]);
+  }
+  for (size_t e = 2 * np + blockIdx.x * size_t(kThreads) + threadIdx.x; e < n; e += size_t(gridDim.x) * kThreads) {
+    double xe[kMX];
+    #pragma unroll
+    for (int a = 0; a < kMX; ++a) {
+      xe[a] = 0.0;
+      if (acc && a < nx) { R r, mm; T::ld_plain(sX[a], e, r, mm); xe[a] = double(r); }
+    }
+    for (int i = 0; i < m; ++i) {
+      R r, mm;
+      T::ld(sV[i], e, r, mm);
+      const double* ci = sc + size_t(i) * nx;
+      #pragma unroll
+      for (int a = 0; a < kMX; ++a)
+        if (a < nx) xe[a] += (acc ? -ci[a] : ci[a]) * double(r);
+    }
+    #pragma unroll
+    for (int a = 0; a < kMX; ++a)
+      if (a < nx) T::st(sX[a], e, R(xe[a]), R(0));
+  }
+}
+
 }  // namespace
 }  // namespace qkd
 
 using namespace qkd;
 
 extern "C" {
+
+int qkd_multi_dot(qk_workspace* w, qk_dtype t, size_t n, int m, const void* const* V, int nx, const void* const* X,
+                  double* out, cudaStream_t s) {
+  if (!w || !V || !X || !out || m <= 0 || nx <= 0 || nx > kMX || (t != QK_F64 && t != QK_F32)) return QKD_EINVAL;
+  const unsigned G = std::max(1u, std::min(unsigned(sm_count(current_device())) * 2, unsigned(kMaxG)));
+  for (int i0 = 0; i0 < m; i0 += kMV) {
+    const int mv = std::min(kMV, m - i0);
+    double* o = out + size_t(2) * i0 * kMX;
+    if (t == QK_F64) k_multi_dot<QK_F64><<<G, kThreads, 0, s>>>(n, mv, V + i0, nx, X, w->partials, w->ticket, o);
+    else k_multi_dot<QK_F32><<<G, kThreads, 0, s>>>(n, mv, V + i0, nx, X, w->partials, w->ticket, o);
+    QKD_LAUNCH_CHECK();
+  }
+  return QKD_OK;
+}
+
+int qkd_multi_update(qk_dtype t, size_t n, int m, const void* const* V, const double* c, int nx, void* const* X,
+                     int accumulate, cudaStream_t s) {
+  if (!V || !c || !X || m <= 0 || m > kMaxK || nx <= 0 || nx > kMX || (t != QK_F64 && t != QK_F32)) return QKD_EINVAL;
+  const size_t smem = size_t(m) * nx * sizeof(double) + size_t(m + kMX) * sizeof(void*);
+  if (smem > 48 * 1024) return QKD_EINVAL;
+  const unsigned G = stream_grid(n, 2);
+  if (t == QK_F64) k_multi_update<QK_F64><<<G, kThreads, smem, s>>>(n, m, V, c, nx, X, accumulate ? 1 : 0);
+  else k_multi_update<QK_F32><<<G, kThreads, smem, s>>>(n, m, V, c, nx, X, accumulate ? 1 : 0);
+  QKD_LAUNCH_CHECK();
+  return QKD_OK;
+}
 
 uint64_t qkd_launch_count(void) { return g_launches.load(); }
 
