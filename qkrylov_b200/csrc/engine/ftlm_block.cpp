@@ -14,9 +14,11 @@
 // w_i = n_r z_0i^2 exp(-beta (e_i - E_min)); Z = exp(-beta E_min) sum w / R,
 // U = sum e w / sum w, Cv = beta^2 (sum e^2 w / sum w - U^2).  The shift by
 // the lowest Ritz value E_min keeps every exponent <= 0; log Z is reported.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <stdexcept>
+#include <thread>
 
 #include "dense.hpp"
 #include "solvers.hpp"
@@ -28,21 +30,39 @@ double wall() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Runs f(i) for i in [0, n) on up to the host's hardware threads, each
+// thread a contiguous range (every f(i) is independent and computed exactly
+// as in a serial loop, so the results do not depend on the thread count).
+template <class F>
+void parallel_range(int n, F f) {
+  const int nth = std::max(1, std::min<int>(n, int(std::thread::hardware_concurrency())));
+  if (nth <= 1) { for (int i = 0; i < n; ++i) f(i); return; }
+  std::vector<std::thread> th;
+  for (int k = 0; k < nth; ++k)
+    th.emplace_back([&, k] { for (int i = n * k / nth; i < n * (k + 1) / nth; ++i) f(i); });
+  for (auto& t : th) t.join();
+}
+
 void thermo(FtlmBlockOut& out, const std::vector<double>& temps) {
   const int R = out.R;
   std::vector<std::vector<double>> ev(R), fc(R);
-  double emin = 1e300;
-  for (int r = 0; r < R; ++r) {
+  // the R tridiagonals' Ritz values and first components (one QL solve
+  // each), then every temperature's sums over all Ritz pairs: both on the
+  // host's cores (64 solves of 100 steps and 200 x 6,400 weights would
+  // otherwise be ~45 ms of host time beside ~0.7 s on the GPU)
+  parallel_range(R, [&](int r) {
     const int m = out.len[r];
     std::vector<double> a(out.alphas.begin() + size_t(r) * out.M, out.alphas.begin() + size_t(r) * out.M + m);
     std::vector<double> b(out.betas.begin() + size_t(r) * out.M, out.betas.begin() + size_t(r) * out.M + std::max(m - 1, 0));
     tridiag_first<double>(a, b, ev[r], fc[r]);
+  });
+  double emin = 1e300;
+  for (int r = 0; r < R; ++r)
     for (double e : ev[r]) emin = std::min(emin, e);
-  }
   out.e_min = emin;
   const size_t nt = temps.size();
   out.logZ.assign(nt, 0.0); out.U.assign(nt, 0.0); out.Cv.assign(nt, 0.0);
-  for (size_t q = 0; q < nt; ++q) {
+  parallel_range(int(nt), [&](int q) {
     const double beta = 1.0 / temps[q];
     double z = 0.0, e1 = 0.0, e2 = 0.0;
     for (int r = 0; r < R; ++r)
@@ -54,7 +74,7 @@ void thermo(FtlmBlockOut& out, const std::vector<double>& temps) {
     out.logZ[q] = std::log(z / R) - beta * emin;
     out.U[q] = u;
     out.Cv[q] = beta * beta * (e2 / z - u * u);
-  }
+  });
 }
 }  // namespace
 
