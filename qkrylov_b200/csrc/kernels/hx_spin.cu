@@ -664,7 +664,7 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
   // to tile_part and are summed in tile order, so they do not depend on
   // which CTA took which tile (grid-stride: per CTA, in CTA order).
   __shared__ uint32_t s_chunk[2];
-  __shared__ double red[2 * 256];
+  __shared__ double red[2 * (256 / 32) * RV];  // per-warp column sums (also the grid-stride form's scratch)
   int die = 0;
   if (wq) {
     uint32_t sid;
@@ -807,29 +807,43 @@ k_hx_rows_block(const SpinPlan* __restrict__ pp, const void* __restrict__ X, voi
       #pragma unroll
       for (int v = 0; v < VPL; ++v) {
         T::st(yv.v, v, ar[v], ai[v]);
-        dr[v] += double(x0r[v]) * double(ar[v]) + double(x0i[v]) * double(ai[v]);
-        di[v] += double(x0r[v]) * double(ai[v]) - double(x0i[v]) * double(ar[v]);
+        if (T::cplx) {
+          dr[v] += double(x0r[v]) * double(ar[v]) + double(x0i[v]) * double(ai[v]);
+          di[v] += double(x0r[v]) * double(ai[v]) - double(x0i[v]) * double(ar[v]);
+        } else {
+          dr[v] += double(x0r[v]) * double(ar[v]);
+        }
       }
       *reinterpret_cast<Pack*>(Ye + size_t(row) * RV + l * VPL) = yv;
     }
    }
-    // queues: this tile's column dots, in thread order
+    // queues: this tile's column dots in a fixed order (the rows a warp
+    // holds by shuffles, then the warps in order), two barriers per tile
     if (tile_part) {
-      for (int v = 0; v < VPL; ++v) {
-        __syncthreads();
-        red[2 * threadIdx.x] = dr[v];
-        red[2 * threadIdx.x + 1] = di[v];
-        __syncthreads();
-        if (threadIdx.x < LPR) {
-          double sr = 0.0, si = 0.0;
-          for (int t = threadIdx.x; t < 256; t += LPR) { sr += red[2 * t]; si += red[2 * t + 1]; }
-          const int c = threadIdx.x * VPL + v;
-          tile_part[(size_t(c) * nchunks + chunk) * 2] = sr;
-          tile_part[(size_t(c) * nchunks + chunk) * 2 + 1] = si;
+      #pragma unroll
+      for (int v = 0; v < VPL; ++v)
+        #pragma unroll
+        for (int o = LPR; o < 32; o <<= 1) {
+          dr[v] += __shfl_xor_sync(0xffffffffu, dr[v], o);
+          if (T::cplx) di[v] += __shfl_xor_sync(0xffffffffu, di[v], o);
         }
-        dr[v] = 0.0;
-        di[v] = 0.0;
+      __syncthreads();  // the previous tile's sums have been read
+      if (lane < LPR) {
+        #pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          red[(warp * RV + l * VPL + v) * 2] = dr[v];
+          red[(warp * RV + l * VPL + v) * 2 + 1] = T::cplx ? di[v] : 0.0;
+        }
       }
+      __syncthreads();
+      for (int c = threadIdx.x; c < RV; c += 256) {
+        double sr = 0.0, si = 0.0;
+        for (int w = 0; w < 256 / 32; ++w) { sr += red[(w * RV + c) * 2]; si += red[(w * RV + c) * 2 + 1]; }
+        tile_part[(size_t(c) * nchunks + chunk) * 2] = sr;
+        tile_part[(size_t(c) * nchunks + chunk) * 2 + 1] = si;
+      }
+      #pragma unroll
+      for (int v = 0; v < VPL; ++v) { dr[v] = 0.0; di[v] = 0.0; }
     }
     uint32_t cn = chunk + gridDim.x;
     if (wq) {
