@@ -34,8 +34,10 @@ int qkrylov_b200_device_count(void);
  * block, x of the block staged in shared memory, per-row class tables)
  * wherever the compiled operator has their tables, with per-die work queues
  * on a two-die GPU; 1: the generic kernel everywhere; 2: as 0 with the
- * blocks handed out in one grid-stride order (no per-die queues).  For
- * comparisons; process-wide.  Other values: QKRYLOV_ERROR_INVALID_ARG. */
+ * blocks handed out in one grid-stride order (no per-die queues); 3: as 0
+ * with Hubbard-type operators on the two-part row kernel instead of their
+ * spin-product path.  For comparisons; process-wide.  Other values:
+ * QKRYLOV_ERROR_INVALID_ARG. */
 int qkrylov_b200_set_kernel_policy(int policy);
 /* Dies of the current device as the row kernels' topology probe measured
  * them (2 on a B200, 1 where the probe saw one) and the SMs of each (first
@@ -84,7 +86,10 @@ uint64_t qkrylov_hamiltonian_device_bytes(qkrylov_hamiltonian_h h);
 /* The H.x kernel of this handle: 1 the two-site exchange kernel (spin
  * models in a single-charge sector), 2 the two-part kernel (operators whose
  * terms factorise over the sector split: Hubbard, t-J, fermion hops with
- * Jordan-Wigner signs), 0 the generic term-table kernel. */
+ * Jordan-Wigner signs), 3 the spin-product path (Hubbard-type operators with
+ * N_up and N_dn conserved: T_up x 1 + 1 x T_dn + D in the (up, down) order,
+ * the vector permuted at the boundary; block applies stay on the two-part
+ * kernel), 0 the generic term-table kernel. */
 int qkrylov_hamiltonian_kernel(qkrylov_hamiltonian_h h);
 /* The CUDA stream (cudaStream_t) the library uses on the handle's device. */
 void* qkrylov_hamiltonian_stream(qkrylov_hamiltonian_h h);

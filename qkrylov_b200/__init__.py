@@ -444,10 +444,13 @@ class MatrixFreeHamiltonian:
     @property
     def kernel(self) -> str:
         """The H.x kernel this operator uses: 'spin-exchange' (two-site
-        exchange in a single-charge sector), 'two-part' (any operator whose
-        terms factorise over the sector split: Hubbard, t-J, fermions) or
-        'generic' (term-table walk)."""
-        return {1: "spin-exchange", 2: "two-part"}.get(int(lib().qkrylov_hamiltonian_kernel(self._h)), "generic")
+        exchange in a single-charge sector), 'spin-product' (Hubbard-type
+        operators with N_up and N_dn conserved: hops of one species applied
+        as T_up x 1 + 1 x T_dn in the (up, down) order), 'two-part' (any
+        operator whose terms factorise over the sector split: Hubbard, t-J,
+        fermions) or 'generic' (term-table walk)."""
+        return {1: "spin-exchange", 2: "two-part", 3: "spin-product"}.get(
+            int(lib().qkrylov_hamiltonian_kernel(self._h)), "generic")
 
     @property
     def stream(self) -> int:
@@ -991,9 +994,10 @@ def die_count():
 def set_kernel_policy(policy: str):
     """'auto' (the specialised row kernels where the operator has their
     tables, per-die work queues on a two-die GPU), 'generic' (the term-walk
-    kernel only) or 'no-die-queues' (auto with one grid-stride order), for
-    comparisons."""
-    codes = {"auto": 0, "generic": 1, "no-die-queues": 2}
+    kernel only), 'no-die-queues' (auto with one grid-stride order) or
+    'no-spin-product' (auto with Hubbard-type operators on the two-part row
+    kernel), for comparisons."""
+    codes = {"auto": 0, "generic": 1, "no-die-queues": 2, "no-spin-product": 3}
     _check(lib().qkrylov_b200_set_kernel_policy(codes[policy]), "set_kernel_policy")
 
 

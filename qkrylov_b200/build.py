@@ -32,7 +32,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
 CXX_FLAGS = ["-O3", "-std=c++20", "-fPIC", "-Wall", "-Wno-unused-function"] + INCLUDES
 
 CU_SOURCES = ["kernels/vec.cu", "kernels/hx.cu", "kernels/krylov.cu", "kernels/block.cu", "kernels/mlp.cu", "kernels/mlp_tc.cu", "kernels/noalloc.cu",
-              "kernels/hx_spin.cu", "kernels/topology.cu", "kernels/spectral.cu"]
+              "kernels/hx_spin.cu", "kernels/hx_pair.cu", "kernels/topology.cu", "kernels/spectral.cu"]
 ENGINE_SOURCES = ["engine/sector.cpp", "engine/compile.cpp", "engine/operator.cpp", "engine/runtime.cpp",
                   "engine/solvers.cpp", "engine/npy.cpp", "engine/ftlm_block.cpp", "engine/warmstart.cpp", "engine/sweep.cpp"]
 API_SOURCES = ["api/objects.cpp", "api/solvers_api.cpp"]  # compiled for fp64 and fp32

@@ -42,8 +42,9 @@ int qkrylov_b200_device_count(void) {
 
 int qkrylov_b200_set_kernel_policy(int policy) {
   // 0 auto (the specialised kernels where the operator has their tables),
-  // 1 the generic term-walk kernel only, 2 auto without per-die work queues
-  if (policy < 0 || policy > 2) return QKRYLOV_ERROR_INVALID_ARG;
+  // 1 the generic term-walk kernel only, 2 auto without per-die work queues,
+  // 3 auto without the spin-product path of Hubbard-type operators
+  if (policy < 0 || policy > 3) return QKRYLOV_ERROR_INVALID_ARG;
   qkd_set_kernel_policy(policy);
   return QKRYLOV_SUCCESS;
 }

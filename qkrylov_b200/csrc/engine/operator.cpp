@@ -23,6 +23,7 @@ Operator::Operator(Family site_family, std::shared_ptr<const SectorTable> basis,
   d.ngroups = uint32_t(op_.groups.size());
   d.has_diag = op_.has_diag;
   d.all_real = op_.all_real;
+  d.pair_sites = is_pair(basis_->family) ? 1 : 0;
   qkd_check(qkd_plan_create(&d, device_, &plan_), "operator upload");
 }
 

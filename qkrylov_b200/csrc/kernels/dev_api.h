@@ -43,6 +43,7 @@ typedef struct {
   const qk_term_t* terms; uint32_t nterms;
   const qk_group_t* groups; uint32_t ngroups;
   int has_diag, all_real;
+  int pair_sites;  /* 1: two bits per site, up-spin at the even bit (Hubbard, t-J) */
 } qk_plan_desc;
 
 typedef struct qk_plan qk_plan;
@@ -56,7 +57,8 @@ size_t qkd_plan_device_bytes(const qk_plan* p);
 
 /* 0: use specialised kernels where the operator qualifies (default);
  * 1: generic kernel only; 2: as 0 without the per-die work queues of the
- * row kernel (for comparisons). */
+ * row kernel; 3: as 0 without the spin-product path of Hubbard-type
+ * operators (for comparisons). */
 int qkd_set_kernel_policy(int policy);
 /* Dies of the current device as measured by the row kernels' topology probe
  * (2 or 1) and the SMs on each. */

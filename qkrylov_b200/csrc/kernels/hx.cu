@@ -19,6 +19,12 @@ namespace qkd {
 struct SpinHandle;
 SpinHandle* spin_plan_create(const qk_plan_desc* d, size_t* dev_bytes);
 SpinHandle* gen_plan_create(const qk_plan_desc* d, size_t* dev_bytes);
+struct PairHandle;
+PairHandle* pair_plan_create(const qk_plan_desc* d, const uint64_t* A_dev, const uint32_t* B_dev,
+                             const double* diag_ref, size_t* dev_bytes);
+void pair_plan_destroy(PairHandle* h);
+int pair_apply(const PairHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,
+               double* dot_out);
 bool spin_plan_is_gen(const SpinHandle* h);
 int spin_plan_set_diag(SpinHandle* h, const double* diag);
 int spin_apply_block(const SpinHandle* h, qk_dtype t, int R, int lpr, const void* X, void* Y, double* dots,
@@ -33,9 +39,11 @@ int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStre
 }  // namespace qkd
 
 static int g_kernel_policy = 0;  // 0: specialised kernels where eligible, 1: generic only
+static bool g_pair_path = true;  // the spin-product path of Hubbard-type operators
 
 struct qk_plan {
   qkd::SpinHandle* spin = nullptr;
+  qkd::PairHandle* pair = nullptr;  // spin-product path (Hubbard-type operators), or null
   int device;
   int nbits, L;
   uint64_t dim, lmask;
@@ -477,24 +485,29 @@ int qkd_plan_create(const qk_plan_desc* d, int device, qk_plan** out) {
     qkd::spin_plan_destroy(p->spin);
     p->spin = nullptr;
   }
+  if (d->pair_sites && p->diag_re) p->pair = qkd::pair_plan_create(d, p->A, p->B, p->diag_re, &p->bytes);
   *out = p;
   return QKD_OK;
 }
 
 int qkd_set_kernel_policy(int policy) {
-  if (policy < 0 || policy > 2) return QKD_EINVAL;
+  if (policy < 0 || policy > 3) return QKD_EINVAL;
   g_kernel_policy = policy == 1 ? 1 : 0;
   qkd::spin_set_die_queues(policy != 2);
+  g_pair_path = policy != 3;
   return QKD_OK;
 }
 
 int qkd_plan_kernel(const qk_plan* p) {
-  if (!p || !p->spin || g_kernel_policy != 0) return 0;
+  if (!p || g_kernel_policy != 0) return 0;
+  if (p->pair && g_pair_path) return 3;
+  if (!p->spin) return 0;
   return qkd::spin_plan_is_gen(p->spin) ? 2 : 1;
 }
 
 int qkd_plan_destroy(qk_plan* p) {
   if (!p) return QKD_OK;
+  qkd::pair_plan_destroy(p->pair);
   qkd::spin_plan_destroy(p->spin);
   cudaFree(p->diag_re);
   cudaFree(p->A); cudaFree(p->B); cudaFree(p->llist);
@@ -511,6 +524,10 @@ int qkd_apply(const qk_plan* p, qk_dtype t, const void* x, void* y, cudaStream_t
   if (!p || !x || !y || x == y) return QKD_EINVAL;
   if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
   if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
+  if (p->pair && g_kernel_policy == 0 && g_pair_path) {
+    const int rc = qkd::pair_apply(p->pair, t, x, y, s, nullptr, nullptr);
+    if (rc != QKD_EINVAL) return rc;
+  }
   if (p->spin && g_kernel_policy == 0) return qkd::spin_apply(p->spin, t, x, y, s, nullptr, nullptr);
   if (p->all_real) { QKD_DISPATCH(t, return launch_apply<DT, false>(p, x, y, s, nullptr, nullptr)); }
   QKD_DISPATCH(t, return launch_apply<DT, true>(p, x, y, s, nullptr, nullptr));
@@ -539,6 +556,10 @@ int qkd_apply_dot(const qk_plan* p, qk_workspace* w, qk_dtype t, const void* x, 
   if (!p || !w || !x || !y || x == y || !dot_out) return QKD_EINVAL;
   if (p->dim == 0 || p->ntiles == 0) return QKD_OK;
   if (!qk_dtype_complex(t) && !p->all_real) return QKD_EINVAL;
+  if (p->pair && g_kernel_policy == 0 && g_pair_path) {
+    const int rc = qkd::pair_apply(p->pair, t, x, y, s, w, dot_out);
+    if (rc != QKD_EINVAL) return rc;
+  }
   if (p->spin && g_kernel_policy == 0) return qkd::spin_apply(p->spin, t, x, y, s, w, dot_out);
   if (p->all_real) { QKD_DISPATCH(t, return launch_apply<DT, false>(p, x, y, s, w, dot_out)); }
   QKD_DISPATCH(t, return launch_apply<DT, true>(p, x, y, s, w, dot_out));

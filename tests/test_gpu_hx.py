@@ -195,10 +195,14 @@ def test_multi_dot_device():
 ])
 def test_two_part_kernel_matches_generic(kind, N, sec, terms):
     H = ham(kind, N, sec, terms)
-    assert H.kernel == "two-part"
     rng = np.random.default_rng(3)
     x = rng.standard_normal(H.dimension) + 1j * rng.standard_normal(H.dimension)
-    y = H.apply(x)
+    qk.set_kernel_policy("no-spin-product")  # Hubbard operators would take the spin-product path
+    try:
+        assert H.kernel == "two-part"
+        y = H.apply(x)
+    finally:
+        qk.set_kernel_policy("auto")
     qk.set_kernel_policy("generic")
     try:
         yg = H.apply(x)
@@ -247,3 +251,46 @@ def test_per_die_work_queues_give_identical_results():
         qk.set_kernel_policy("auto")
     assert np.array_equal(rs[0].U, rs[1].U)
     assert np.allclose(rs[0].U, rs[2].U, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("N,nup,ndn,lat", [(9, 4, 5, (3, 3)), (16, 2, 3, (4, 4)), (8, 3, 2, (4, 2))])
+def test_spin_product_path_matches_two_part_and_oracle(N, nup, ndn, lat):
+    """Hubbard operators with N_up and N_dn conserved apply as
+    T_up x 1 + 1 x T_dn + D in the (up, down) order (signs S(u, d) at the
+    boundary): against the two-part row kernel and the CPU oracle for every
+    vector type, and through the fused dot of the solvers (Lanczos energy)."""
+    sec = dict(use_nup=1, nup=nup, use_ndn=1, ndn=ndn)
+    terms = O.hubbard_square(*lat, 1.0, 4.0)
+    H = ham("hubbard", N, sec, terms)
+    if H.kernel != "spin-product":
+        pytest.skip(f"operator runs on {H.kernel}")
+    ref = O.port().hamiltonian("hubbard", N, sec, terms)
+    rng = np.random.default_rng(N + nup)
+    xh = rng.standard_normal(H.dimension) + 1j * rng.standard_normal(H.dimension)
+    yo = ref.apply(xh)
+    assert rel(H.apply(xh), yo) < 1e-13
+    H32 = ham("hubbard", N, sec, terms, dtype=np.float32)
+    assert rel(H32.apply(xh.astype(np.complex64)).astype(np.complex128), yo) < 2e-6
+    for code, tdt, tol in [(qk.DTYPE_F64, torch.float64, 1e-13), (qk.DTYPE_C128, torch.complex128, 1e-13),
+                           (qk.DTYPE_F32, torch.float32, 1e-5), (qk.DTYPE_C64, torch.complex64, 1e-5)]:
+        x = torch.randn(H.dimension, dtype=tdt, device="cuda", generator=torch.Generator("cuda").manual_seed(N))
+        ys = []
+        try:
+            for pol in ("auto", "no-spin-product"):
+                qk.set_kernel_policy(pol)
+                y = torch.full_like(x, float("nan"))
+                torch.cuda.synchronize()
+                H.apply_device(x.data_ptr(), y.data_ptr(), code)
+                torch.cuda.synchronize()
+                ys.append(y.to(torch.complex128).cpu().numpy())
+        finally:
+            qk.set_kernel_policy("auto")
+        assert rel(ys[0], ys[1]) < tol, (code, rel(ys[0], ys[1]))
+    es = []
+    try:
+        for pol in ("auto", "no-spin-product"):
+            qk.set_kernel_policy(pol)
+            es.append(qk.lanczos_fp64(H, seed=4, tol=1e-12).energy)
+    finally:
+        qk.set_kernel_policy("auto")
+    assert abs(es[0] - es[1]) < 1e-11 * abs(es[1])
