@@ -53,6 +53,7 @@ struct PairPlan {
 namespace {
 
 constexpr int kPT = 256;  // threads per CTA; k_pair_up takes row slabs of 2 * kPT elements
+constexpr int kDT = 1024; // k_pair_dn: one staged row shared by 32 warps (two CTAs per SM)
 
 __device__ __forceinline__ uint32_t spread16(uint32_t x) {  // bit i -> bit 2i (16 -> 32 bits)
   x &= 0xFFFFu;
@@ -148,7 +149,7 @@ __global__ void __launch_bounds__(kPT) k_pair_up(const PairPlan* __restrict__ pp
 // reference-order slot with the sign S.  DOT: <x, y> summed per CTA in a
 // fixed order, then over CTAs (deterministic for a given grid).
 template <int DT, bool DOT>
-__global__ void __launch_bounds__(kPT) k_pair_dn(const PairPlan* __restrict__ pp, const void* __restrict__ xp,
+__global__ void __launch_bounds__(kDT) k_pair_dn(const PairPlan* __restrict__ pp, const void* __restrict__ xp,
                                                  const void* __restrict__ yp, void* __restrict__ y,
                                                  double* partials, unsigned* ticket, double* dot_out) {
   using T = VT<DT>;
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(kPT) k_pair_dn(const PairPlan* __restrict__ pp
   using E = typename T::E;
   extern __shared__ __align__(16) unsigned char smraw[];
   E* xs = reinterpret_cast<E*>(smraw);
-  __shared__ double s_red[2 * (kPT / 32)];
+  __shared__ double s_red[2 * (kDT / 32)];
   const PairPlan& p = *pp;
   double dr = 0.0, di = 0.0;
   const bool packed = p.dn_ent != nullptr;
@@ -164,10 +165,10 @@ __global__ void __launch_bounds__(kPT) k_pair_dn(const PairPlan* __restrict__ pp
   for (uint32_t iu = blockIdx.x; iu < p.Du; iu += gridDim.x) {
     const uint64_t rb = uint64_t(iu) * p.Dd;
     __syncthreads();  // the previous row is finished with the staging
-    for (uint32_t c = threadIdx.x; c < p.Dd; c += kPT) xs[c] = reinterpret_cast<const E*>(xp)[rb + c];
+    for (uint32_t c = threadIdx.x; c < p.Dd; c += kDT) xs[c] = reinterpret_cast<const E*>(xp)[rb + c];
     __syncthreads();
     const uint32_t u = __ldg(p.ulist + iu);
-    for (uint32_t c = threadIdx.x; c < p.Dd; c += kPT) {
+    for (uint32_t c = threadIdx.x; c < p.Dd; c += kDT) {
       R ar, ai, xr, xi;
       T::ld(yp, rb + c, ar, ai);
       {
@@ -444,13 +445,13 @@ int pair_apply(const PairHandle* h, qk_dtype t, const void* x, void* y, cudaStre
       auto k = k_pair_dn<DT, true>;                                                                        \
       if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)   \
         return QKD_EINVAL;                                                                                 \
-      const unsigned g = resident_grid(k, kPT, smem, std::min<unsigned>(h->host.Du, kMaxG));               \
-      k<<<g, kPT, smem, s>>>(h->dev, xp, yp, y, w->partials, w->ticket, dot_out);                          \
+      const unsigned g = resident_grid(k, kDT, smem, std::min<unsigned>(h->host.Du, kMaxG));               \
+      k<<<g, kDT, smem, s>>>(h->dev, xp, yp, y, w->partials, w->ticket, dot_out);                          \
     } else {                                                                                               \
       auto k = k_pair_dn<DT, false>;                                                                       \
       if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)   \
         return QKD_EINVAL;                                                                                 \
-      k<<<resident_grid(k, kPT, smem, h->host.Du), kPT, smem, s>>>(h->dev, xp, yp, y, nullptr, nullptr, nullptr); \
+      k<<<resident_grid(k, kDT, smem, h->host.Du), kDT, smem, s>>>(h->dev, xp, yp, y, nullptr, nullptr, nullptr); \
     }                                                                                                      \
   }
   switch (t) {
