@@ -144,11 +144,12 @@ __global__ void __launch_bounds__(kPT) k_pair_up(const PairPlan* __restrict__ pp
   }
 }
 
-// Row u of the product order staged in shared memory; per element the down
-// hops and the diagonal are added to y_p and the result goes to its
+// NR rows u of the product order staged in shared memory; per column d the
+// down hops' table words are read once and serve all NR rows; per element
+// the hops and the diagonal are added to y_p and the result goes to its
 // reference-order slot with the sign S.  DOT: <x, y> summed per CTA in a
 // fixed order, then over CTAs (deterministic for a given grid).
-template <int DT, bool DOT>
+template <int DT, bool DOT, int NR>
 __global__ void __launch_bounds__(kDT) k_pair_dn(const PairPlan* __restrict__ pp, const void* __restrict__ xp,
                                                  const void* __restrict__ yp, void* __restrict__ y,
                                                  double* partials, unsigned* ticket, double* dot_out) {
@@ -156,57 +157,81 @@ __global__ void __launch_bounds__(kDT) k_pair_dn(const PairPlan* __restrict__ pp
   using R = typename T::R;
   using E = typename T::E;
   extern __shared__ __align__(16) unsigned char smraw[];
-  E* xs = reinterpret_cast<E*>(smraw);
+  E* xs = reinterpret_cast<E*>(smraw);  // [NR][Dd]
   __shared__ double s_red[2 * (kDT / 32)];
   const PairPlan& p = *pp;
+  const uint32_t Dd = p.Dd;
   double dr = 0.0, di = 0.0;
   const bool packed = p.dn_ent != nullptr;
   const R mag = R(p.dn_mag);
-  for (uint32_t iu = blockIdx.x; iu < p.Du; iu += gridDim.x) {
-    const uint64_t rb = uint64_t(iu) * p.Dd;
-    __syncthreads();  // the previous row is finished with the staging
-    for (uint32_t c = threadIdx.x; c < p.Dd; c += kDT) xs[c] = reinterpret_cast<const E*>(xp)[rb + c];
+  auto split = [](const E& v, R& re, R& im) {
+    if constexpr (T::cplx) { re = v.x; im = v.y; } else { re = v; im = R(0); }
+  };
+  for (uint32_t iu0 = blockIdx.x * NR; iu0 < p.Du; iu0 += gridDim.x * NR) {
+    const uint32_t nr = min(uint32_t(NR), p.Du - iu0);
+    __syncthreads();  // the previous rows are finished with the staging
+    for (uint32_t i = threadIdx.x; i < nr * Dd; i += kDT)
+      xs[i] = reinterpret_cast<const E*>(xp)[uint64_t(iu0) * Dd + i];
     __syncthreads();
-    const uint32_t u = __ldg(p.ulist + iu);
-    for (uint32_t c = threadIdx.x; c < p.Dd; c += kDT) {
-      R ar, ai, xr, xi;
-      T::ld(yp, rb + c, ar, ai);
-      {
-        const E v = xs[c];
-        if constexpr (T::cplx) { xr = v.x; xi = v.y; } else { xr = v; xi = R(0); }
-      }
-      const R dg = R(__ldg(p.diag + rb + c));
-      ar += dg * xr;
-      if (T::cplx) ai += dg * xi;
+    for (uint32_t c = threadIdx.x; c < Dd; c += kDT) {
       const uint32_t k0 = __ldg(p.dn_ptr + c), k1 = __ldg(p.dn_ptr + c + 1);
-      R sr = R(0), si = R(0);
+      R sr[NR], si[NR];
+      #pragma unroll
+      for (int r = 0; r < NR; ++r) { sr[r] = R(0); si[r] = R(0); }
       if (packed) {
-        for (uint32_t k = k0; k < k1; ++k) {
-          const uint32_t e = __ldg(p.dn_ent + k);
-          const E v = xs[e & 0x7FFFu];
-          R vr, vi;
-          if constexpr (T::cplx) { vr = v.x; vi = v.y; } else { vr = v; vi = R(0); }
-          if (e & 0x8000u) { sr -= vr; if (T::cplx) si -= vi; }
-          else { sr += vr; if (T::cplx) si += vi; }
+        // four hops at a time: their table words, then their row values
+        auto hop = [&](uint32_t e) {
+          const uint32_t col = e & 0x7FFFu;
+          #pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            R vr, vi;
+            split(xs[r * Dd + col], vr, vi);
+            if (e & 0x8000u) { sr[r] -= vr; if (T::cplx) si[r] -= vi; }
+            else { sr[r] += vr; if (T::cplx) si[r] += vi; }
+          }
+        };
+        uint32_t k = k0;
+        for (; k + 4 <= k1; k += 4) {
+          uint32_t e[4];
+          #pragma unroll
+          for (int j = 0; j < 4; ++j) e[j] = __ldg(p.dn_ent + k + j);
+          #pragma unroll
+          for (int j = 0; j < 4; ++j) hop(e[j]);
         }
-        ar += mag * sr;
-        if (T::cplx) ai += mag * si;
+        for (; k < k1; ++k) hop(__ldg(p.dn_ent + k));
+        #pragma unroll
+        for (int r = 0; r < NR; ++r) { sr[r] *= mag; si[r] *= mag; }
       } else {
         for (uint32_t k = k0; k < k1; ++k) {
-          const E v = xs[__ldg(p.dn_col + k)];
+          const uint32_t col = __ldg(p.dn_col + k);
           const R w = R(__ldg(p.dn_val + k));
-          R vr, vi;
-          if constexpr (T::cplx) { vr = v.x; vi = v.y; } else { vr = v; vi = R(0); }
-          ar += w * vr;
-          if (T::cplx) ai += w * vi;
+          #pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            R vr, vi;
+            split(xs[r * Dd + col], vr, vi);
+            sr[r] += w * vr;
+            if (T::cplx) si[r] += w * vi;
+          }
         }
       }
       const uint32_t d = __ldg(p.dlist + c);
-      const R sg = R(pair_sign(u, d));
-      T::st(y, pair_rank(p, u, d), sg * ar, sg * ai);
-      if (DOT) {  // <x, y> = <x_p, y_p> (S^2 = 1)
-        dr += double(xr) * double(ar) + double(xi) * double(ai);
-        di += double(xr) * double(ai) - double(xi) * double(ar);
+      #pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        if (uint32_t(r) >= nr) break;
+        const uint64_t i = uint64_t(iu0 + r) * Dd + c;
+        R ar, ai, xr, xi;
+        T::ld(yp, i, ar, ai);
+        split(xs[r * Dd + c], xr, xi);
+        const R dg = R(__ldg(p.diag + i));
+        ar += dg * xr + sr[r];
+        if (T::cplx) ai += dg * xi + si[r];
+        const uint32_t u = __ldg(p.ulist + iu0 + r);
+        const R sg = R(pair_sign(u, d));
+        T::st(y, pair_rank(p, u, d), sg * ar, sg * ai);
+        if (DOT) {  // <x, y> = <x_p, y_p> (S^2 = 1)
+          dr += double(xr) * double(ar) + double(xi) * double(ai);
+          di += double(xr) * double(ai) - double(xi) * double(ar);
+        }
       }
     }
   }
@@ -435,23 +460,30 @@ int pair_apply(const PairHandle* h, qk_dtype t, const void* x, void* y, cudaStre
   }
   void* xp = scr;
   void* yp = static_cast<char*>(scr) + n * es;
-  const size_t smem = es * h->host.Dd;
-  if (smem > 200 * 1024) return QKD_EINVAL;
+  // rows staged per pass of the down-hop kernel: as many as 220 KB hold (1, 2
+  // or 4; a CTA may use up to 227 KB of shared memory)
+  constexpr size_t kStage = 220 * 1024;
+  const size_t row_bytes = es * h->host.Dd;
+  if (row_bytes > kStage) return QKD_EINVAL;
+  const int nr = row_bytes * 4 <= kStage ? 4 : row_bytes * 2 <= kStage ? 2 : 1;
+  const size_t smem = row_bytes * nr;
+#define QKD_PAIR_DN(DT, DOT, NR)                                                                           \
+  {                                                                                                        \
+    auto k = k_pair_dn<DT, DOT, NR>;                                                                       \
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)     \
+      return QKD_EINVAL;                                                                                   \
+    const unsigned rows = (h->host.Du + NR - 1) / NR;                                                      \
+    const unsigned g = resident_grid(k, kDT, smem, DOT ? std::min<unsigned>(rows, kMaxG) : rows);          \
+    k<<<g, kDT, smem, s>>>(h->dev, xp, yp, y, DOT ? w->partials : nullptr, DOT ? w->ticket : nullptr, dot_out); \
+  }
 #define QKD_PAIR(DT)                                                                                       \
   {                                                                                                        \
     k_pair_in<DT, true><<<resident_grid(k_pair_in<DT, true>, kPT, 0, 1u << 20), kPT, 0, s>>>(h->dev, x, xp); \
     k_pair_up<DT><<<resident_grid(k_pair_up<DT>, kPT, 0, 1u << 20), kPT, 0, s>>>(h->dev, xp, yp);       \
     if (dot_out) {                                                                                         \
-      auto k = k_pair_dn<DT, true>;                                                                        \
-      if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)   \
-        return QKD_EINVAL;                                                                                 \
-      const unsigned g = resident_grid(k, kDT, smem, std::min<unsigned>(h->host.Du, kMaxG));               \
-      k<<<g, kDT, smem, s>>>(h->dev, xp, yp, y, w->partials, w->ticket, dot_out);                          \
+      if (nr == 4) QKD_PAIR_DN(DT, true, 4) else if (nr == 2) QKD_PAIR_DN(DT, true, 2) else QKD_PAIR_DN(DT, true, 1) \
     } else {                                                                                               \
-      auto k = k_pair_dn<DT, false>;                                                                       \
-      if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)   \
-        return QKD_EINVAL;                                                                                 \
-      k<<<resident_grid(k, kDT, smem, h->host.Du), kDT, smem, s>>>(h->dev, xp, yp, y, nullptr, nullptr, nullptr); \
+      if (nr == 4) QKD_PAIR_DN(DT, false, 4) else if (nr == 2) QKD_PAIR_DN(DT, false, 2) else QKD_PAIR_DN(DT, false, 1) \
     }                                                                                                      \
   }
   switch (t) {
@@ -462,6 +494,7 @@ int pair_apply(const PairHandle* h, qk_dtype t, const void* x, void* y, cudaStre
     default: return QKD_EINVAL;
   }
 #undef QKD_PAIR
+#undef QKD_PAIR_DN
   QKD_LAUNCH_CHECK();
   return QKD_OK;
 }
