@@ -48,6 +48,7 @@ struct PairPlan {
   const double* dn_val;
   double dn_mag;
   const double* diag;      // D in product order (Du * Dd)
+  const uint32_t* perm;    // rank(u, d) in product order (Du * Dd), or null: computed from A, B
 };
 
 namespace {
@@ -89,9 +90,19 @@ __global__ void __launch_bounds__(kPT) k_pair_in(const PairPlan* __restrict__ pp
     const uint32_t iu = uint32_t(i / p.Dd), id = uint32_t(i - uint64_t(iu) * p.Dd);
     const uint32_t u = __ldg(p.ulist + iu), d = __ldg(p.dlist + id);
     R re, im;
-    T::ld(x, pair_rank(p, u, d), re, im);
+    T::ld(x, p.perm ? __ldg(p.perm + i) : pair_rank(p, u, d), re, im);
     const R sg = SIGN ? R(pair_sign(u, d)) : R(1);
     T::st(xp, i, sg * re, sg * im);
+  }
+}
+
+// perm[i] = rank(u, d) for the product index i = iu * Dd + id
+__global__ void __launch_bounds__(kPT) k_pair_perm(const PairPlan* __restrict__ pp, uint32_t* __restrict__ perm) {
+  const PairPlan& p = *pp;
+  const uint64_t n = uint64_t(p.Du) * p.Dd;
+  for (uint64_t i = blockIdx.x * uint64_t(kPT) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * kPT) {
+    const uint32_t iu = uint32_t(i / p.Dd), id = uint32_t(i - uint64_t(iu) * p.Dd);
+    perm[i] = pair_rank(p, __ldg(p.ulist + iu), __ldg(p.dlist + id));
   }
 }
 
@@ -227,7 +238,7 @@ __global__ void __launch_bounds__(kDT) k_pair_dn(const PairPlan* __restrict__ pp
         if (T::cplx) ai += dg * xi + si[r];
         const uint32_t u = __ldg(p.ulist + iu0 + r);
         const R sg = R(pair_sign(u, d));
-        T::st(y, pair_rank(p, u, d), sg * ar, sg * ai);
+        T::st(y, p.perm ? __ldg(p.perm + i) : pair_rank(p, u, d), sg * ar, sg * ai);
         if (DOT) {  // <x, y> = <x_p, y_p> (S^2 = 1)
           dr += double(xr) * double(ar) + double(xi) * double(ai);
           di += double(xr) * double(ai) - double(xi) * double(ar);
@@ -425,6 +436,22 @@ PairHandle* pair_plan_create(const qk_plan_desc* d, const uint64_t* A_dev, const
     const unsigned g = resident_grid(k_pair_in<QK_F64, false>, kPT, 0, 4096);
     k_pair_in<QK_F64, false><<<g, kPT>>>(out->dev, diag_ref, dp);
     ok = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess;
+  }
+  if (ok) {
+    // the reference rank of every product index, read coalesced by the
+    // gather and the scatter instead of two scattered table lookups per
+    // element (4 bytes per state; without the memory the kernels compute it)
+    uint32_t* pm = nullptr;
+    if (cudaMalloc(&pm, d->dim * 4) == cudaSuccess) {
+      out->bufs.push_back(pm);
+      *dev_bytes += d->dim * 4;
+      k_pair_perm<<<resident_grid(k_pair_perm, kPT, 0, 4096), kPT>>>(out->dev, pm);
+      ok = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess;
+      h.perm = pm;
+      ok = ok && cudaMemcpy(out->dev, &h, sizeof(PairPlan), cudaMemcpyHostToDevice) == cudaSuccess;
+    } else {
+      (void)cudaGetLastError();
+    }
   }
   if (!ok) {
     (void)cudaGetLastError();
