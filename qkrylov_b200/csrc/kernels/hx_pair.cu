@@ -160,6 +160,9 @@ __global__ void __launch_bounds__(kPT) k_pair_up(const PairPlan* __restrict__ pp
 // the hops and the diagonal are added to y_p and the result goes to its
 // reference-order slot with the sign S.  DOT: <x, y> summed per CTA in a
 // fixed order, then over CTAs (deterministic for a given grid).
+template <class E, int NR>
+struct alignas(sizeof(E) * NR) RowPack { E v[NR]; };
+
 template <int DT, bool DOT, int NR>
 __global__ void __launch_bounds__(kDT) k_pair_dn(const PairPlan* __restrict__ pp, const void* __restrict__ xp,
                                                  const void* __restrict__ yp, void* __restrict__ y,
@@ -168,7 +171,11 @@ __global__ void __launch_bounds__(kDT) k_pair_dn(const PairPlan* __restrict__ pp
   using R = typename T::R;
   using E = typename T::E;
   extern __shared__ __align__(16) unsigned char smraw[];
-  E* xs = reinterpret_cast<E*>(smraw);  // [NR][Dd]
+  // the NR rows interleaved: element (r, d) at d * NR + r, so one vector
+  // load fetches a column of all NR rows
+  using Pack = RowPack<E, NR>;
+  E* xs = reinterpret_cast<E*>(smraw);
+  const Pack* xsp = reinterpret_cast<const Pack*>(smraw);
   __shared__ double s_red[2 * (kDT / 32)];
   const PairPlan& p = *pp;
   const uint32_t Dd = p.Dd;
@@ -181,8 +188,10 @@ __global__ void __launch_bounds__(kDT) k_pair_dn(const PairPlan* __restrict__ pp
   for (uint32_t iu0 = blockIdx.x * NR; iu0 < p.Du; iu0 += gridDim.x * NR) {
     const uint32_t nr = min(uint32_t(NR), p.Du - iu0);
     __syncthreads();  // the previous rows are finished with the staging
-    for (uint32_t i = threadIdx.x; i < nr * Dd; i += kDT)
-      xs[i] = reinterpret_cast<const E*>(xp)[uint64_t(iu0) * Dd + i];
+    for (uint32_t i = threadIdx.x; i < nr * Dd; i += kDT) {
+      const uint32_t r = i / Dd, c = i - r * Dd;
+      xs[c * NR + r] = reinterpret_cast<const E*>(xp)[uint64_t(iu0) * Dd + i];
+    }
     __syncthreads();
     for (uint32_t c = threadIdx.x; c < Dd; c += kDT) {
       const uint32_t k0 = __ldg(p.dn_ptr + c), k1 = __ldg(p.dn_ptr + c + 1);
@@ -192,11 +201,11 @@ __global__ void __launch_bounds__(kDT) k_pair_dn(const PairPlan* __restrict__ pp
       if (packed) {
         // four hops at a time: their table words, then their row values
         auto hop = [&](uint32_t e) {
-          const uint32_t col = e & 0x7FFFu;
+          const Pack pk = xsp[e & 0x7FFFu];
           #pragma unroll
           for (int r = 0; r < NR; ++r) {
             R vr, vi;
-            split(xs[r * Dd + col], vr, vi);
+            split(pk.v[r], vr, vi);
             if (e & 0x8000u) { sr[r] -= vr; if (T::cplx) si[r] -= vi; }
             else { sr[r] += vr; if (T::cplx) si[r] += vi; }
           }
@@ -214,12 +223,12 @@ __global__ void __launch_bounds__(kDT) k_pair_dn(const PairPlan* __restrict__ pp
         for (int r = 0; r < NR; ++r) { sr[r] *= mag; si[r] *= mag; }
       } else {
         for (uint32_t k = k0; k < k1; ++k) {
-          const uint32_t col = __ldg(p.dn_col + k);
+          const Pack pk = xsp[__ldg(p.dn_col + k)];
           const R w = R(__ldg(p.dn_val + k));
           #pragma unroll
           for (int r = 0; r < NR; ++r) {
             R vr, vi;
-            split(xs[r * Dd + col], vr, vi);
+            split(pk.v[r], vr, vi);
             sr[r] += w * vr;
             if (T::cplx) si[r] += w * vi;
           }
@@ -232,7 +241,7 @@ __global__ void __launch_bounds__(kDT) k_pair_dn(const PairPlan* __restrict__ pp
         const uint64_t i = uint64_t(iu0 + r) * Dd + c;
         R ar, ai, xr, xi;
         T::ld(yp, i, ar, ai);
-        split(xs[r * Dd + c], xr, xi);
+        split(xs[c * NR + r], xr, xi);
         const R dg = R(__ldg(p.diag + i));
         ar += dg * xr + sr[r];
         if (T::cplx) ai += dg * xi + si[r];
