@@ -651,8 +651,9 @@ def profile_case(qk, name):
                        reorthogonalisation, at C3's vector length / 10)
       sweep-n20        the batched coupling sweep on the J1-J2 chain N=20 (its
                        column multi-dot / multi-update kernels)
-      hub44-hx         Hubbard 4x4, U=4, 8 up 8 down (dim 165,636,900) two-part
-                       row kernel, float64, 3 applies (2.6 GB of vectors)"""
+      hub44-hx         Hubbard 4x4, U=4, 8 up 8 down (dim 165,636,900) H.x on
+                       its default path (spin-product), float64, 3 applies
+      hub44-hx-two-part  the same on the two-part row kernel"""
     import torch
     out = {}
     if name in ("tj20-hx", "tj20-ftlm-block"):
@@ -684,7 +685,9 @@ def profile_case(qk, name):
             L.qkrylov_b200_multi_dot(torch.cuda.current_device(), qk.DTYPE_F64, n, k, ptrs,
                                      ctypes.c_void_p(x.data_ptr()), o.ctypes.data)
         out.update(n=n, k=k)
-    elif name == "hub44-hx":
+    elif name in ("hub44-hx", "hub44-hx-two-part"):
+        if name == "hub44-hx-two-part":
+            qk.set_kernel_policy("no-spin-product")
         H = qk.MatrixFreeHamiltonian(qk.HubbardBasis(16, nup=8, ndn=8), qk.HubbardSite(),
                                      hubbard_opsum(qk, 4, 4, 1.0, 4.0), dtype=np.float64)
         out["dim"] = H.dimension
