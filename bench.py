@@ -836,6 +836,10 @@ def run_b200(args):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / ke2e
+    if dist is not None and world > 1:  # the slowest rank's host round trip
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
 
     traffic = profiled_traffic() if N == 28 else None
 
@@ -855,7 +859,9 @@ def run_b200(args):
             "variants": variants,
             "gpu_launches": launches,
             "clocks": clk.summary()}
-    if rank == 0 and not args.no_solvers:
+    # the solver legs and the CPU baseline are single-GPU measurements: they
+    # run with one rank (N=1) only
+    if rank == 0 and world == 1 and not args.no_solvers:
         try:
             torch.cuda.empty_cache()
             line["time_to_e0"] = time_to_e0(qk, N)
@@ -889,7 +895,7 @@ def run_b200(args):
             line["hubbard_c3"] = hubbard_c3(qk)
         except Exception as e:
             line["hubbard_c3"] = {"error": str(e)}
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cb = cpu_reference_gbs(N=24, steps=5)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
