@@ -31,7 +31,6 @@ int spin_apply_block(const SpinHandle* h, qk_dtype t, int R, int lpr, const void
                      cudaStream_t s, qk_workspace* w, const double* gacc = nullptr, int tilec = 0);
 void spin_plan_destroy(SpinHandle* h);
 void spin_set_die_queues(bool on);
-void spin_set_row_flags(uint32_t f);
 int spin_apply_range(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, uint64_t row_lo,
                      uint64_t row_hi);
 int spin_apply(const SpinHandle* h, qk_dtype t, const void* x, void* y, cudaStream_t s, qk_workspace* w,

@@ -906,9 +906,9 @@ bool die_map(const uint8_t** dev_map, int* nsmid, int* n0, int* n1);
 
 // Per-die work queues (process-wide switch, for comparisons).
 static bool g_die_queues = true;
-// Launch flags of the row kernel, process-wide: y is written once and not
-// read again by the kernel, so it is stored with the streaming hint.
-static uint32_t g_row_flags = kRowStreamY;
+// Launch flags of the row kernel: y is written once and not read again by
+// the kernel, so it is stored with the streaming hint.
+constexpr uint32_t g_row_flags = kRowStreamY;
 
 // When the GPU has two dies: split the visiting sequence into a share per
 // die in proportion to its SMs (by rows), and allocate the queue counters.
@@ -1692,7 +1692,6 @@ int spin_apply_range(const SpinHandle* h, qk_dtype t, const void* x, void* y, cu
 }
 
 void spin_set_die_queues(bool on) { g_die_queues = on; }
-void spin_set_row_flags(uint32_t f) { g_row_flags = f; }
 
 }  // namespace qkd
 

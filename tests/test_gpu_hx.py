@@ -294,3 +294,19 @@ def test_spin_product_path_matches_two_part_and_oracle(N, nup, ndn, lat):
     finally:
         qk.set_kernel_policy("auto")
     assert abs(es[0] - es[1]) < 1e-11 * abs(es[1])
+
+
+@pytest.mark.parametrize("nup,ndn", [(0, 3), (4, 0), (1, 1), (6, 5)])
+def test_spin_product_edge_sectors(nup, ndn):
+    """Edge sectors of the spin-product path: one species empty (a factor
+    with no hops), a single electron of each species, a nearly full
+    lattice; against the CPU oracle."""
+    N = 6
+    sec = dict(use_nup=1, nup=nup, use_ndn=1, ndn=ndn)
+    terms = O.hubbard_square(3, 2, 1.0, 4.0)
+    H = ham("hubbard", N, sec, terms)
+    ref = O.port().hamiltonian("hubbard", N, sec, terms)
+    assert H.dimension == ref.dim
+    rng = np.random.default_rng(nup * 7 + ndn)
+    x = rng.standard_normal(H.dimension) + 1j * rng.standard_normal(H.dimension)
+    assert rel(H.apply(x), ref.apply(x)) < 1e-13, H.kernel
