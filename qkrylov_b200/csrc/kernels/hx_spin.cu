@@ -204,7 +204,7 @@ k_hx_spin(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void* __r
 // plan builder checks the high-bond sizes.
 constexpr int kRowThreads = 256;
 constexpr uint32_t kRowStreamY = 1u;  // launch flag: store y with the streaming (evict-first) hint
-constexpr int kRowHighC128 = 4;   // complex128: high bonds held in registers (more spill)
+constexpr int kRowHighC128 = 3;   // complex128: high bonds held in registers (4: 1% slower, 6: 2%)
 constexpr int kRowMinCtaC128 = 2; // complex128: CTAs per SM the registers are sized for
 constexpr int kRowThreadsC128 = 512;  // complex128: threads per CTA (one staged block shared by 16 warps)
 constexpr int kPrefetchAhead = 2; // row chunks of high-bond partner rows prefetched into L2
