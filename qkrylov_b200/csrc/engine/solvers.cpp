@@ -394,6 +394,16 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
   DevVec coef(size_t(2) * (maxiter + 8), QK_F64, H.device());
   double e = 0.0, eps_prev = 1e300, t_fp64 = 0.0;
   int steps = 0;
+  // passes of at most `pass` steps: the reorthogonalisation cost of a pass
+  // grows with the square of its length, a restart from the Ritz vector
+  // resets it.  Heisenberg N=28 to residual 1e-10: 0.315 s with passes of
+  // 64 (112 FP32 steps), 0.234 s with 32 (118), 0.252 s with 24; 16 made
+  // Hubbard 4x4's FP32 passes stall and fall back to FP64 (4.2 s vs 2.5 s).
+  // A pass that cuts the residual less than tenfold (a small relative gap,
+  // where restarting from the Ritz vector alone converges slowly) doubles
+  // the length of the next one.
+  constexpr int kPass = 32;
+  int pass = std::min(maxiter, kPass);
   for (int outer = 0; outer < 40; ++outer) {
     const double tr0 = now_s();
     const double nr = residual(e);
@@ -410,16 +420,11 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
       psi_t = DevVec(dim, ti, H.device(), false);
       wt = DevVec(dim, ti, H.device(), false);
     }
+    if (outer > 0 && eps > 0.1 * eps_prev) pass = std::min(maxiter, 2 * pass);
     eps_prev = eps;
     const double target = std::max(0.3 * tol_res, 1e-6 * eps);
     const double tp0 = now_s();
-    // passes of at most kPass steps: the reorthogonalisation cost of a pass
-    // grows with the square of its length, a restart from the Ritz vector
-    // resets it.  Heisenberg N=28 to residual 1e-10: 0.315 s with passes of
-    // 64 (112 FP32 steps), 0.234 s with 32 (118), 0.252 s with 24; 16 made
-    // Hubbard 4x4's FP32 passes stall and fall back to FP64 (4.2 s vs 2.5 s)
-    constexpr int kPass = 32;
-    const int m = refine_pass(H, ti, hi, psi, w, e, nr, std::min(maxiter, kPass), target, V, psi_t, wt, tmp, P,
+    const int m = refine_pass(H, ti, hi, psi, w, e, nr, pass, target, V, psi_t, wt, tmp, P,
                               coef, out.trace, steps + out.iters_high, t0);
     steps += m;
     if (ti == lo) out.iters_low += m;

@@ -220,7 +220,10 @@ constexpr int kRowCoef = 32, kRowEnt = 48, kRowCross = 16, kRowCls = 4;
 // 8 CTAs).  complex128: one row per thread, 512-thread CTAs, 2 per SM.
 template <int DT, bool GEN> constexpr int kRowBatchG = DT == QK_C128 ? 1 : DT == QK_F32 ? 1 : GEN && DT == QK_F64 ? 1 : 2;
 template <int DT, bool GEN> constexpr int kRowMinCta = DT == QK_C128 ? kRowMinCtaC128 : DT == QK_F32 ? 8 : 6;
-template <int DT> constexpr int kRowHighRegs = DT == QK_C128 ? kRowHighC128 : 8;  // high bonds held in registers
+// high bonds held in registers (two-part tables: 4, t-J N=20 float64
+// 0.347 -> 0.336 ms and float32 0.275 -> 0.265 ms against 8; exchange
+// tables: 8, where 4, 6 and 12 were 1-8% slower)
+template <int DT, bool GEN> constexpr int kRowHighRegs = DT == QK_C128 ? kRowHighC128 : GEN ? 4 : 8;
 template <int DT> constexpr bool kRowPipe = DT == QK_C128;  // rows pipelined one ahead (one row per thread)
 template <int DT> constexpr int kRowNT = DT == QK_C128 ? kRowThreadsC128 : kRowThreads;  // threads per CTA
 // two-part crossing groups whose loads are issued together (fewer where a
@@ -386,7 +389,7 @@ k_hx_spin_rows(const SpinPlan* __restrict__ pp, const void* __restrict__ x, void
     if constexpr (GEN)
       for (int q = 0; q < ncross; ++q) chm |= (((s_ebit[q] >> 16) | (s_ebit[q] >> 18)) & 1u) << q;
     // block-uniform entries in registers: the first NB high bonds, 2 crossing
-    constexpr int NB = kRowHighRegs<DT>;
+    constexpr int NB = kRowHighRegs<DT, GEN>;
     const int nh8 = nh < uint32_t(NB) ? int(nh) : NB;
     uint32_t eb[NB];
     R ec[NB];

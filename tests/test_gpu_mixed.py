@@ -49,6 +49,21 @@ def test_mixed_j1j2_vs_oracle():
     assert abs(r.energy - E_ref) < 1e-10
 
 
+def test_mixed_converges_at_a_small_relative_gap():
+    """J1-J2 chain N=24, J2 = 191/255 (dimerised phase: the two lowest
+    singlets nearly degenerate), random start seed 2: with passes of a fixed
+    32 steps the restarted recurrence stalled near residual 2e-9 and ran out
+    of passes; passes that grow when the residual falls less than tenfold
+    reach tol."""
+    N, J2 = 24, 191 / 255
+    H = ham("spin", N, dict(use_sz=1, sz2=0), O.j1j2_chain(N, 1.0, J2))
+    r = qk.lanczos_mixed(H, seed=2, tol=TOL)
+    ref = qk.lanczos_fp64(H, seed=2, tol=TOL)
+    assert ref.converged
+    assert r.converged and r.residual <= TOL
+    assert abs(r.energy - ref.energy) < 1e-10
+
+
 def test_fp64_baseline_reaches_the_same_energy(golden):
     m = golden["models"]["heis16_sz0"]
     H = ham("spin", 16, m["sector"], O.heisenberg_chain(16))
