@@ -290,6 +290,22 @@ int refine_pass(const Operator& H, qk_dtype ti, qk_dtype hi, DevVec& psi, const 
   P.set(0, psi_t.data(), d.c.stream);
   P.set(1, V[0].data(), d.c.stream);
   std::vector<double> a{E}, b{nr}, z;
+  // Partial reorthogonalisation (H. D. Simon, "The Lanczos algorithm with
+  // partial reorthogonalization", Math. Comp. 42 (1984) 115-142): a step
+  // orthogonalises w against psi only, after the three-term recurrence; the
+  // omega recurrence estimates <v_{j+1}, v_k> for the stored v_k, and when
+  // the largest estimate passes sqrt(u) (u the unit roundoff of the pass's
+  // vectors) w is orthogonalised against all of them, at that step and the
+  // next, and the estimates restart at u.  The Krylov basis stays
+  // semi-orthogonal, which keeps the tridiagonal's Ritz values those of the
+  // projection to working accuracy.
+  const double u = (ti == QK_F32 || ti == QK_C64) ? 0x1p-24 : 0x1p-53, wmax = std::sqrt(u);
+  PtrArray L(2, H.device());
+  L.set(0, psi_t.data(), d.c.stream);
+  L.set(1, wt.data(), d.c.stream);
+  std::vector<double> wprev, wcur{1.0}, wnew;  // omega_{j-1,k}, omega_{j,k}, omega_{j+1,k} over the stored v_k
+  double anorm = std::abs(E) + nr;
+  bool full = false;
   int m = 0;
   for (int j = 0; j < maxiter; ++j) {
     m = j + 1;
@@ -299,22 +315,56 @@ int refine_pass(const Operator& H, qk_dtype ti, qk_dtype hi, DevVec& psi, const 
     const void* U[2] = {V[j].data(), j > 0 ? V[j - 1].data() : nullptr};
     const double co[4] = {alpha, 0.0, j > 0 ? b.back() : 0.0, 0.0};
     const int np = j + 2;  // psi_t, v_1..v_{j+1}
-    P.set(np, wt.data(), d.c.stream);
-    d.update_mdot(j > 0 ? 2 : 1, U, co, P, np + 1, wt.data(), cd);
-    d.mupdate(P, np, cd, wt.data(), cd + 2 * (np + 1));
-    const double* hh = d.c.fetch(cd + 2 * np, 4);
-    double after = hh[2];
-    if (after < 0.25 * hh[0]) {
+    auto orth_all = [&]() {  // w -= sum <P_i, w> P_i over psi_t and every stored v; returns |w|^2
       d.update_mdot(0, nullptr, nullptr, P, np, wt.data(), cd);
       d.mupdate(P, np, cd, wt.data(), cd + 2 * (np + 1));
-      after = d.c.fetch(cd + 2 * (np + 1), 1)[0];
+      return d.c.fetch(cd + 2 * (np + 1), 1)[0];
+    };
+    double before, after;
+    if (full) {
+      P.set(np, wt.data(), d.c.stream);
+      d.update_mdot(j > 0 ? 2 : 1, U, co, P, np + 1, wt.data(), cd);
+      d.mupdate(P, np, cd, wt.data(), cd + 2 * (np + 1));
+      const double* hh = d.c.fetch(cd + 2 * np, 4);
+      before = hh[0];
+      after = hh[2];
+      if (after < 0.25 * before) after = orth_all();
+    } else {
+      d.update_mdot(j > 0 ? 2 : 1, U, co, L, 2, wt.data(), cd);
+      d.mupdate(L, 1, cd, wt.data(), cd + 4);
+      const double* hh = d.c.fetch(cd + 2, 4);
+      before = hh[0];
+      after = hh[2];
     }
-    const double beta = std::sqrt(after);
+    double beta = std::sqrt(after);
+    anorm = std::max(anorm, std::abs(alpha) + b[j] + beta);
+    wnew.assign(size_t(j) + 2, 0.0);
+    double worst = 0.0;
+    if (!full && beta > 0.0) {
+      for (int k = 0; k < j; ++k) {
+        double v = b[k + 1] * wcur[k + 1] + (a[k + 1] - alpha) * wcur[k] - b[j] * wprev[k];
+        if (k > 0) v += b[k] * wcur[k - 1];
+        v += std::copysign(2.0 * u * anorm, v);  // rounding of this step
+        wnew[k] = v / beta;
+        worst = std::max(worst, std::abs(wnew[k]));
+      }
+    }
+    const bool now = !full && (worst > wmax || after < 0.25 * before);
+    if (now) {
+      after = orth_all();
+      beta = std::sqrt(after);
+    }
+    if (full || now) std::fill(wnew.begin(), wnew.begin() + j, u);
+    wnew[j] = beta > 0.0 ? std::max(u, u * anorm / beta) : u;
+    wnew[j + 1] = 1.0;
+    full = now;  // a step that orthogonalised against all is followed by one more
     const double theta = tridiag_ground<double>(a, b, int(a.size()), &z);
     const double est = beta * std::abs(z.back()) / std::abs(theta);
     trace.push_back({it0 + m, theta, now_s() - t0, est});
     if (est <= target || beta < 1e-15 || j + 1 == maxiter) break;
     b.push_back(beta);
+    wprev.swap(wcur);
+    wcur.swap(wnew);
     if (int(V.size()) < j + 2) V.push_back(d.vec(false));
     d.scale_into(1.0 / beta, wt.data(), V[j + 1].data());
     P.set(j + 2, V[j + 1].data(), d.c.stream);
@@ -394,14 +444,16 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
   DevVec coef(size_t(2) * (maxiter + 8), QK_F64, H.device());
   double e = 0.0, eps_prev = 1e300, t_fp64 = 0.0;
   int steps = 0;
-  // passes of at most `pass` steps: the reorthogonalisation cost of a pass
-  // grows with the square of its length, a restart from the Ritz vector
-  // resets it.  Heisenberg N=28 to residual 1e-10: 0.315 s with passes of
-  // 64 (112 FP32 steps), 0.234 s with 32 (118), 0.252 s with 24; 16 made
-  // Hubbard 4x4's FP32 passes stall and fall back to FP64 (4.2 s vs 2.5 s).
-  // A pass that cuts the residual less than tenfold (a small relative gap,
-  // where restarting from the Ritz vector alone converges slowly) doubles
-  // the length of the next one.
+  // passes of at most `pass` steps: the orthogonalisations a pass needs
+  // grow with its length, a restart from the Ritz vector resets them.
+  // Heisenberg N=28 to residual 1e-10 (partial reorthogonalisation): 0.126 s
+  // with passes of 32 (118 FP32 steps), 0.130 s with 48 (110), 0.135 s with
+  // 64 (112); Hubbard 4x4 1.62 s / 1.22 s / 1.26 s (239 / 177 / 179 steps).
+  // With full reorthogonalisation of every step, 32 was also the best of 24,
+  // 32 and 64 on Heisenberg, and 16 made Hubbard's FP32 passes stall and fall
+  // back to FP64.  A pass that cuts the residual less than tenfold (a small
+  // relative gap, where restarting from the Ritz vector alone converges
+  // slowly) doubles the length of the next one.
   constexpr int kPass = 32;
   int pass = std::min(maxiter, kPass);
   for (int outer = 0; outer < 40; ++outer) {
@@ -420,7 +472,13 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
       psi_t = DevVec(dim, ti, H.device(), false);
       wt = DevVec(dim, ti, H.device(), false);
     }
-    if (outer > 0 && eps > 0.1 * eps_prev) pass = std::min(maxiter, 2 * pass);
+    if (outer > 0 && eps > 0.1 * eps_prev) {
+      // a longer pass stores more vectors: at most half of the device's free memory more
+      size_t free_b = 0, total_b = 0;
+      cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+      const size_t room = V.size() + free_b / 2 / (dim * qk_dtype_size(ti));
+      pass = int(std::min<size_t>({size_t(maxiter), size_t(2) * pass, std::max(room, size_t(pass))}));
+    }
     eps_prev = eps;
     const double target = std::max(0.3 * tol_res, 1e-6 * eps);
     const double tp0 = now_s();
