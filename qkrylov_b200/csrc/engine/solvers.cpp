@@ -451,9 +451,12 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
   // 64 (112); Hubbard 4x4 1.62 s / 1.22 s / 1.26 s (239 / 177 / 179 steps).
   // With full reorthogonalisation of every step, 32 was also the best of 24,
   // 32 and 64 on Heisenberg, and 16 made Hubbard's FP32 passes stall and fall
-  // back to FP64.  A pass that cuts the residual less than tenfold (a small
-  // relative gap, where restarting from the Ritz vector alone converges
-  // slowly) doubles the length of the next one.
+  // back to FP64.  A pass that cuts the residual less than twentyfold (a
+  // small relative gap, where restarting from the Ritz vector alone
+  // converges slowly) doubles the length of the next one: Hubbard 4x4 1.62 s
+  // (239 steps) with a tenfold rule, 1.09 s (159) with twentyfold, the same
+  // with 33- and 100-fold; J1-J2 N=24 over 224 couplings 6.2 s with ten- and
+  // twentyfold, 6.6 s with 33-fold.
   constexpr int kPass = 32;
   int pass = std::min(maxiter, kPass);
   for (int outer = 0; outer < 40; ++outer) {
@@ -472,7 +475,7 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
       psi_t = DevVec(dim, ti, H.device(), false);
       wt = DevVec(dim, ti, H.device(), false);
     }
-    if (outer > 0 && eps > 0.1 * eps_prev) {
+    if (outer > 0 && eps > 0.05 * eps_prev) {
       // a longer pass stores more vectors: at most half of the device's free memory more
       size_t free_b = 0, total_b = 0;
       cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");

@@ -53,7 +53,7 @@ def test_mixed_converges_at_a_small_relative_gap():
     """J1-J2 chain N=24, J2 = 191/255 (dimerised phase: the two lowest
     singlets nearly degenerate), random start seed 2: with passes of a fixed
     32 steps the restarted recurrence stalled near residual 2e-9 and ran out
-    of passes; passes that grow when the residual falls less than tenfold
+    of passes; passes that grow when the residual falls less than twentyfold
     reach tol."""
     N, J2 = 24, 191 / 255
     H = ham("spin", N, dict(use_sz=1, sz2=0), O.j1j2_chain(N, 1.0, J2))
