@@ -361,13 +361,17 @@ def cpu_reference_solvers(qk, N=22, tj_N=14, R=64, M=100):
 def time_to_e0(qk, N, tol=1e-10, seed=1):
     """Plain FP64 GPU Lanczos vs the mixed-precision form on the Heisenberg
     chain, both from a GPU random start, both stopped at the explicit FP64
-    residual ||H psi - E psi|| / |E| <= tol; each form runs twice and the
-    second (warm) run is reported."""
+    residual ||H psi - E psi|| / |E| <= tol; the mixed form with partial
+    reorthogonalisation (the default) and with full reorthogonalisation of
+    every FP32 step; each form runs twice and the second (warm) run is
+    reported."""
     H = qk.MatrixFreeHamiltonian(qk.SpinHalfBasis(N, sz=0), qk.SpinHalfSite(), heisenberg_opsum(qk, N, np.float64),
                                  dtype=np.float64)
     out = {"workload": f"heisenberg_chain_N{N}_Sz0", "dim": H.dimension, "tol_residual": tol,
            "start": f"GPU uniform [-1,1) from seed {seed}"}
-    for name, fn in (("plain_fp64", qk.lanczos_fp64), ("mixed", qk.lanczos_mixed)):
+    legs = (("plain_fp64", qk.lanczos_fp64), ("mixed", qk.lanczos_mixed),
+            ("mixed_full_reorth", lambda H, **kw: qk.lanczos_mixed(H, reorth="full", **kw)))
+    for name, fn in legs:
         r = None
         for _ in range(2):
             t0 = time.perf_counter()
@@ -381,10 +385,11 @@ def time_to_e0(qk, N, tol=1e-10, seed=1):
         from oracle import bethe
         eb = bethe.ground_energy(N)
         out["E0_bethe"] = eb
-        out["dE_vs_bethe"] = {k: abs(out[k]["energy"] - eb) for k in ("plain_fp64", "mixed")}
+        out["dE_vs_bethe"] = {k: abs(out[k]["energy"] - eb) for k in ("plain_fp64", "mixed", "mixed_full_reorth")}
     except Exception as e:
         out["E0_bethe"] = {"error": str(e)}
     out["speedup_mixed"] = out["plain_fp64"]["seconds"] / out["mixed"]["seconds"]
+    out["speedup_mixed_full_reorth"] = out["plain_fp64"]["seconds"] / out["mixed_full_reorth"]["seconds"]
     del H
     return out
 
@@ -923,6 +928,7 @@ def summary(line):
     return {"hx_c128_frac": get("roofline", "frac"), "hx_f32_ms": get("variants", "f32", "ms_per_apply"),
             "e2e_GBs": get("e2e", "value"),
             "t2e0_mixed_vs_fp64": get("time_to_e0", "speedup_mixed"),
+            "t2e0_mixed_full_reorth_vs_fp64": get("time_to_e0", "speedup_mixed_full_reorth"),
             "dE_bethe": get("time_to_e0", "dE_vs_bethe"),
             "ftlm_fp64_vs_loop": get("batched_ftlm", "speedup_block_fp64"),
             "ftlm_fp32_vs_loop": get("batched_ftlm", "speedup_block_fp32"),

@@ -236,8 +236,16 @@ int qkrylov_ftlm_sweep_f64(qkrylov_hamiltonian_h h, int n_beta, const double* be
  * orthogonal to psi, followed by the Rayleigh-Ritz step on span{psi, v_1..
  * v_m}.  It stops when ||H psi - E psi|| / |E| <= tol; a pass stops when
  * its Ritz residual estimate drops below max(0.3 tol, 1e-6 |r| / |E|) or
- * after maxiter (<= 511) steps; a pass that fails to halve the residual
- * switches the remaining passes to FP64.
+ * after its length in steps (32 for the first pass, doubled after a pass
+ * that cut the residual less than twentyfold, at most maxiter <= 511 and
+ * half of the device's free memory); a pass that fails to halve the
+ * residual switches the remaining passes to FP64.  Inside a pass the
+ * Krylov vectors are kept semi-orthogonal by partial reorthogonalisation
+ * (Simon 1984: orthogonalised against psi every step, against all stored
+ * vectors only when the omega recurrence's estimate of their loss of
+ * orthogonality exceeds the square root of the vectors' unit roundoff, and
+ * at the step after); qkrylov_b200_lanczos_mixed_full below orthogonalises
+ * every step against all of them.
  *   start: NULL for a random start generated on the GPU from `seed`
  *          (uniform in [-1, 1)), else dimension() elements of the FP32
  *          vector type, in host memory, or in device memory of the
@@ -261,6 +269,16 @@ typedef struct {
 int qkrylov_b200_lanczos_mixed(qkrylov_hamiltonian_h h, uint64_t seed, const void* start, int start_on_device,
                                int maxiter, double tol, qkrylov_b200_mixed_result_t* result, void* psi_out,
                                int trace_cap, int* trace_iteration, double* trace_energy, double* trace_seconds);
+
+/* No counterpart in the reference.  qkrylov_b200_lanczos_mixed with every
+ * step of every pass orthogonalised against psi and all the pass's stored
+ * vectors (classical Gram-Schmidt, a second pass when a vector loses more
+ * than 3/4 of its norm): the FP32-vector form with full
+ * reorthogonalisation, same arguments and results. */
+int qkrylov_b200_lanczos_mixed_full(qkrylov_hamiltonian_h h, uint64_t seed, const void* start,
+                                    int start_on_device, int maxiter, double tol,
+                                    qkrylov_b200_mixed_result_t* result, void* psi_out, int trace_cap,
+                                    int* trace_iteration, double* trace_energy, double* trace_seconds);
 
 /* Plain FP64 Lanczos with full reorthogonalisation from the start (FP64
  * vector type) or a random FP64 start, restarted from its Ritz vector (at

@@ -541,13 +541,17 @@ def _two_phase(fn, H, seed, start, start_device, maxiter, tol, want_vector, low)
 
 def lanczos_mixed(H: MatrixFreeHamiltonian, seed: int = 0, start: Optional[np.ndarray] = None,
                   maxiter: int = 200, tol: float = 1e-10, start_device: Optional[int] = None,
-                  eigenvector: bool = False) -> MixedLanczosResult:
+                  eigenvector: bool = False, reorth: str = "partial") -> MixedLanczosResult:
     """FP32-vector Lanczos (FP64 scalars) followed by FP64 refinement until the
     explicit residual ||H psi - E psi|| / |E| <= tol.  `start`: host FP32
     vector (float32 for real operators, complex64 otherwise), or
-    `start_device`: a device pointer to one; neither: GPU random start."""
-    return _two_phase(lib().qkrylov_b200_lanczos_mixed, H, seed, start, start_device, maxiter, tol, eigenvector,
-                      True)
+    `start_device`: a device pointer to one; neither: GPU random start.
+    `reorth`: "partial" (Simon's partial reorthogonalisation inside the FP32
+    passes) or "full" (every step against all the pass's vectors)."""
+    fns = {"partial": "qkrylov_b200_lanczos_mixed", "full": "qkrylov_b200_lanczos_mixed_full"}
+    if reorth not in fns:
+        raise ValueError('reorth must be "partial" or "full"')
+    return _two_phase(getattr(lib(), fns[reorth]), H, seed, start, start_device, maxiter, tol, eigenvector, True)
 
 
 def lanczos_fp64(H: MatrixFreeHamiltonian, seed: int = 0, start: Optional[np.ndarray] = None,

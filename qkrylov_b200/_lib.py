@@ -105,6 +105,7 @@ PROTOTYPES = {
     "qkrylov_b200_apply_block_device": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp]),
     "qkrylov_ftlm_sweep_f64": (_i, [_vp, _i, _vp, _i, _i, _vp, _vp, _vp]),
     "qkrylov_b200_lanczos_mixed": (_i, [_vp, _u64, _vp, _i, _i, _d, _vp, _vp, _i, _vp, _vp, _vp]),
+    "qkrylov_b200_lanczos_mixed_full": (_i, [_vp, _u64, _vp, _i, _i, _d, _vp, _vp, _i, _vp, _vp, _vp]),
     "qkrylov_b200_lanczos_fp64": (_i, [_vp, _u64, _vp, _i, _i, _d, _vp, _vp, _i, _vp, _vp, _vp]),
     "qkrylov_b200_ftlm_block": (_i, [_vp, _i, _i, _i, _u64, _i, _vp, _vp, _vp, _vp, _i, _vp]),
     "qkrylov_b200_ftlm_loop": (_i, [_vp, _i, _i, _i, _u64, _i, _i, _vp, _vp, _vp, _vp, _vp]),

@@ -398,7 +398,7 @@ int qkrylov_lanczos_ground_state_f64(qkrylov_hamiltonian_h h, int maxiter, doubl
 static int lanczos_two_phase(qkrylov_hamiltonian_h h, bool low_phase, uint64_t seed, const void* start,
                              int start_on_device, int maxiter, double tol, qkrylov_b200_mixed_result_t* result,
                              void* psi_out, int trace_cap, int* trace_iteration, double* trace_energy,
-                             double* trace_seconds) {
+                             double* trace_seconds, bool partial = true) {
   if (!h || !h->op || !result || maxiter < 1 || maxiter > 511 || !(tol > 0) || trace_cap < 0)
     return QKRYLOV_ERROR_INVALID_ARG;
   return guarded([&] {
@@ -416,7 +416,7 @@ static int lanczos_two_phase(qkrylov_hamiltonian_h h, bool low_phase, uint64_t s
       sptr = sdev->data();
     }
     if (psi_out) pdev = std::make_unique<qkb::DevVec>(dim, hi, H.device(), false);
-    auto r = qkb::lanczos_mixed(H, sptr, seed, maxiter, tol, pdev ? pdev->data() : nullptr, low_phase);
+    auto r = qkb::lanczos_mixed(H, sptr, seed, maxiter, tol, pdev ? pdev->data() : nullptr, low_phase, partial);
     if (psi_out) {
       qkb::cuda_check(cudaMemcpyAsync(psi_out, pdev->data(), dim * qk_dtype_size(hi), cudaMemcpyDeviceToHost,
                                       H.ctx().stream), "D2H");
@@ -446,6 +446,14 @@ int qkrylov_b200_lanczos_mixed(qkrylov_hamiltonian_h h, uint64_t seed, const voi
                                int trace_cap, int* trace_iteration, double* trace_energy, double* trace_seconds) {
   return lanczos_two_phase(h, true, seed, start, start_on_device, maxiter, tol, result, psi_out, trace_cap,
                            trace_iteration, trace_energy, trace_seconds);
+}
+
+int qkrylov_b200_lanczos_mixed_full(qkrylov_hamiltonian_h h, uint64_t seed, const void* start, int start_on_device,
+                                    int maxiter, double tol, qkrylov_b200_mixed_result_t* result, void* psi_out,
+                                    int trace_cap, int* trace_iteration, double* trace_energy,
+                                    double* trace_seconds) {
+  return lanczos_two_phase(h, true, seed, start, start_on_device, maxiter, tol, result, psi_out, trace_cap,
+                           trace_iteration, trace_energy, trace_seconds, false);
 }
 
 int qkrylov_b200_lanczos_fp64(qkrylov_hamiltonian_h h, uint64_t seed, const void* start, int start_on_device,

@@ -276,9 +276,11 @@ namespace {
 // correction, whose size is that of the residual, so their rounding enters
 // psi at (FP32 epsilon) x |r|.  Stops when the Ritz residual estimate
 // b_m |z_m| / |theta| <= target, at breakdown or after maxiter steps.
+// partial: partial reorthogonalisation (below); otherwise every step is
+// orthogonalised against psi and all stored v_k.
 int refine_pass(const Operator& H, qk_dtype ti, qk_dtype hi, DevVec& psi, const DevVec& r, double E, double nr,
                 int maxiter, double target, std::vector<DevVec>& V, DevVec& psi_t, DevVec& wt, DevVec& tmp,
-                PtrArray& P, DevVec& coef, std::vector<TraceEntry>& trace, int it0, double t0) {
+                PtrArray& P, DevVec& coef, std::vector<TraceEntry>& trace, int it0, double t0, bool partial) {
   Dev d(H, ti), dh(H, hi);
   const uint64_t dim = H.dim();
   double* cd = static_cast<double*>(coef.data());
@@ -305,7 +307,7 @@ int refine_pass(const Operator& H, qk_dtype ti, qk_dtype hi, DevVec& psi, const 
   L.set(1, wt.data(), d.c.stream);
   std::vector<double> wprev, wcur{1.0}, wnew;  // omega_{j-1,k}, omega_{j,k}, omega_{j+1,k} over the stored v_k
   double anorm = std::abs(E) + nr;
-  bool full = false;
+  bool full = !partial;
   int m = 0;
   for (int j = 0; j < maxiter; ++j) {
     m = j + 1;
@@ -357,7 +359,7 @@ int refine_pass(const Operator& H, qk_dtype ti, qk_dtype hi, DevVec& psi, const 
     if (full || now) std::fill(wnew.begin(), wnew.begin() + j, u);
     wnew[j] = beta > 0.0 ? std::max(u, u * anorm / beta) : u;
     wnew[j + 1] = 1.0;
-    full = now;  // a step that orthogonalised against all is followed by one more
+    full = now || !partial;  // a step that orthogonalised against all is followed by one more
     const double theta = tridiag_ground<double>(a, b, int(a.size()), &z);
     const double est = beta * std::abs(z.back()) / std::abs(theta);
     trace.push_back({it0 + m, theta, now_s() - t0, est});
@@ -382,7 +384,7 @@ int refine_pass(const Operator& H, qk_dtype ti, qk_dtype hi, DevVec& psi, const 
 }  // namespace
 
 MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int maxiter, double tol_res,
-                       void* psi_out, bool low_phase) {
+                       void* psi_out, bool low_phase, bool partial) {
   MixedOut out;
   const uint64_t dim = H.dim();
   if (dim == 0) return out;
@@ -486,7 +488,7 @@ MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int 
     const double target = std::max(0.3 * tol_res, 1e-6 * eps);
     const double tp0 = now_s();
     const int m = refine_pass(H, ti, hi, psi, w, e, nr, pass, target, V, psi_t, wt, tmp, P,
-                              coef, out.trace, steps + out.iters_high, t0);
+                              coef, out.trace, steps + out.iters_high, t0, partial);
     steps += m;
     if (ti == lo) out.iters_low += m;
     else { out.iters_high += m; t_fp64 += now_s() - tp0; }

@@ -99,8 +99,10 @@ struct MixedOut {
   double seconds_low = 0, seconds_high = 0;         // wall time in FP32 passes / FP64 work
   std::vector<TraceEntry> trace;                    // every step, seconds from the start
 };
+// partial: partial reorthogonalisation inside the passes (the default);
+// false: every pass step orthogonalised against all the pass's vectors.
 MixedOut lanczos_mixed(const Operator& H, const void* start, uint64_t seed, int maxiter, double tol_res,
-                       void* psi_out_high, bool low_phase = true);
+                       void* psi_out_high, bool low_phase = true, bool partial = true);
 
 // Batched FTLM on R (32, 64, 128) Rademacher vectors as one row-interleaved
 // block of dtype t, M Lanczos steps without reorthogonalisation (the

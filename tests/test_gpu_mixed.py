@@ -64,6 +64,25 @@ def test_mixed_converges_at_a_small_relative_gap():
     assert abs(r.energy - ref.energy) < 1e-10
 
 
+@pytest.mark.parametrize("N,J2", [(18, 0.35), (20, 0.6)])
+def test_partial_and_full_reorthogonalisation_agree(N, J2):
+    """The default form (partial reorthogonalisation inside the FP32 passes)
+    and the form that orthogonalises every step against all the pass's
+    vectors reach the same energy at the same explicit residual; the
+    oracle's FP64 Lanczos pins both."""
+    model = ("spin", N, dict(use_sz=1, sz2=0), O.j1j2_chain(N, 1.0, J2))
+    E_ref = O.port().hamiltonian(*model).lanczos(200, 1e-13)["energy"]
+    H = ham(*model)
+    rp = qk.lanczos_mixed(H, seed=4, tol=TOL, eigenvector=True)
+    rf = qk.lanczos_mixed(H, seed=4, tol=TOL, eigenvector=True, reorth="full")
+    for r in (rp, rf):
+        assert r.converged and r.residual <= TOL
+        assert abs(r.energy - E_ref) < 1e-10
+        assert residual(H, r.energy, r.eigenvector) < 2 * TOL
+    with pytest.raises(ValueError):
+        qk.lanczos_mixed(H, reorth="none")
+
+
 def test_fp64_baseline_reaches_the_same_energy(golden):
     m = golden["models"]["heis16_sz0"]
     H = ham("spin", 16, m["sector"], O.heisenberg_chain(16))
