@@ -691,9 +691,13 @@ DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int bl
         append(std::move(pv));
       }
     }
-    // the corrections against the basis as one block (classical Gram-Schmidt,
-    // twice: a projection pass and an update pass over the basis per kX
-    // corrections), then one by one against the corrections already taken
+    // the corrections against the basis as one block (classical Gram-Schmidt:
+    // a projection pass and an update pass over the basis per kX
+    // corrections), then one by one against the corrections already taken.
+    // Each is repeated only when the first round removed more than half of a
+    // vector's squared norm ("twice is enough": Daniel, Gragg, Kaufman and
+    // Stewart, Math. Comp. 30 (1976) 772-795); the norm after the block round
+    // is |x|^2 - sum_i <v_i, x>^2, known from the projections.
     int added = 0;
     const int m_old = m;
     for (size_t c0 = 0; c0 < C.size(); c0 += kX) {
@@ -707,15 +711,26 @@ DavidsonBlockOut davidson_block(const Operator& H, qk_dtype t, int n_eig, int bl
       for (int pass = 0; pass < 2; ++pass) {
         const std::vector<double> D = multi_dot(m_old, xs);
         multi_update(m_old, D, xs, true);
+        bool again = false;
+        for (int b = 0; b < cnt; ++b) {
+          double s2 = 0.0;
+          for (int i = 0; i < m_old; ++i) s2 += D[size_t(i) * cnt + b] * D[size_t(i) * cnt + b];
+          again = again || before[b] - s2 < 0.5 * before[b];
+        }
+        if (!again) break;
       }
       for (int b = 0; b < cnt; ++b) {
         if (m >= max_subspace) break;
         DevVec x = std::move(C[c0 + b]);
+        double nn = d.dot(x.data(), x.data()).real();
         for (int pass = 0; pass < 2 && added > 0; ++pass) {  // against the corrections taken so far
           d.update_mdot(0, nullptr, nullptr, PN, added, x.data(), cd);
           d.mupdate(PN, added, cd, x.data(), cd + 2 * (added + 1));
+          const double now = d.c.fetch(cd + 2 * (added + 1), 1)[0];
+          const bool enough = now >= 0.5 * nn;
+          nn = now;
+          if (enough) break;
         }
-        const double nn = d.dot(x.data(), x.data()).real();
         if (!(nn > 1e-20 * std::max(before[b], 1e-300)) || nn == 0.0) continue;
         d.scal(1.0 / std::sqrt(nn), x.data());
         P.set(m, x.data(), d.c.stream);
