@@ -294,8 +294,9 @@ int qkrylov_b200_lanczos_fp64(qkrylov_hamiltonian_h h, uint64_t seed, const void
  * For real operators on float32 (precision 32) or float64 (64) vectors: a
  * seeded random start block of `block` vectors, corrections r / (diag -
  * theta) with the reference's clamp (davidson.cpp:171-175) for the
- * unconverged among the lowest `block` Ritz pairs, orthogonalised twice
- * against the basis; restart from the lowest 2*block Ritz vectors when the
+ * unconverged among the lowest `block` Ritz pairs, orthogonalised against
+ * the basis (a second round when the first removed more than half of a
+ * correction's squared norm); restart from the lowest 2*block Ritz vectors when the
  * basis would exceed max_subspace (3*block <= max_subspace <= 510).  Only
  * the basis is stored (H is applied again to the Ritz vectors for the
  * residuals).  Converged when the n_eig lowest residual norms
