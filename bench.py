@@ -667,6 +667,10 @@ def profile_case(qk, name):
                        reorthogonalisation, at C3's vector length / 10)
       sweep-n20        the batched coupling sweep on the J1-J2 chain N=20 (its
                        column multi-dot / multi-update kernels)
+      davidson-n24     block Davidson (block 8, subspace 64, float64) on the
+                       Heisenberg chain N=24 (dim 2,704,156; a 64-vector basis
+                       is 1.4 GB), 8 iterations: its many-against-many
+                       projection and combination kernels at C3's shapes
       hub44-hx         Hubbard 4x4, U=4, 8 up 8 down (dim 165,636,900) H.x on
                        its default path (spin-product), float64, 3 applies
       hub44-hx-two-part  the same on the two-part row kernel"""
@@ -715,6 +719,12 @@ def profile_case(qk, name):
         torch.cuda.synchronize()
     elif name == "sweep-n20":
         out.update(coupling_sweep(qk, N=20, sequential=False))
+    elif name == "davidson-n24":
+        N = 24
+        H = qk.MatrixFreeHamiltonian(qk.SpinHalfBasis(N, sz=0), qk.SpinHalfSite(), heisenberg_opsum(qk, N, np.float64),
+                                     dtype=np.float64)
+        d = qk.davidson_block(H, n_eig=4, block=8, max_subspace=64, tol=1e-12, seed=1, maxiter=8, precision=64)
+        out.update(dim=H.dimension, iterations=d.iterations, applies=d.applies)
     else:
         raise ValueError(f"unknown profile case {name}")
     return out
