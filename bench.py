@@ -309,12 +309,19 @@ def H_dim_bytes(N):
     return comb(N, N // 2) * 32
 
 
-def cpu_reference_solvers(qk, N=22, tj_N=14, R=64, M=100):
+def cpu_reference_solvers(qk, N=22, tj_N=14, R=64, M=100, j1j2_N=24, j1j2_k=100, hub=(4, 3)):
     """The reference's own CPU solvers (its unchanged sources, oracle/_ref,
     all host threads) beside the library's GPU solvers on the same models at
     sizes the CPU finishes in seconds:
       lanczos  Heisenberg chain N, Sz=0: lanczos_ground_state(maxiter 200,
                tol 1e-12), the reference's start vector on both sides
+      j1j2_coupling  the warm-start workload's chain (J1-J2, j1j2_N, Sz=0) at
+               one coupling J2 = j1j2_k / 255: the reference's time per
+               coupling (set-up and Lanczos) against the GPU's
+               reference-semantics Lanczos and the mixed-precision form
+      hubbard  a periodic hub[0] x hub[1] Hubbard lattice at half filling
+               (the reference cannot build the 4x4 one): reference Lanczos on
+               both sides, and the GPU's mixed-precision form
       ftlm     t-J chain tj_N (2 holes): the reference's ftlm at one
                temperature (R complex Gaussian vectors, M steps) against the
                GPU's reference-semantics ftlm at one temperature and the
@@ -343,6 +350,43 @@ def cpu_reference_solvers(qk, N=22, tj_N=14, R=64, M=100):
                       "cpu_iterations": rc["iterations"], "gpu_seconds": t_gpu, "gpu_iterations": rg.iterations,
                       "dE": abs(rc["energy"] - rg.energy), "speedup": t_cpu / t_gpu}
     del Hg
+    for leg, model, Hg_make in (
+            ("j1j2_coupling", ("spin", j1j2_N, sec, O.j1j2_chain(j1j2_N, 1.0, j1j2_k / 255.0)),
+             lambda: qk.MatrixFreeHamiltonian(qk.SpinHalfBasis(j1j2_N, sz=0), qk.SpinHalfSite(),
+                                              j1j2_opsum(qk, j1j2_N, 1.0, j1j2_k / 255.0), dtype=np.float64)),
+            ("hubbard", ("hubbard", hub[0] * hub[1],
+                         dict(use_nup=1, nup=hub[0] * hub[1] // 2, use_ndn=1, ndn=hub[0] * hub[1] // 2),
+                         O.hubbard_square(hub[0], hub[1], 1.0, 4.0)),
+             lambda: qk.MatrixFreeHamiltonian(qk.HubbardBasis(hub[0] * hub[1], nup=hub[0] * hub[1] // 2,
+                                                              ndn=hub[0] * hub[1] // 2), qk.HubbardSite(),
+                                              hubbard_opsum(qk, hub[0], hub[1], 1.0, 4.0), dtype=np.float64))):
+        t0 = time.perf_counter()
+        Hc = back.hamiltonian(*model)
+        setup = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rc = Hc.lanczos(200, 1e-12, want_vector=False)
+        t_cpu = time.perf_counter() - t0
+        del Hc
+        t0 = time.perf_counter()
+        Hg = Hg_make()
+        g_setup = time.perf_counter() - t0
+        qk.lanczos_ground_state(Hg, 20, 1e-12)  # warm-up
+        t0 = time.perf_counter()
+        rg = qk.lanczos_ground_state(Hg, 200, 1e-12)
+        t_gpu = time.perf_counter() - t0
+        qk.lanczos_mixed(Hg, seed=1, tol=1e-10)  # warm-up
+        t0 = time.perf_counter()
+        rm = qk.lanczos_mixed(Hg, seed=1, tol=1e-10)
+        t_mix = time.perf_counter() - t0
+        out[leg] = {"workload": (f"j1j2_chain_N{j1j2_N}_Sz0_J2_{j1j2_k}/255" if leg == "j1j2_coupling"
+                                 else f"hubbard_{hub[0]}x{hub[1]}_U4_half_filling"),
+                    "dim": Hg.dimension, "cpu_setup_seconds": setup, "cpu_seconds": t_cpu,
+                    "cpu_iterations": rc["iterations"], "gpu_setup_seconds": g_setup, "gpu_seconds": t_gpu,
+                    "gpu_iterations": rg.iterations, "gpu_mixed_seconds": t_mix, "gpu_mixed_residual": rm.residual,
+                    "dE": abs(rc["energy"] - rg.energy), "dE_mixed": abs(rc["energy"] - rm.energy),
+                    "speedup": t_cpu / t_gpu, "speedup_with_setup": (setup + t_cpu) / (g_setup + t_gpu),
+                    "speedup_mixed": t_cpu / t_mix}
+        del Hg
     ne = tj_N - 2
     tsec = dict(use_nup=1, nup=ne // 2, use_ndn=1, ndn=ne - ne // 2)
     Hc = back.hamiltonian("tj", tj_N, tsec, O.tj_chain(tj_N, 1.0, 0.4))
@@ -959,7 +1003,8 @@ def summary(line):
             "hubbard_hx_ms": get("hubbard_c3", "hx_f64_ms"),
             "hubbard_mixed_vs_fp64": get("hubbard_c3", "speedup_mixed_vs_fp64"),
             "hubbard_davidson_ok": get("hubbard_c3", "davidson_block", "converged"),
-            "cpu_ref_GBs": get("cpu_baseline", "value")}
+            "cpu_ref_GBs": get("cpu_baseline", "value"),
+            "j1j2_coupling_cpu_vs_gpu_mixed": get("cpu_baseline", "solvers", "j1j2_coupling", "speedup_mixed")}
 
 
 def main():
